@@ -1,0 +1,127 @@
+"""Known-answer tests from viprs's unit tests, run against the CPU restatement."""
+import numpy as np
+import pytest
+
+
+def test_reduceh_gradient_factor2_bilinear(oracle):
+    # reduceh.rs:595-603
+    img = np.arange(8, dtype=np.uint8).reshape(1, 8, 1)
+    assert oracle.reduce_h(img, 2.0, "bilinear").ravel().tolist() == [1, 3, 5, 6]
+
+
+def test_reduceh_small_multiband_edge_copy(oracle):
+    # reduceh.rs:605-610
+    img = np.array([10, 20, 30, 40, 50, 60, 70, 80, 90, 100, 110, 120], np.uint8).reshape(2, 2, 3)
+    assert oracle.reduce_h(img, 2.0, "bilinear").ravel().tolist() == [25, 35, 45, 85, 95, 105]
+
+
+@pytest.mark.parametrize("kernel", ["nearest", "bilinear", "bicubic", "catmullrom", "lanczos2", "lanczos3"])
+def test_reduceh_single_pixel_edge_copy(oracle, kernel):
+    # reduceh.rs:575-593
+    img = np.array([[[173]]], np.uint8)
+    assert oracle.reduce_h(img, 2.0, kernel).ravel().tolist() == [173]
+
+
+def test_bound_offset_factor2(oracle):
+    # reduce_common.rs:374-383
+    taps, pad, off, _, _ = oracle.reduce_tables(2.0, "bilinear", 8, True)
+    assert abs(off + 0.5) < 1e-12
+    start, phase, pos = oracle.reduce_plan(2.0, "bilinear", 8, True, 0.0)
+    assert abs(pos - 1.0) < 1e-12
+    assert start == -1
+
+
+@pytest.mark.parametrize("kernel", ["nearest", "bilinear", "bicubic", "catmullrom", "lanczos2", "lanczos3"])
+@pytest.mark.parametrize("factor", [1.0, 1.5, 2.0, 2.5, 4.0])
+def test_fixed_point_coefficients_within_truncation_budget(oracle, kernel, factor):
+    # reduce_common.rs:350-372
+    taps, _, _, c64, c16 = oracle.reduce_tables(factor, kernel, 0, False)
+    sums = c16.astype(np.int64).sum(axis=1)
+    assert np.all(np.abs(sums - 4096) <= taps)
+    if kernel in ("bilinear", "lanczos3") and factor in (2.0, 1.5):
+        assert np.all(np.abs(c64.sum(axis=1) - 1.0) < 1e-12)
+
+
+def test_tap_limit(oracle):
+    # reduce_common.rs:412-432: factor 400 exceeds MAX_POINT, factor 4 does not
+    with pytest.raises(ValueError):
+        oracle.reduce_tables(400.0, "lanczos3")
+    assert oracle.reduce_tables(4.0, "lanczos3")[0] == 25
+
+
+def test_shrinkv_factor19_fixed_point_average(oracle):
+    # shrinkv.rs:980-994 against the libvips fixed-point formula
+    w, b, f = 6, 3, 19
+    h = f * 2
+    data = ((np.arange(w * h * b) * 37 + 11) & 0xFF).astype(np.uint8).reshape(h, w, b)
+    out = oracle.shrink_v(data, f)
+    mult = (1 << 32) // (256 * f)
+    sums = data.astype(np.uint64).reshape(2, f, w, b).sum(axis=1) + f // 2
+    ref = ((sums * mult) >> 24).astype(np.uint8)
+    assert np.array_equal(out, ref)
+
+
+def test_thumbnail_plan_4000x3000_width99(oracle):
+    # thumbnail.rs:531-550
+    nodes, (ow, oh), sol = oracle.thumbnail_plan(4000, 3000, 3, "width", 99, 0, allow_shrink_hint=True)
+    assert sol == 16 and (ow, oh) == (99, 74)
+    assert [n["kind"] for n in nodes] == ["shrinkh", "shrinkv", "reduceh", "reducev"]
+    assert nodes[0]["factor"] == 2 and nodes[1]["factor"] == 2
+
+
+def test_thumbnail_plan_crop_extract(oracle):
+    # thumbnail.rs:552-575
+    nodes, (ow, oh), sol = oracle.thumbnail_plan(400, 200, 3, "fitbox", 120, 120, crop=True)
+    assert sol == 0 and (ow, oh) == (120, 120)
+    assert any(n["kind"] == "extract" and n["w"] == 120 and n["h"] == 120 for n in nodes)
+
+
+def test_thumbnail_plan_2048_to_400(oracle):
+    # thumbnail.rs:587-600: integer shrink 4, no affine
+    nodes, _, _ = oracle.thumbnail_plan(2048, 2048, 3, "width", 400, 0, allow_shrink_hint=False)
+    assert nodes[0] == {"kind": "shrinkh", "factor": 4}
+    assert nodes[1] == {"kind": "shrinkv", "factor": 4}
+    assert all(n["kind"] != "affine" for n in nodes)
+
+
+def test_thumbnail_plan_8192_to_400_is_shrink19(oracle):
+    # the in-memory plan for the 8192^2 thumbnail-400 workload
+    nodes, (ow, oh), _ = oracle.thumbnail_plan(8192, 8192, 3, "width", 400, 0, allow_shrink_hint=False)
+    assert (ow, oh) == (400, 400)
+    assert [n["kind"] for n in nodes] == ["shrinkh", "shrinkv", "reduceh", "reducev"]
+    assert nodes[0]["factor"] == 19 and nodes[1]["factor"] == 19
+    assert nodes[2]["factor"] == (8192 / 400) / 19
+
+
+def test_thumbnail_alpha_wrapping(oracle):
+    # thumbnail.rs:438-456: 4-band images are wrapped in premultiply ... unpremultiply
+    nodes, _, _ = oracle.thumbnail_plan(1000, 700, 4, "fitbox", 256, 256, allow_shrink_hint=False)
+    assert nodes[0]["kind"] == "premultiply" and nodes[-1]["kind"] == "unpremultiply"
+
+
+def test_resize_plan_cfg2b(oracle):
+    # resize.rs:216-238: ShrinkV, ShrinkH, ReduceV, ReduceH order; 6000x4000 x0.37
+    nodes, (ow, oh) = oracle.resize_plan(6000, 4000, 0.37, 0.37, "lanczos3")
+    assert (ow, oh) == (2220, 1480)
+    assert [n["kind"] for n in nodes] == ["reducev", "reduceh"]
+
+
+def test_uniform_input_stays_uniform(oracle):
+    img = np.full((37, 53, 3), 77, np.uint8)
+    for out in (oracle.reduce_h(img, 1.7), oracle.reduce_v(img, 2.3), oracle.shrink_h(img, 3),
+                oracle.thumbnail(img, "width", 20, 0)):
+        assert np.all(out == 77)
+
+
+def test_factor_one_identity(oracle):
+    rng = np.random.default_rng(1)
+    img = rng.integers(0, 256, (9, 11, 3), dtype=np.uint8)
+    assert np.array_equal(oracle.reduce_h(img, 1.0), img)
+    assert np.array_equal(oracle.shrink_v(img, 1), img)
+
+
+def test_affine_identity_nearest(oracle):
+    rng = np.random.default_rng(2)
+    img = rng.integers(0, 256, (20, 30, 3), dtype=np.uint8)
+    out = oracle.affine(img, [1, 0, 0, 1], 0, 0, 30, 20, kernel="nearest")
+    assert np.array_equal(out, img)
