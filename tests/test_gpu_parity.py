@@ -1,0 +1,250 @@
+"""Parity of the sm_100a path (through the C ABI) with the CPU restatement of
+viprs and with viprs's golden fixtures.  u8/u16 must be bit-exact; f32 is
+checked with the floored relative error max|a-b|/max(|b|, 1e-3) <= 1e-5."""
+import numpy as np
+import pytest
+
+from golden_cases import CASES, expected
+from gpu_helpers import assert_same, rand_image, smooth_image, to_dev, to_host
+from oracle_chain import run_chain
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from viprs_b200 import api  # noqa: E402
+from viprs_b200._native import ViprsError  # noqa: E402
+
+FMTS = [np.uint8, np.uint16, np.float32]
+KERNELS = ["nearest", "bilinear", "bicubic", "lanczos2", "lanczos3"]
+
+
+def gpu_chain(img, chain):
+    b = api.PipelineBuilder.from_tensor(to_dev(img))
+    for op, kw in chain:
+        if op == "reduce_h":
+            b.reduce_h(kw["factor"], kw["kernel"])
+        elif op == "reduce_v":
+            b.reduce_v(kw["factor"], kw["kernel"])
+        elif op == "reduce":
+            b.reduce(kw["hfactor"], kw["vfactor"], kw["kernel"])
+        elif op == "shrink_h":
+            b.shrink_h(kw["factor"], kw.get("ceil", False))
+        elif op == "shrink_v":
+            b.shrink_v(kw["factor"], kw.get("ceil", False))
+        elif op == "resize":
+            b.resize(kw["hscale"], kw["vscale"], kw.get("kernel", "lanczos3"))
+        elif op == "thumbnail":
+            b.thumbnail(kw["target"], kw["tw"], kw["th"], kw.get("kernel", "lanczos3"), kw.get("crop", False))
+        else:
+            raise ValueError(op)
+    return to_host(b.run())
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_golden_fixture_on_gpu(name):
+    build, chain, shape, tol = CASES[name]
+    img = build()
+    got = gpu_chain(img, chain)
+    exp = expected(name, shape)
+    assert got.shape == exp.shape
+    assert np.abs(got.astype(int) - exp.astype(int)).max() <= tol
+    # and bit-exact against the restatement
+    assert np.array_equal(got, run_chain(img, chain))
+
+
+@pytest.mark.parametrize("fmt", FMTS)
+@pytest.mark.parametrize("kernel", KERNELS)
+@pytest.mark.parametrize("factor", [1.0, 1.3, 2.0, 2.7027027027027026, 4.0])
+@pytest.mark.parametrize("bands", [1, 3, 4])
+def test_reduce_h_v(oracle, fmt, kernel, factor, bands):
+    rng = np.random.default_rng(hash((str(fmt), kernel, factor, bands)) % 2**32)
+    img = rand_image(rng, 23, 41, bands, fmt)
+    assert_same(to_host(api.reduce_h(to_dev(img), factor, kernel)), oracle.reduce_h(img, factor, kernel), fmt)
+    img = rand_image(rng, 41, 23, bands, fmt)
+    assert_same(to_host(api.reduce_v(to_dev(img), factor, kernel)), oracle.reduce_v(img, factor, kernel), fmt)
+
+
+@pytest.mark.parametrize("fmt", FMTS)
+@pytest.mark.parametrize("hv", [(2.0, 2.0), (1.5, 3.25), (4.0, 1.0)])
+def test_reduce_op(oracle, fmt, hv):
+    rng = np.random.default_rng(7)
+    img = rand_image(rng, 33, 29, 3, fmt)
+    got = to_host(api.reduce(to_dev(img), hv[0], hv[1], "lanczos3"))
+    assert_same(got, oracle.reduce(img, hv[0], hv[1], "lanczos3"), fmt)
+
+
+@pytest.mark.parametrize("fmt", FMTS)
+@pytest.mark.parametrize("factor", [1, 2, 3, 5, 7, 19])
+@pytest.mark.parametrize("bands", [1, 2, 3, 4, 5])
+def test_shrink_h_v(oracle, fmt, factor, bands):
+    rng = np.random.default_rng(factor * 10 + bands)
+    img = rand_image(rng, 45, 61, bands, fmt)
+    for ceil in (False, True):
+        assert_same(to_host(api.shrink_h(to_dev(img), factor, ceil)), oracle.shrink_h(img, factor, ceil), fmt)
+        assert_same(to_host(api.shrink_v(to_dev(img), factor, ceil)), oracle.shrink_v(img, factor, ceil), fmt)
+
+
+@pytest.mark.parametrize("fmt", FMTS)
+@pytest.mark.parametrize("fhv", [(2, 2), (3, 5), (19, 19), (1, 4), (6, 1)])
+def test_shrink_chains_both_orders(oracle, fmt, fhv):
+    rng = np.random.default_rng(fhv[0] * 100 + fhv[1])
+    img = rand_image(rng, 77, 83, 3, fmt)
+    fh, fv = fhv
+    hv = [("shrink_h", dict(factor=fh)), ("shrink_v", dict(factor=fv))]
+    vh = [("shrink_v", dict(factor=fv)), ("shrink_h", dict(factor=fh))]
+    for chain in (hv, vh):
+        assert_same(gpu_chain(img, chain), run_chain(img, chain), fmt)
+    assert_same(to_host(api.shrink(to_dev(img), fh, fv)), oracle.pipeline(img, [oracle.make_node("shrink", ufactor=fh, ceil_mode=fv)]), fmt)
+
+
+@pytest.mark.parametrize("fmt", FMTS)
+def test_virtual_plane_chain(oracle, fmt):
+    # shrink -> reduce chain: reduce taps beyond the shrunk image read the shrink
+    # of edge-replicated source pixels, not clamped shrunk pixels
+    rng = np.random.default_rng(11)
+    img = rand_image(rng, 190, 230, 3, fmt)
+    chain = [("shrink_h", dict(factor=7)), ("shrink_v", dict(factor=6)),
+             ("reduce_h", dict(factor=1.37, kernel="lanczos3")), ("reduce_v", dict(factor=1.21, kernel="lanczos3"))]
+    assert_same(gpu_chain(img, chain), run_chain(img, chain), fmt)
+
+
+def test_premultiply_unpremultiply(oracle):
+    rng = np.random.default_rng(3)
+    img = rand_image(rng, 31, 17, 4, np.uint8)
+    pm = oracle.pipeline(img, [oracle.make_node("premultiply")])
+    assert np.array_equal(to_host(api.premultiply(to_dev(img))), pm)
+    up = oracle.pipeline(img, [oracle.make_node("unpremultiply")])
+    assert np.array_equal(to_host(api.unpremultiply(to_dev(img))), up)
+
+
+THUMB_CASES = [
+    (640, 480, 3, "width", 100, 0), (1000, 700, 4, "fitbox", 256, 256), (300, 900, 3, "fitbox", 256, 256),
+    (257, 255, 4, "fitbox", 256, 256), (2049, 1537, 3, "width", 400, 0), (999, 1001, 4, "height", 0, 333),
+    (500, 1, 3, "width", 100, 0), (1, 1, 4, "fitbox", 10, 10), (400, 200, 3, "fitbox", 120, 120),
+    (731, 389, 4, "force", 97, 211), (1536, 1024, 3, "fitbox", 256, 256), (96, 64, 1, "fitbox", 40, 24),
+]
+
+
+@pytest.mark.parametrize("case", THUMB_CASES)
+def test_thumbnail(oracle, case):
+    w, h, b, target, tw, th = case
+    rng = np.random.default_rng(w * 7 + h)
+    img = smooth_image(rng, h, w, b)
+    for crop in (False, True):
+        got = to_host(api.thumbnail(to_dev(img), target, tw, th, "lanczos3", crop))
+        exp = oracle.thumbnail(img, target, tw, th, "lanczos3", crop, threads=4)
+        assert_same(got, exp, np.uint8)
+
+
+def test_thumbnail_with_affine_tail(oracle):
+    # find sizes whose plan ends in the bicubic affine correction
+    rng = np.random.default_rng(5)
+    found = 0
+    for w in range(300, 2000, 37):
+        h = int(w * 0.77) + 3
+        plan, _, _ = oracle.thumbnail_plan(w, h, 4, "fitbox", 256, 256, allow_shrink_hint=False)
+        if any(n["kind"] == "affine" for n in plan):
+            img = smooth_image(rng, h, w, 4)
+            got = to_host(api.thumbnail(to_dev(img), "fitbox", 256, 256))
+            assert_same(got, oracle.thumbnail(img, "fitbox", 256, 256, threads=4), np.uint8)
+            found += 1
+            if found >= 3:
+                break
+    assert found > 0
+
+
+@pytest.mark.parametrize("fmt", [np.uint8, np.float32])
+@pytest.mark.parametrize("scale", [0.75, 0.5, 0.37, 0.2, 0.13])
+def test_resize(oracle, fmt, scale):
+    rng = np.random.default_rng(int(scale * 100))
+    img = rand_image(rng, 157, 211, 4, fmt)
+    got = to_host(api.resize(to_dev(img), scale, scale, "lanczos3"))
+    assert_same(got, oracle.resize(img, scale, scale, "lanczos3"), fmt)
+
+
+def _rot(theta, s):
+    return [s * np.cos(theta), -s * np.sin(theta), s * np.sin(theta), s * np.cos(theta)]
+
+
+@pytest.mark.parametrize("fmt", [np.uint8, np.float32])
+@pytest.mark.parametrize("kernel", ["nearest", "bilinear", "bicubic", "lanczos3"])
+@pytest.mark.parametrize("bands", [1, 3, 4])
+def test_affine_rotated(oracle, fmt, kernel, bands):
+    rng = np.random.default_rng(bands * 13 + len(kernel))
+    img = rand_image(rng, 150, 170, bands, fmt)
+    m = _rot(0.3, 1.15)
+    cx, cy = 85.0, 75.0
+    tx = cx - (m[0] * cx + m[1] * cy) + 4.5
+    ty = cy - (m[2] * cx + m[3] * cy) - 3.25
+    got = to_host(api.affine(to_dev(img), m, tx, ty, 181, 143, kernel))
+    exp = oracle.affine(img, m, tx, ty, 181, 143, kernel)
+    if kernel == "lanczos3" and fmt == np.uint8:
+        # device sin() may differ from glibc's by an ulp: allow rare one-step rounding flips
+        d = np.abs(got.astype(int) - exp.astype(int))
+        assert d.max() <= 1 and (d > 0).mean() < 1e-3
+    else:
+        assert_same(got, exp, fmt)
+
+
+@pytest.mark.parametrize("fmt", [np.uint8, np.float32])
+@pytest.mark.parametrize("kernel", ["nearest", "bilinear", "bicubic"])
+@pytest.mark.parametrize("extend", ["background", "copy", "white", "mirror", "repeat"])
+def test_affine_axis_aligned_and_extend(oracle, fmt, kernel, extend):
+    rng = np.random.default_rng(17)
+    img = rand_image(rng, 60, 70, 3, fmt)
+    m = [0.61, 0.0, 0.0, 0.83]
+    got = to_host(api.affine_backward_matrix(to_dev(img), m, -3.3, 2.1, 130, 90, kernel, extend, 7.0))
+    exp = oracle.affine_backward(img, m, -3.3, 2.1, 130, 90, kernel, extend, 7.0)
+    assert_same(got, exp, fmt)
+
+
+@pytest.mark.parametrize("fmt", [np.uint8, np.float32])
+@pytest.mark.parametrize("kernel", ["nearest", "bilinear", "bicubic", "lanczos3"])
+@pytest.mark.parametrize("bands", [1, 3])
+def test_mapim(oracle, fmt, kernel, bands):
+    rng = np.random.default_rng(bands + len(kernel))
+    src = rand_image(rng, 64, 80, bands, fmt)
+    yy, xx = np.mgrid[0:50, 0:70].astype(np.float32)
+    idx = np.stack([xx * 1.13 - 3.7 + rng.normal(0, 2, xx.shape), yy * 1.21 - 2.2 + rng.normal(0, 2, yy.shape)],
+                   -1).astype(np.float32)
+    idx[3, 5, 0] = np.nan
+    idx[7, 9, 1] = np.inf
+    for extend_copy in (False, True):
+        got = to_host(api.mapim(to_dev(src), to_dev(idx), kernel, extend_copy, 5.0))
+        exp = oracle.mapim(src, idx, kernel, extend_copy, 5.0)
+        if kernel == "lanczos3" and fmt == np.uint8:
+            d = np.abs(got.astype(int) - exp.astype(int))
+            assert d.max() <= 1 and (d > 0).mean() < 1e-3
+        else:
+            assert_same(got, exp, fmt)
+
+
+def test_errors_are_statuses():
+    t = to_dev(np.zeros((8, 8, 3), np.uint8))
+    with pytest.raises(ViprsError) as e:
+        api.reduce_h(t, 0.5)
+    assert e.value.status == 1
+    with pytest.raises(ViprsError) as e:
+        api.reduce_h(t, 400.0, "lanczos3")
+    assert e.value.status == 3
+    with pytest.raises(ViprsError) as e:
+        api.reduce_v(t, 2.0, "lbb")
+    assert e.value.status == 7
+    with pytest.raises(ViprsError) as e:
+        api.affine(t, [1, 2, 2, 4], 0, 0, 8, 8)
+    assert e.value.status == 8
+    with pytest.raises(ViprsError):
+        api.shrink_h(t, 0)
+
+
+def test_plan_reuse_and_launch_count():
+    rng = np.random.default_rng(1)
+    img = smooth_image(rng, 1200, 1600, 3)
+    plan = api.thumbnail_plan(1600, 1200, 3, torch.uint8, "width", 200)
+    a = to_host(plan(to_dev(img)))
+    b = to_host(plan(to_dev(img)))
+    assert np.array_equal(a, b)
+    assert 1 <= plan.launches <= 4

@@ -1,0 +1,90 @@
+"""Build the sm_100a library in-tree: viprs_b200/_lib/libviprs_b200.so.
+
+nvcc compiles the device translation units for sm_100a only
+(-gencode arch=compute_100a,code=sm_100a) with --fmad=false, so that a
+multiply and an add are fused only where the source calls fma(); the host
+planning code is compiled with -ffp-contract=off for the same reason.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+OUT_DIR = os.path.join(HERE, "_lib")
+LIB = os.path.join(OUT_DIR, "libviprs_b200.so")
+OBJ_DIR = os.path.join(ROOT, "_build", "obj")
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
+
+CU_SOURCES = ["resample.cu", "affine.cu", "adjoint.cu", "batch.cu"]
+CPP_SOURCES = ["plan.cpp", "affine_plan.cpp", "capi.cpp", "batch_plan.cpp", "adjoint_plan.cpp"]
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _sources_present():
+    cu = [s for s in CU_SOURCES if os.path.exists(os.path.join(CSRC, s))]
+    cpp = [s for s in CPP_SOURCES if os.path.exists(os.path.join(CSRC, s))]
+    return cu, cpp
+
+
+def _stale(obj, deps):
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(force=False, verbose=False, jobs=8):
+    os.makedirs(OUT_DIR, exist_ok=True)
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    cu, cpp = _sources_present()
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".hpp", ".cuh", ".h"))]
+    headers.append(os.path.join(ROOT, "include", "viprs_b200.h"))
+    inc = ["-I", os.path.join(ROOT, "include"), "-I", CSRC]
+    cmds = []
+    objs = []
+    for s in cu:
+        src = os.path.join(CSRC, s)
+        obj = os.path.join(OBJ_DIR, s + ".o")
+        objs.append(obj)
+        if force or _stale(obj, [src] + headers):
+            cmds.append([NVCC, *ARCH, "-lineinfo", "-O3", "--fmad=false", "-std=c++17",
+                         "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", *inc,
+                         "-c", src, "-o", obj])
+    for s in cpp:
+        src = os.path.join(CSRC, s)
+        obj = os.path.join(OBJ_DIR, s + ".o")
+        objs.append(obj)
+        if force or _stale(obj, [src] + headers):
+            cmds.append(["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
+                         "-Wall", "-Wno-unused-function", *inc, "-I", os.path.join(CUDA_HOME, "include"),
+                         "-c", src, "-o", obj])
+    procs = []
+    for c in cmds:
+        if verbose:
+            print(" ".join(c))
+        procs.append(subprocess.Popen(c))
+        if len(procs) >= jobs:
+            _wait(procs)
+            procs = []
+    _wait(procs)
+    if force or cmds or not os.path.exists(LIB):
+        link = [NVCC, *ARCH, "-shared", "-cudart", "shared", "-o", LIB, *objs,
+                "-Xlinker", "-rpath," + os.path.join(CUDA_HOME, "lib64")]
+        if verbose:
+            print(" ".join(link))
+        subprocess.check_call(link)
+    return LIB
+
+
+def _wait(procs):
+    bad = [p.args for p in procs if p.wait() != 0]
+    if bad:
+        raise RuntimeError("compile failed: " + " ".join(bad[0]))
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

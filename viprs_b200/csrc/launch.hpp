@@ -1,0 +1,82 @@
+// launch.hpp -- host-visible argument blocks and launch wrappers of the
+// resample kernels.  Plain structs only, so that host C++ (capi.cpp) and
+// device code (resample.cu, affine.cu, batch.cu) share one definition.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace viprs {
+
+struct PlaneArg {
+    const uint8_t* data = nullptr;
+    int64_t x0 = 0, y0 = 0;
+    int32_t w = 0, h = 0;
+    int64_t pitch = 0;
+    int64_t total_bytes = 0;
+};
+
+struct OutPlaneArg {
+    uint8_t* data = nullptr;
+    int64_t x0 = 0, y0 = 0;
+    int32_t w = 0, h = 0;
+    int64_t pitch = 0;
+};
+
+// Sample formats (values of viprs_format).
+enum : int32_t { kU8 = 0, kU16 = 1, kF32 = 2 };
+
+// Box shrink of one or two axes (ShrinkH then ShrinkV when hv_order, ShrinkV
+// then ShrinkH otherwise); factor 1 on an axis means that op is absent.
+struct ShrinkArgs {
+    PlaneArg in;
+    OutPlaneArg out;
+    int32_t bands = 1;
+    int32_t fmt = kU8;
+    uint32_t fh = 1, fv = 1;
+    int32_t hv_order = 1;
+    int32_t premul_in = 0;     // apply Premultiply<U8> to every source sample read
+    int32_t unpremul_out = 0;  // apply Unpremultiply<U8> to every stored pixel
+    int32_t nx = 0;            // output columns per block (set by the launcher)
+};
+
+// Reduce accumulation modes.
+enum : int32_t {
+    kReduceFixed = 0,    // u8/u16: i16 x sample, int32 accumulator, (acc+2048)>>12
+    kReduceF32Simd = 1,  // f32: x86 AVX2 order of viprs (f64 products, lane sums)
+    kReduceF64Fma = 2    // sequential f64 fma, FromF64 rounding (ReduceOp, scalar paths)
+};
+
+struct ReduceArgs {
+    PlaneArg in;
+    OutPlaneArg out;
+    int32_t bands = 1;
+    int32_t fmt = kU8;
+    int32_t mode = kReduceFixed;
+    int32_t taps = 1;
+    const int32_t* starts = nullptr;  // absolute first tap per output column (H) or row (V)
+    const uint8_t* phases = nullptr;  // phase row (0..64) per output column / row
+    const void* coeffs = nullptr;     // 65 x taps, int16 (fixed) or double (float modes)
+    int32_t vector_len = 0;           // V f32: samples below this index use mul+add
+    int32_t premul_in = 0;
+    int32_t unpremul_out = 0;
+};
+
+struct PixelArgs {
+    PlaneArg in;
+    OutPlaneArg out;
+    int32_t bands = 1;
+    int32_t fmt = kU8;
+    int32_t op = 0;  // 0 copy, 1 premultiply, 2 unpremultiply
+};
+
+namespace launch {
+cudaError_t shrink2d(ShrinkArgs a, cudaStream_t s);
+cudaError_t reduce_h(const ReduceArgs& a, cudaStream_t s);
+cudaError_t reduce_v(const ReduceArgs& a, cudaStream_t s);
+cudaError_t pixel(const PixelArgs& a, cudaStream_t s);
+// Dynamic shared memory a shrink2d launch needs; 0 if the factor is too large.
+size_t shrink2d_smem_bytes(const ShrinkArgs& a, int32_t* nx);
+}  // namespace launch
+
+}  // namespace viprs

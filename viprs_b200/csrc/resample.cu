@@ -1,0 +1,506 @@
+// resample.cu -- sm_100a kernels for the box shrink and separable reduce ops
+// of viprs's resample path, with their launch wrappers.
+//
+//   shrink2d_kernel ..... ShrinkH / ShrinkV / Shrink (resample/shrinkh.rs:255-874,
+//                         shrinkv.rs:153-537, shrink.rs:179-293), premultiply fused
+//                         into the source read, unpremultiply into the store
+//   reduce_h_kernel ..... ReduceH (reduceh.rs:100-163; reduce_simd.rs:179-231,
+//                         2421-2538 for u8, 2544-2615 u16, 2621-2694 f32) and the
+//                         horizontal half of ReduceOp (reduce.rs:103-135)
+//   reduce_v_kernel ..... ReduceV (reducev.rs:99-162; reduce_simd.rs:2700-2888) and
+//                         the vertical half of ReduceOp (reduce.rs:137-170)
+//   pixel_kernel ........ Premultiply / Unpremultiply / ExtractArea copies
+//
+// Memory traffic: the shrink reads every source sample exactly once with
+// 16-byte loads into shared memory (coalesced across the block) and writes
+// each output once; it is HBM-bound.  The reduce kernels gather taps from
+// the (L2-resident) shrunk plane with coefficient tables in shared memory.
+#include <algorithm>
+#include <cstdio>
+
+#include "common.cuh"
+
+namespace viprs {
+namespace dev {
+
+constexpr int kShrinkThreads = 256;
+constexpr int kShrinkMaxItems = 4;  // (column, band) outputs per thread
+constexpr int kShrinkSegCap = 16384;  // target staging bytes per input row
+
+// ---------------------------------------------------------------- shrink
+
+// u8 rounding of ShrinkH (shrinkh.rs:323-397): factor 1 copies, 2 rounds up a
+// half, 5 with 1/3/4 bands divides exactly, anything else uses libvips's
+// multiplier (sum + f/2) * floor(2^32 / (256 f)) >> 24.
+__device__ __forceinline__ uint32_t shrinkh_round_u8(uint32_t sum, uint32_t f, int bands) {
+    if (f == 1) return sum;
+    if (f == 2) return (sum + 1) >> 1;
+    if (f == 5 && (bands == 1 || bands == 3 || bands == 4)) return (sum + 2) / 5;
+    const unsigned long long mult = (1ull << 32) / (256ull * f);
+    return static_cast<uint32_t>(((unsigned long long)(sum + f / 2) * mult) >> 24);
+}
+// u8 rounding of ShrinkV (shrinkv.rs:191-339): no factor-5 special case.
+__device__ __forceinline__ uint32_t shrinkv_round_u8(uint32_t sum, uint32_t f) {
+    if (f == 1) return sum;
+    if (f == 2) return (sum + 1) >> 1;
+    const unsigned long long mult = (uint32_t)((1ull << 32) / (256ull * f));
+    return static_cast<uint32_t>(((unsigned long long)(sum + f / 2) * mult) >> 24);
+}
+
+template <typename T>
+__device__ __forceinline__ double as_f64(T v) { return static_cast<double>(v); }
+
+// Copy `nelem` samples of local row `ly`, starting at local column `c0`, into
+// shared memory.  Interior segments use 16-byte loads of the aligned span
+// that covers them; the returned pointer is the first sample.  Segments that
+// leave the plane read per sample with clamped columns (edge replication).
+template <typename T>
+__device__ const T* stage_row(const Plane& in, int64_t ly, int64_t c0, int nin, int bands,
+                              uint8_t* raw) {
+    ly = ly < 0 ? 0 : (ly >= in.h ? in.h - 1 : ly);
+    const int nelem = nin * bands;
+    const uint8_t* row = in.data + ly * in.pitch;
+    if (c0 >= 0 && c0 + nin <= in.w) {
+        const int64_t s = (row - in.data) + c0 * bands * (int64_t)sizeof(T);
+        const int64_t e = s + (int64_t)nelem * sizeof(T);
+        const int64_t as = s & ~int64_t(15);
+        const int64_t ae = (e + 15) & ~int64_t(15);
+        if (ae <= in.total_bytes && (reinterpret_cast<uintptr_t>(in.data) & 15) == 0) {
+            const uint4* src = reinterpret_cast<const uint4*>(in.data + as);
+            uint4* dst = reinterpret_cast<uint4*>(raw);
+            const int nv = int((ae - as) >> 4);
+            for (int i = threadIdx.x; i < nv; i += blockDim.x) dst[i] = __ldg(src + i);
+            return reinterpret_cast<const T*>(raw + (s - as));
+        }
+        const T* srow = reinterpret_cast<const T*>(row) + c0 * bands;
+        T* d = reinterpret_cast<T*>(raw);
+        for (int i = threadIdx.x; i < nelem; i += blockDim.x) d[i] = srow[i];
+        return d;
+    }
+    const T* srow = reinterpret_cast<const T*>(row);
+    T* d = reinterpret_cast<T*>(raw);
+    for (int i = threadIdx.x; i < nelem; i += blockDim.x) {
+        int64_t col = c0 + i / bands;
+        col = col < 0 ? 0 : (col >= in.w ? in.w - 1 : col);
+        d[i] = srow[col * bands + (i % bands)];
+    }
+    return d;
+}
+
+// Premultiply the staged samples of a row in place (u8, alpha last).
+__device__ void premultiply_staged(uint8_t* seg, int nin, int bands) {
+    const int ab = bands - 1;
+    for (int p = threadIdx.x; p < nin; p += blockDim.x) {
+        const uint32_t a = seg[p * bands + ab];
+        for (int b = 0; b < ab; ++b) seg[p * bands + b] = (uint8_t)premultiply_u8(seg[p * bands + b], a);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void store_sample(uint8_t* row, int64_t idx, T v) {
+    reinterpret_cast<T*>(row)[idx] = v;
+}
+
+// One block: output row blockIdx.y, output columns [blockIdx.x*nx, +nx).
+template <typename T, bool HV>
+__global__ void __launch_bounds__(kShrinkThreads) shrink2d_kernel(ShrinkArgs a) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int bands = a.bands;
+    const uint32_t fh = a.fh, fv = a.fv;
+    const int nx = a.nx;
+    const int64_t oy = blockIdx.y;
+    const int64_t Y = a.out.y0 + oy;
+    const int64_t xb = (int64_t)blockIdx.x * nx;
+    const int64_t rem = a.out.w - xb;
+    const int ncols = (int)(rem < nx ? rem : nx);
+    if (ncols <= 0) return;
+    const int64_t X0 = a.out.x0 + xb;
+    const int64_t c0 = X0 * (int64_t)fh - a.in.x0;
+    const int nin = ncols * (int)fh;
+    const int nitems = ncols * bands;
+    const int seg_bytes = ((nin * bands * (int)sizeof(T)) + 15) / 16 * 16 + 32;
+    uint8_t* raw = smem;
+    uint8_t* extra = smem + seg_bytes;  // VH accumulators / output staging
+    const double inv_h = 1.0 / double(fh), inv_v = 1.0 / double(fv);
+
+    if (HV) {
+        uint32_t vacc_u[kShrinkMaxItems];
+        double vacc_d[kShrinkMaxItems];
+#pragma unroll
+        for (int s = 0; s < kShrinkMaxItems; ++s) { vacc_u[s] = 0; vacc_d[s] = 0.0; }
+        for (uint32_t k = 0; k < fv; ++k) {
+            const int64_t ly = Y * (int64_t)fv + k - a.in.y0;
+            const T* seg = stage_row<T>(a.in, ly, c0, nin, bands, raw);
+            __syncthreads();
+            if (sizeof(T) == 1 && a.premul_in) {
+                premultiply_staged(reinterpret_cast<uint8_t*>(const_cast<T*>(seg)), nin, bands);
+                __syncthreads();
+            }
+#pragma unroll
+            for (int s = 0; s < kShrinkMaxItems; ++s) {
+                const int item = threadIdx.x + s * kShrinkThreads;
+                if (item < nitems) {
+                    const int x = item / bands, b = item - (item / bands) * bands;
+                    const T* p = seg + (int64_t)x * fh * bands + b;
+                    if (sizeof(T) == 1) {
+                        uint32_t sum = 0;
+                        for (uint32_t j = 0; j < fh; ++j) sum += (uint32_t)p[j * bands];
+                        vacc_u[s] += shrinkh_round_u8(sum, fh, bands);
+                    } else {
+                        double hv;
+                        if (fh == 1) {
+                            hv = as_f64(p[0]);
+                        } else {
+                            double sum = 0.0;
+                            for (uint32_t j = 0; j < fh; ++j) sum += as_f64(p[j * bands]);
+                            hv = as_f64(shrink_from_f64<T>(sum * inv_h));
+                        }
+                        vacc_d[s] += hv;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        T outv[kShrinkMaxItems];
+#pragma unroll
+        for (int s = 0; s < kShrinkMaxItems; ++s) {
+            if (sizeof(T) == 1) outv[s] = (T)shrinkv_round_u8(vacc_u[s], fv);
+            else outv[s] = fv == 1 ? (T)vacc_d[s] : shrink_from_f64<T>(vacc_d[s] * inv_v);
+        }
+        uint8_t* orow = a.out.data + oy * a.out.pitch;
+        if (sizeof(T) == 1 && a.unpremul_out) {
+            uint8_t* ob = extra;
+#pragma unroll
+            for (int s = 0; s < kShrinkMaxItems; ++s) {
+                const int item = threadIdx.x + s * kShrinkThreads;
+                if (item < nitems) ob[item] = (uint8_t)outv[s];
+            }
+            __syncthreads();
+            const int ab = bands - 1;
+            for (int item = threadIdx.x; item < nitems; item += blockDim.x) {
+                const int x = item / bands, b = item - x * bands;
+                uint32_t v = ob[item];
+                if (b != ab) v = unpremultiply_u8(v, ob[x * bands + ab]);
+                orow[xb * bands + item] = (uint8_t)v;
+            }
+        } else {
+#pragma unroll
+            for (int s = 0; s < kShrinkMaxItems; ++s) {
+                const int item = threadIdx.x + s * kShrinkThreads;
+                if (item < nitems) store_sample<T>(orow, xb * bands + item, outv[s]);
+            }
+        }
+    } else {
+        // ShrinkV first (per input sample), then ShrinkH (resize.rs:216-224 order).
+        const int nelem = nin * bands;
+        uint32_t* acc_u = reinterpret_cast<uint32_t*>(extra);
+        double* acc_d = reinterpret_cast<double*>(extra);
+        for (int i = threadIdx.x; i < nelem; i += blockDim.x) {
+            if (sizeof(T) == 1) acc_u[i] = 0; else acc_d[i] = 0.0;
+        }
+        __syncthreads();
+        for (uint32_t k = 0; k < fv; ++k) {
+            const int64_t ly = Y * (int64_t)fv + k - a.in.y0;
+            const T* seg = stage_row<T>(a.in, ly, c0, nin, bands, raw);
+            __syncthreads();
+            if (sizeof(T) == 1 && a.premul_in) {
+                premultiply_staged(reinterpret_cast<uint8_t*>(const_cast<T*>(seg)), nin, bands);
+                __syncthreads();
+            }
+            for (int i = threadIdx.x; i < nelem; i += blockDim.x) {
+                if (sizeof(T) == 1) acc_u[i] += (uint32_t)seg[i]; else acc_d[i] += as_f64(seg[i]);
+            }
+            __syncthreads();
+        }
+        T* vvals = reinterpret_cast<T*>(raw);
+        for (int i = threadIdx.x; i < nelem; i += blockDim.x) {
+            if (sizeof(T) == 1) vvals[i] = (T)shrinkv_round_u8(acc_u[i], fv);
+            else vvals[i] = fv == 1 ? (T)acc_d[i] : shrink_from_f64<T>(acc_d[i] * inv_v);
+        }
+        __syncthreads();
+        uint8_t* orow = a.out.data + oy * a.out.pitch;
+        for (int item = threadIdx.x; item < nitems; item += blockDim.x) {
+            const int x = item / bands, b = item - x * bands;
+            const T* p = vvals + (int64_t)x * fh * bands + b;
+            T o;
+            if (sizeof(T) == 1) {
+                uint32_t sum = 0;
+                for (uint32_t j = 0; j < fh; ++j) sum += (uint32_t)p[j * bands];
+                o = (T)shrinkh_round_u8(sum, fh, bands);
+            } else if (fh == 1) {
+                o = p[0];
+            } else {
+                double sum = 0.0;
+                for (uint32_t j = 0; j < fh; ++j) sum += as_f64(p[j * bands]);
+                o = shrink_from_f64<T>(sum * inv_h);
+            }
+            store_sample<T>(orow, xb * bands + item, o);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- reduce
+
+template <typename T>
+__device__ __forceinline__ uint32_t load_premul(const Plane& p, int64_t lx, int64_t ly, int bands, int b,
+                                                bool premul) {
+    uint32_t v = (uint32_t)load_sample<T>(p, lx, ly, bands, b);
+    if (premul && b != bands - 1) v = premultiply_u8(v, (uint32_t)load_sample<T>(p, lx, ly, bands, bands - 1));
+    return v;
+}
+
+// Store one output row chunk; unpremultiply (u8) needs the pixel's alpha, which
+// another thread of the block computed: stage through shared memory.
+template <typename T>
+__device__ __forceinline__ void store_or_unpremul(uint8_t* orow, int64_t item, int nitems, T v, bool unpremul,
+                                                  int bands, uint8_t* stage) {
+    if (!unpremul) {
+        if (item < nitems) reinterpret_cast<T*>(orow)[item] = v;
+        return;
+    }
+    const int local = threadIdx.x;
+    if (item < nitems) stage[local] = (uint8_t)v;
+    __syncthreads();
+    if (item < nitems) {
+        const int b = int(item % bands);
+        uint32_t o = stage[local];
+        if (b != bands - 1) o = unpremultiply_u8(o, stage[local + (bands - 1 - b)]);
+        orow[item] = (uint8_t)o;
+    }
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) reduce_h_kernel(ReduceArgs a) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int taps = a.taps, bands = a.bands;
+    const int coef_bytes = 65 * taps * (MODE == kReduceFixed ? 2 : 8);
+    const bool coef_in_smem = coef_bytes <= 48 * 1024;
+    const uint8_t* coef = reinterpret_cast<const uint8_t*>(a.coeffs);
+    if (coef_in_smem) {
+        for (int i = threadIdx.x * 4; i < coef_bytes; i += blockDim.x * 4)
+            *reinterpret_cast<uint32_t*>(smem + i) = *reinterpret_cast<const uint32_t*>(coef + i);
+        __syncthreads();
+        coef = smem;
+    }
+    uint8_t* stage = smem + ((coef_in_smem ? coef_bytes : 0) + 15) / 16 * 16;
+    const int nitems = a.out.w * bands;
+    const int64_t item = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t oy = blockIdx.y;
+    const int64_t ly = a.out.y0 + oy - a.in.y0;
+    T outv = T(0);
+    if (item < nitems) {
+        const int x = int(item / bands), b = int(item - (item / bands) * bands);
+        const int64_t base = (int64_t)a.starts[x] - a.in.x0;
+        const int ph = a.phases[x];
+        if (MODE == kReduceFixed) {
+            const int16_t* c = reinterpret_cast<const int16_t*>(coef) + ph * taps;
+            int32_t acc = 0;
+            for (int t = 0; t < taps; ++t)
+                acc += (int32_t)c[t] * (int32_t)load_premul<T>(a.in, base + t, ly, bands, b, a.premul_in);
+            outv = from_fixed<T>(acc);
+        } else {
+            const double* c = reinterpret_cast<const double*>(coef) + ph * taps;
+            double acc = 0.0;
+            if (MODE == kReduceF32Simd) {
+                // reduce_h_f32_avx2_pixel: 4-tap products summed in lane order, fma tail
+                int t = 0;
+                for (; t + 4 <= taps; t += 4) {
+                    double lanes = as_f64(load_sample<T>(a.in, base + t, ly, bands, b)) * c[t];
+                    lanes = lanes + as_f64(load_sample<T>(a.in, base + t + 1, ly, bands, b)) * c[t + 1];
+                    lanes = lanes + as_f64(load_sample<T>(a.in, base + t + 2, ly, bands, b)) * c[t + 2];
+                    lanes = lanes + as_f64(load_sample<T>(a.in, base + t + 3, ly, bands, b)) * c[t + 3];
+                    acc = acc + lanes;
+                }
+                for (; t < taps; ++t) acc = fma(as_f64(load_sample<T>(a.in, base + t, ly, bands, b)), c[t], acc);
+            } else {
+                for (int t = 0; t < taps; ++t)
+                    acc = fma(as_f64(load_sample<T>(a.in, base + t, ly, bands, b)), c[t], acc);
+            }
+            outv = from_f64<T>(acc);
+        }
+    }
+    store_or_unpremul<T>(a.out.data + oy * a.out.pitch, item, nitems, outv, a.unpremul_out != 0, bands, stage);
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) reduce_v_kernel(ReduceArgs a) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int taps = a.taps, bands = a.bands;
+    const int coef_bytes = 65 * taps * (MODE == kReduceFixed ? 2 : 8);
+    const bool coef_in_smem = coef_bytes <= 48 * 1024;
+    const uint8_t* coef = reinterpret_cast<const uint8_t*>(a.coeffs);
+    if (coef_in_smem) {
+        for (int i = threadIdx.x * 4; i < coef_bytes; i += blockDim.x * 4)
+            *reinterpret_cast<uint32_t*>(smem + i) = *reinterpret_cast<const uint32_t*>(coef + i);
+        __syncthreads();
+        coef = smem;
+    }
+    uint8_t* stage = smem + ((coef_in_smem ? coef_bytes : 0) + 15) / 16 * 16;
+    const int nitems = a.out.w * bands;
+    const int64_t item = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t oy = blockIdx.y;
+    const int64_t base = (int64_t)a.starts[oy] - a.in.y0;
+    const int ph = a.phases[oy];
+    T outv = T(0);
+    if (item < nitems) {
+        const int x = int(item / bands), b = int(item - (item / bands) * bands);
+        const int64_t lx = a.out.x0 + x - a.in.x0;
+        if (MODE == kReduceFixed) {
+            const int16_t* c = reinterpret_cast<const int16_t*>(coef) + ph * taps;
+            int32_t acc = 0;
+            for (int t = 0; t < taps; ++t)
+                acc += (int32_t)c[t] * (int32_t)load_premul<T>(a.in, lx, base + t, bands, b, a.premul_in);
+            outv = from_fixed<T>(acc);
+        } else {
+            const double* c = reinterpret_cast<const double*>(coef) + ph * taps;
+            double acc = 0.0;
+            if (MODE == kReduceF32Simd && item < a.vector_len) {
+                for (int t = 0; t < taps; ++t) acc = acc + as_f64(load_sample<T>(a.in, lx, base + t, bands, b)) * c[t];
+            } else {
+                for (int t = 0; t < taps; ++t) acc = fma(as_f64(load_sample<T>(a.in, lx, base + t, bands, b)), c[t], acc);
+            }
+            outv = from_f64<T>(acc);
+        }
+    }
+    store_or_unpremul<T>(a.out.data + oy * a.out.pitch, item, nitems, outv, a.unpremul_out != 0, bands, stage);
+}
+
+// ---------------------------------------------------------------- pixel ops
+template <typename T>
+__global__ void pixel_kernel(PixelArgs a) {
+    const int64_t npx = (int64_t)a.out.w * a.out.h;
+    const int bands = a.bands;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npx; p += (int64_t)gridDim.x * blockDim.x) {
+        // the input plane of a pixel-local op or an ExtractArea starts at the
+        // pixel that maps to the output's first pixel: local coordinates agree
+        const int64_t y = p / a.out.w, x = p - y * a.out.w;
+        const T* src = reinterpret_cast<const T*>(a.in.data + y * a.in.pitch) + x * bands;
+        T* dst = reinterpret_cast<T*>(a.out.data + y * a.out.pitch) + x * bands;
+        if (a.op == 0 || bands < 2) {
+            for (int b = 0; b < bands; ++b) dst[b] = src[b];
+        } else if (sizeof(T) == 1) {
+            const uint32_t al = (uint32_t)src[bands - 1];
+            for (int b = 0; b < bands - 1; ++b)
+                dst[b] = (T)(a.op == 1 ? premultiply_u8((uint32_t)src[b], al) : unpremultiply_u8((uint32_t)src[b], al));
+            dst[bands - 1] = src[bands - 1];
+        } else if (sizeof(T) == 4 && a.op == 2) {
+            // Unpremultiply<F32> (structural/unpremultiply.rs:137-170)
+            const float al = (float)src[bands - 1];
+            for (int b = 0; b < bands - 1; ++b) {
+                float v = 0.0f;
+                if (al > 0.0f) {
+                    v = __fmul_rn((float)src[b], __frcp_rn(al));
+                    v = v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v);
+                }
+                dst[b] = (T)v;
+            }
+            dst[bands - 1] = src[bands - 1];
+        } else {
+            for (int b = 0; b < bands; ++b) dst[b] = src[b];
+        }
+    }
+}
+
+}  // namespace dev
+
+namespace launch {
+
+static int fmt_size(int32_t fmt) { return fmt == kU8 ? 1 : (fmt == kU16 ? 2 : 4); }
+
+size_t shrink2d_smem_bytes(const ShrinkArgs& a, int32_t* nx_out) {
+    const int es = fmt_size(a.fmt);
+    const int64_t per_col = int64_t(a.fh) * a.bands * es;
+    int64_t nx = std::max<int64_t>(1, dev::kShrinkSegCap / std::max<int64_t>(per_col, 1));
+    nx = std::min<int64_t>(nx, (int64_t)dev::kShrinkMaxItems * dev::kShrinkThreads / a.bands);
+    nx = std::max<int64_t>(1, std::min<int64_t>(nx, std::max(a.out.w, 1)));
+    const int64_t nin = nx * a.fh;
+    const int64_t seg = (nin * a.bands * es + 15) / 16 * 16 + 32;
+    int64_t extra;
+    if (a.hv_order) extra = a.unpremul_out ? (nx * a.bands + 15) / 16 * 16 : 0;
+    else extra = nin * a.bands * (es == 1 ? 4 : 8);
+    const int64_t total = seg + extra;
+    *nx_out = int32_t(nx);
+    if (total > 200 * 1024) return 0;
+    return size_t(total);
+}
+
+template <typename T>
+static cudaError_t shrink_typed(ShrinkArgs a, cudaStream_t s) {
+    int32_t nx;
+    const size_t smem = shrink2d_smem_bytes(a, &nx);
+    if (smem == 0) return cudaErrorInvalidValue;
+    a.nx = nx;
+    dim3 grid((unsigned)((a.out.w + nx - 1) / nx), (unsigned)a.out.h);
+    if (a.hv_order) {
+        auto k = dev::shrink2d_kernel<T, true>;
+        if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k<<<grid, dev::kShrinkThreads, smem, s>>>(a);
+    } else {
+        auto k = dev::shrink2d_kernel<T, false>;
+        if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k<<<grid, dev::kShrinkThreads, smem, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t shrink2d(ShrinkArgs a, cudaStream_t s) {
+    if (a.out.w <= 0 || a.out.h <= 0) return cudaSuccess;
+    switch (a.fmt) {
+    case kU8: return shrink_typed<uint8_t>(a, s);
+    case kU16: return shrink_typed<uint16_t>(a, s);
+    default: return shrink_typed<float>(a, s);
+    }
+}
+
+template <typename T, int MODE, bool H>
+static cudaError_t reduce_typed(const ReduceArgs& a, cudaStream_t s) {
+    const int coef_bytes = 65 * a.taps * (MODE == kReduceFixed ? 2 : 8);
+    size_t smem = (coef_bytes <= 48 * 1024 ? (coef_bytes + 15) / 16 * 16 : 0) + 256;
+    const int64_t nitems = (int64_t)a.out.w * a.bands;
+    dim3 grid((unsigned)((nitems + 255) / 256), (unsigned)a.out.h);
+    if (H) {
+        auto k = dev::reduce_h_kernel<T, MODE>;
+        if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k<<<grid, 256, smem, s>>>(a);
+    } else {
+        auto k = dev::reduce_v_kernel<T, MODE>;
+        if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k<<<grid, 256, smem, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+template <bool H>
+static cudaError_t reduce_any(const ReduceArgs& a, cudaStream_t s) {
+    if (a.out.w <= 0 || a.out.h <= 0) return cudaSuccess;
+    if (a.unpremul_out && (256 % a.bands) != 0) return cudaErrorInvalidValue;
+    switch (a.fmt) {
+    case kU8:
+        if (a.mode == kReduceFixed) return reduce_typed<uint8_t, kReduceFixed, H>(a, s);
+        return reduce_typed<uint8_t, kReduceF64Fma, H>(a, s);
+    case kU16:
+        if (a.mode == kReduceFixed) return reduce_typed<uint16_t, kReduceFixed, H>(a, s);
+        return reduce_typed<uint16_t, kReduceF64Fma, H>(a, s);
+    default:
+        if (a.mode == kReduceF32Simd) return reduce_typed<float, kReduceF32Simd, H>(a, s);
+        return reduce_typed<float, kReduceF64Fma, H>(a, s);
+    }
+}
+
+cudaError_t reduce_h(const ReduceArgs& a, cudaStream_t s) { return reduce_any<true>(a, s); }
+cudaError_t reduce_v(const ReduceArgs& a, cudaStream_t s) { return reduce_any<false>(a, s); }
+
+cudaError_t pixel(const PixelArgs& a, cudaStream_t s) {
+    const int64_t npx = (int64_t)a.out.w * a.out.h;
+    if (npx <= 0) return cudaSuccess;
+    const unsigned grid = (unsigned)std::min<int64_t>((npx + 255) / 256, 148 * 16);
+    switch (a.fmt) {
+    case kU8: dev::pixel_kernel<uint8_t><<<grid, 256, 0, s>>>(a); break;
+    case kU16: dev::pixel_kernel<uint16_t><<<grid, 256, 0, s>>>(a); break;
+    default: dev::pixel_kernel<float><<<grid, 256, 0, s>>>(a); break;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace launch
+}  // namespace viprs
