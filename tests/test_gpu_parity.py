@@ -139,21 +139,21 @@ def test_thumbnail(oracle, case):
         assert_same(got, exp, np.uint8)
 
 
-def test_thumbnail_with_affine_tail(oracle):
-    # find sizes whose plan ends in the bicubic affine correction
-    rng = np.random.default_rng(5)
-    found = 0
-    for w in range(300, 2000, 37):
-        h = int(w * 0.77) + 3
-        plan, _, _ = oracle.thumbnail_plan(w, h, 4, "fitbox", 256, 256, allow_shrink_hint=False)
-        if any(n["kind"] == "affine" for n in plan):
-            img = smooth_image(rng, h, w, 4)
-            got = to_host(api.thumbnail(to_dev(img), "fitbox", 256, 256))
-            assert_same(got, oracle.thumbnail(img, "fitbox", 256, 256, threads=4), np.uint8)
-            found += 1
-            if found >= 3:
-                break
-    assert found > 0
+AFFINE_TAIL_CASES = [(731, 389, 640, 480), (1200, 700, 1500, 100), (600, 900, 640, 480),
+                     (300, 200, 97, 211), (50, 41, 97, 211), (300, 200, 640, 480)]
+
+
+@pytest.mark.parametrize("case", AFFINE_TAIL_CASES)
+@pytest.mark.parametrize("bands", [3, 4])
+def test_thumbnail_with_affine_tail(oracle, case, bands):
+    # ForceExact plans whose geometry needs the bicubic affine correction
+    # (Copy extend; ThinStrip tiles above 512 px, SmallTile below)
+    w, h, tw, th = case
+    plan, _, _ = oracle.thumbnail_plan(w, h, bands, "force", tw, th, allow_shrink_hint=False)
+    assert any(n["kind"] == "affine" for n in plan)
+    img = smooth_image(np.random.default_rng(w + h + bands), h, w, bands)
+    got = to_host(api.thumbnail(to_dev(img), "force", tw, th))
+    assert_same(got, oracle.thumbnail(img, "force", tw, th, threads=4), np.uint8)
 
 
 @pytest.mark.parametrize("fmt", [np.uint8, np.float32])

@@ -38,6 +38,15 @@ struct ShrinkArgs {
     int32_t premul_in = 0;     // apply Premultiply<U8> to every source sample read
     int32_t unpremul_out = 0;  // apply Unpremultiply<U8> to every stored pixel
     int32_t nx = 0;            // output columns per block (set by the launcher)
+    int32_t col_lo = 0;        // local output columns [col_lo, col_hi) handled
+    int32_t col_hi = -1;       //   (-1: all)
+    // rounding constants of ShrinkH / ShrinkV for u8 (host-computed)
+    int32_t hmode = 0, vmode = 0;       // 0 copy, 1 factor 2, 2 exact /5, 3 multiplier
+    uint64_t hmult = 0, vmult = 0;
+    // bulk-copy pipeline of the interior columns (u8, ShrinkH then ShrinkV)
+    int32_t chunks = 0, nxf = 0, stages = 0;
+    uint32_t stage_bytes = 0;
+    int32_t* err = nullptr;    // device error word (timeout), may be null
 };
 
 // Reduce accumulation modes.

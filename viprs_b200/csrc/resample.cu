@@ -19,6 +19,8 @@
 #include <cstdio>
 
 #include "common.cuh"
+#include "tma.cuh"
+#include "viprs_b200.h"
 
 namespace viprs {
 namespace dev {
@@ -45,6 +47,17 @@ __device__ __forceinline__ uint32_t shrinkv_round_u8(uint32_t sum, uint32_t f) {
     if (f == 2) return (sum + 1) >> 1;
     const unsigned long long mult = (uint32_t)((1ull << 32) / (256ull * f));
     return static_cast<uint32_t>(((unsigned long long)(sum + f / 2) * mult) >> 24);
+}
+
+// The same rounding with host-computed constants (mode 0 copy, 1 factor 2,
+// 2 exact division by 5, 3 multiplier), avoiding 64-bit division on the device.
+__device__ __forceinline__ uint32_t round_mode_u8(uint32_t sum, int mode, uint32_t f, uint64_t mult) {
+    switch (mode) {
+    case 0: return sum;
+    case 1: return (sum + 1) >> 1;
+    case 2: return (sum + 2) / 5;
+    default: return (uint32_t)(((unsigned long long)(sum + f / 2) * mult) >> 24);
+    }
 }
 
 template <typename T>
@@ -110,8 +123,8 @@ __global__ void __launch_bounds__(kShrinkThreads) shrink2d_kernel(ShrinkArgs a) 
     const int nx = a.nx;
     const int64_t oy = blockIdx.y;
     const int64_t Y = a.out.y0 + oy;
-    const int64_t xb = (int64_t)blockIdx.x * nx;
-    const int64_t rem = a.out.w - xb;
+    const int64_t xb = a.col_lo + (int64_t)blockIdx.x * nx;
+    const int64_t rem = a.col_hi - xb;
     const int ncols = (int)(rem < nx ? rem : nx);
     if (ncols <= 0) return;
     const int64_t X0 = a.out.x0 + xb;
@@ -145,7 +158,7 @@ __global__ void __launch_bounds__(kShrinkThreads) shrink2d_kernel(ShrinkArgs a) 
                     if (sizeof(T) == 1) {
                         uint32_t sum = 0;
                         for (uint32_t j = 0; j < fh; ++j) sum += (uint32_t)p[j * bands];
-                        vacc_u[s] += shrinkh_round_u8(sum, fh, bands);
+                        vacc_u[s] += round_mode_u8(sum, a.hmode, fh, a.hmult);
                     } else {
                         double hv;
                         if (fh == 1) {
@@ -164,7 +177,7 @@ __global__ void __launch_bounds__(kShrinkThreads) shrink2d_kernel(ShrinkArgs a) 
         T outv[kShrinkMaxItems];
 #pragma unroll
         for (int s = 0; s < kShrinkMaxItems; ++s) {
-            if (sizeof(T) == 1) outv[s] = (T)shrinkv_round_u8(vacc_u[s], fv);
+            if (sizeof(T) == 1) outv[s] = (T)round_mode_u8(vacc_u[s], a.vmode, fv, a.vmult);
             else outv[s] = fv == 1 ? (T)vacc_d[s] : shrink_from_f64<T>(vacc_d[s] * inv_v);
         }
         uint8_t* orow = a.out.data + oy * a.out.pitch;
@@ -214,7 +227,7 @@ __global__ void __launch_bounds__(kShrinkThreads) shrink2d_kernel(ShrinkArgs a) 
         }
         T* vvals = reinterpret_cast<T*>(raw);
         for (int i = threadIdx.x; i < nelem; i += blockDim.x) {
-            if (sizeof(T) == 1) vvals[i] = (T)shrinkv_round_u8(acc_u[i], fv);
+            if (sizeof(T) == 1) vvals[i] = (T)round_mode_u8(acc_u[i], a.vmode, fv, a.vmult);
             else vvals[i] = fv == 1 ? (T)acc_d[i] : shrink_from_f64<T>(acc_d[i] * inv_v);
         }
         __syncthreads();
@@ -226,7 +239,7 @@ __global__ void __launch_bounds__(kShrinkThreads) shrink2d_kernel(ShrinkArgs a) 
             if (sizeof(T) == 1) {
                 uint32_t sum = 0;
                 for (uint32_t j = 0; j < fh; ++j) sum += (uint32_t)p[j * bands];
-                o = (T)shrinkh_round_u8(sum, fh, bands);
+                o = (T)round_mode_u8(sum, a.hmode, fh, a.hmult);
             } else if (fh == 1) {
                 o = p[0];
             } else {
@@ -236,6 +249,144 @@ __global__ void __launch_bounds__(kShrinkThreads) shrink2d_kernel(ShrinkArgs a) 
             }
             store_sample<T>(orow, xb * bands + item, o);
         }
+    }
+}
+
+// ShrinkH then ShrinkV over u8 for the interior output columns, whose source
+// spans lie inside the plane: each source row segment of an (output row,
+// column chunk) item is fetched by one thread with a TMA bulk copy into a
+// ring of `stages` shared-memory buffers, so several rows are in flight while
+// the block sums the current one.  Blocks walk items grid-stride; the ring
+// runs across item boundaries.  Every source byte is read once.
+__global__ void __launch_bounds__(kShrinkThreads) shrink_hv_u8_tma(ShrinkArgs a) {
+    extern __shared__ __align__(128) uint8_t smem_tma[];
+    uint8_t* smem = smem_tma;
+    const int S = a.stages;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
+    volatile int32_t* flag = reinterpret_cast<volatile int32_t*>(smem + 64);
+    uint8_t* bufs = smem + 128;
+    uint8_t* ostage = bufs + (size_t)S * a.stage_bytes;
+    const int bands = a.bands;
+    const uint32_t fh = a.fh, fv = a.fv;
+    const int64_t n_items = (int64_t)a.out.h * a.chunks;
+    const int64_t G = gridDim.x;
+    if ((int64_t)blockIdx.x >= n_items) return;
+    const int64_t n_my = (n_items - 1 - blockIdx.x) / G + 1;
+    const int64_t total = n_my * fv;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < S; ++i) mbar_init(&bars[i], 1);
+        *flag = 0;
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    // geometry of step t (item, source row)
+    auto geom = [&](int64_t t, int64_t* oy, int* lx0, int* ncols, int64_t* as, uint32_t* bytes, int* lead) {
+        const int64_t item = blockIdx.x + (t / fv) * G;
+        const int64_t k = t % fv;
+        *oy = item / a.chunks;
+        const int c = int(item - *oy * a.chunks);
+        *lx0 = a.col_lo + c * a.nxf;
+        *ncols = min(a.nxf, a.col_hi - *lx0);
+        const int64_t X0 = a.out.x0 + *lx0, Y = a.out.y0 + *oy;
+        int64_t ly = Y * (int64_t)fv + k - a.in.y0;
+        ly = ly < 0 ? 0 : (ly >= a.in.h ? a.in.h - 1 : ly);
+        const int64_t s = ly * a.in.pitch + (X0 * (int64_t)fh - a.in.x0) * bands;
+        const int64_t e = s + (int64_t)(*ncols) * fh * bands;
+        *as = s & ~int64_t(15);
+        *bytes = uint32_t(((e + 15) & ~int64_t(15)) - *as);
+        *lead = int(s - *as);
+    };
+    auto issue = [&](int64_t t) {
+        int64_t oy, as; int lx0, ncols, lead; uint32_t bytes;
+        geom(t, &oy, &lx0, &ncols, &as, &bytes, &lead);
+        const int st = int(t % S);
+        mbar_arrive_expect_tx(&bars[st], bytes);
+        bulk_load(bufs + (size_t)st * a.stage_bytes, a.in.data + as, bytes, &bars[st]);
+    };
+    const int64_t first = total < S ? total : (int64_t)S;
+    if (threadIdx.x == 0)
+        for (int64_t t = 0; t < first; ++t) issue(t);
+
+    uint32_t vacc[kShrinkMaxItems];
+    int off[kShrinkMaxItems];
+    int64_t issued = first;
+    int64_t t_fail = -1;
+    for (int64_t t = 0; t < total; ++t) {
+        const int st = int(t % S);
+        const uint32_t parity = uint32_t((t / S) & 1);
+        if (threadIdx.x == 0 && !mbar_wait(&bars[st], parity)) *flag = 1;
+        __syncthreads();
+        if (*flag) { t_fail = t; break; }
+        int64_t oy, as; int lx0, ncols, lead; uint32_t bytes;
+        geom(t, &oy, &lx0, &ncols, &as, &bytes, &lead);
+        const int64_t k = t % fv;
+        const int nitems = ncols * bands;
+        if (k == 0) {
+#pragma unroll
+            for (int q = 0; q < kShrinkMaxItems; ++q) {
+                vacc[q] = 0;
+                const int item = threadIdx.x + q * kShrinkThreads;
+                const int x = item / bands;
+                off[q] = x * int(fh) * bands + (item - x * bands);
+            }
+        }
+        const uint8_t* row = bufs + (size_t)st * a.stage_bytes + lead;
+        if (a.premul_in) {
+            premultiply_staged(const_cast<uint8_t*>(row), ncols * int(fh), bands);
+            __syncthreads();
+        }
+#pragma unroll
+        for (int q = 0; q < kShrinkMaxItems; ++q) {
+            const int item = threadIdx.x + q * kShrinkThreads;
+            if (item < nitems) {
+                const uint8_t* p = row + off[q];
+                uint32_t sum = 0;
+#pragma unroll 4
+                for (uint32_t j = 0; j < fh; ++j) sum += p[j * bands];
+                vacc[q] += round_mode_u8(sum, a.hmode, fh, a.hmult);
+            }
+        }
+        __syncthreads();  // all reads of this buffer are done
+        if (threadIdx.x == 0 && issued < total) {
+            fence_proxy_async_smem();
+            issue(issued);
+            ++issued;
+        }
+        if (k == fv - 1) {
+            uint8_t* orow = a.out.data + oy * a.out.pitch + (int64_t)lx0 * bands;
+            if (a.unpremul_out) {
+#pragma unroll
+                for (int q = 0; q < kShrinkMaxItems; ++q) {
+                    const int item = threadIdx.x + q * kShrinkThreads;
+                    if (item < nitems) ostage[item] = (uint8_t)round_mode_u8(vacc[q], a.vmode, fv, a.vmult);
+                }
+                __syncthreads();
+                const int ab = bands - 1;
+                for (int item = threadIdx.x; item < nitems; item += blockDim.x) {
+                    const int x = item / bands, b = item - x * bands;
+                    uint32_t v = ostage[item];
+                    if (b != ab) v = unpremultiply_u8(v, ostage[x * bands + ab]);
+                    orow[item] = (uint8_t)v;
+                }
+                __syncthreads();
+            } else {
+#pragma unroll
+                for (int q = 0; q < kShrinkMaxItems; ++q) {
+                    const int item = threadIdx.x + q * kShrinkThreads;
+                    if (item < nitems) orow[item] = (uint8_t)round_mode_u8(vacc[q], a.vmode, fv, a.vmult);
+                }
+            }
+        }
+    }
+    if (t_fail >= 0) {
+        // a copy never completed: record it, then wait (bounded) for the copies
+        // this block still has in flight before its shared memory goes away
+        if (threadIdx.x == 0) {
+            if (a.err) atomicExch(a.err, VIPRS_ERR_TIMEOUT);
+            for (int64_t tt = t_fail + 1; tt < issued; ++tt) mbar_wait(&bars[tt % S], uint32_t((tt / S) & 1));
+        }
+        __syncthreads();
     }
 }
 
@@ -426,11 +577,13 @@ size_t shrink2d_smem_bytes(const ShrinkArgs& a, int32_t* nx_out) {
 
 template <typename T>
 static cudaError_t shrink_typed(ShrinkArgs a, cudaStream_t s) {
+    if (a.col_hi < 0) { a.col_lo = 0; a.col_hi = a.out.w; }
+    if (a.col_hi <= a.col_lo) return cudaSuccess;
     int32_t nx;
     const size_t smem = shrink2d_smem_bytes(a, &nx);
     if (smem == 0) return cudaErrorInvalidValue;
     a.nx = nx;
-    dim3 grid((unsigned)((a.out.w + nx - 1) / nx), (unsigned)a.out.h);
+    dim3 grid((unsigned)((a.col_hi - a.col_lo + nx - 1) / nx), (unsigned)a.out.h);
     if (a.hv_order) {
         auto k = dev::shrink2d_kernel<T, true>;
         if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -443,8 +596,93 @@ static cudaError_t shrink_typed(ShrinkArgs a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+static int g_sm_count = 0;
+
+static int sm_count() {
+    if (g_sm_count == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
+        if (g_sm_count <= 0) g_sm_count = 148;
+    }
+    return g_sm_count;
+}
+
+static void round_consts(uint32_t f, int bands, bool horizontal, int32_t* mode, uint64_t* mult) {
+    *mult = (1ull << 32) / (256ull * f);
+    if (f == 1) *mode = 0;
+    else if (f == 2) *mode = 1;
+    else if (horizontal && f == 5 && (bands == 1 || bands == 3 || bands == 4)) *mode = 2;
+    else *mode = 3;
+    if (!horizontal) *mult = (uint32_t)*mult;
+}
+
+// Interior output columns [lo, hi): their source span lies inside the plane
+// and its 16-byte aligned cover lies inside the buffer for every row.
+static void interior_columns(const ShrinkArgs& a, int32_t* lo, int32_t* hi) {
+    const int64_t fh = a.fh;
+    int64_t xlo = (a.in.x0 + fh - 1) / fh;  // ceil for non-negative x0
+    if (a.in.x0 < 0) xlo = -((-a.in.x0) / fh);
+    int64_t xhi = (a.in.x0 + a.in.w) >= 0 ? (a.in.x0 + a.in.w) / fh : -1;
+    int64_t l = std::max<int64_t>(xlo - a.out.x0, 0), h = std::min<int64_t>(xhi - a.out.x0, a.out.w);
+    // the last source row's aligned span must stay inside the buffer
+    while (h > l) {
+        const int64_t ly = a.in.h - 1;
+        const int64_t e = ly * a.in.pitch + ((a.out.x0 + h) * fh - a.in.x0) * a.bands;
+        if (((e + 15) & ~int64_t(15)) <= a.in.total_bytes) break;
+        --h;
+    }
+    *lo = int32_t(l);
+    *hi = int32_t(std::max(l, h));
+}
+
 cudaError_t shrink2d(ShrinkArgs a, cudaStream_t s) {
     if (a.out.w <= 0 || a.out.h <= 0) return cudaSuccess;
+    round_consts(a.fh, a.bands, true, &a.hmode, &a.hmult);
+    round_consts(a.fv, a.bands, false, &a.vmode, &a.vmult);
+    if (a.fmt == kU8 && a.hv_order && (reinterpret_cast<uintptr_t>(a.in.data) & 15) == 0) {
+        int32_t lo, hi;
+        interior_columns(a, &lo, &hi);
+        const int64_t iw = hi - lo;
+        const int64_t per_col = int64_t(a.fh) * a.bands;
+        if (iw > 0 && per_col <= 16384) {
+            // columns per item: about 4 KB of source per row, at most 1024 outputs per block
+            const int64_t target_cols = std::max<int64_t>(1, 4096 / per_col);
+            int64_t chunks = std::max<int64_t>(1, (iw + target_cols - 1) / target_cols);
+            int64_t nxf = (iw + chunks - 1) / chunks;
+            nxf = std::min<int64_t>(nxf, (int64_t)dev::kShrinkMaxItems * dev::kShrinkThreads / a.bands);
+            chunks = (iw + nxf - 1) / nxf;
+            const int stages = 4;
+            const uint32_t stage_bytes = uint32_t((nxf * per_col + 32 + 127) / 128 * 128);
+            const size_t smem = 128 + size_t(stages) * stage_bytes + size_t(nxf * a.bands + 16);
+            if (smem <= 200 * 1024) {
+                ShrinkArgs f = a;
+                f.col_lo = lo; f.col_hi = hi; f.nxf = int32_t(nxf); f.chunks = int32_t(chunks);
+                f.stages = stages; f.stage_bytes = stage_bytes;
+                auto k = dev::shrink_hv_u8_tma;
+                cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                int per_sm = 0;
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, dev::kShrinkThreads, smem);
+                const int64_t items = int64_t(a.out.h) * chunks;
+                const int64_t grid = std::min<int64_t>(items, int64_t(std::max(per_sm, 1)) * sm_count());
+                k<<<(unsigned)grid, dev::kShrinkThreads, smem, s>>>(f);
+                cudaError_t e = cudaGetLastError();
+                if (e != cudaSuccess) return e;
+                // the edge columns whose source spans leave the plane
+                ShrinkArgs g = a;
+                if (lo > 0) {
+                    g.col_lo = 0; g.col_hi = lo;
+                    e = shrink_typed<uint8_t>(g, s);
+                    if (e != cudaSuccess) return e;
+                }
+                if (hi < a.out.w) {
+                    g.col_lo = hi; g.col_hi = a.out.w;
+                    e = shrink_typed<uint8_t>(g, s);
+                }
+                return e;
+            }
+        }
+    }
     switch (a.fmt) {
     case kU8: return shrink_typed<uint8_t>(a, s);
     case kU16: return shrink_typed<uint16_t>(a, s);
