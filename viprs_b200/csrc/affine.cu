@@ -64,10 +64,47 @@ __device__ double kernel_w(int k, double x) {
     }
 }
 
+__device__ __forceinline__ int64_t tile_origin(int64_t v, int64_t off, int64_t t) {
+    const int64_t d = v - off;
+    const int64_t q = d >= 0 ? d / t : -((-d + t - 1) / t);
+    return off + q * t;
+}
+
 template <typename T>
 struct AffineCtx {
     const AffineArgs& a;
+    // the scheduler tile's input region (Affine::required_input_region clipped
+    // to the source bounds): viprs samples outside it read the fill value
+    int64_t rx0 = 0, rx1 = -1, ry0 = 0, ry1 = -1;
     __device__ AffineCtx(const AffineArgs& args) : a(args) {}
+
+    __device__ void set_tile(int64_t X, int64_t Y) {
+        rx0 = 0; rx1 = (int64_t)a.src_w - 1; ry0 = 0; ry1 = (int64_t)a.src_h - 1;
+        if (X < a.tile_off_x || X >= a.tile_off_x + (int64_t)a.final_w || Y < a.tile_off_y ||
+            Y >= a.tile_off_y + (int64_t)a.final_h)
+            return;  // outside the tile grid (a downstream halo): image bounds only
+        const int64_t X0 = tile_origin(X, a.tile_off_x, a.tile_w), Y0 = tile_origin(Y, a.tile_off_y, a.tile_h);
+        const int64_t TW = min((int64_t)a.tile_w, a.tile_off_x + (int64_t)a.final_w - X0);
+        const int64_t TH = min((int64_t)a.tile_h, a.tile_off_y + (int64_t)a.final_h - Y0);
+        const double* m = a.m;
+        const double xs[2] = {(double)X0, (double)X0 + (double)(TW - 1)};
+        const double ys[2] = {(double)Y0, (double)Y0 + (double)(TH - 1)};
+        double mnx = 0, mxx = 0, mny = 0, mxy = 0;
+        for (int i = 0; i < 4; ++i) {
+            const double x = xs[i & 1], y = ys[i >> 1];
+            const double cx = fma(m[1], y, m[0] * x) + a.tx, cy = fma(m[3], y, m[2] * x) + a.ty;
+            if (i == 0) { mnx = mxx = cx; mny = mxy = cy; }
+            else { mnx = fmin(mnx, cx); mxx = fmax(mxx, cx); mny = fmin(mny, cy); mxy = fmax(mxy, cy); }
+        }
+        int lp = 1, rp = 2;
+        if (a.kernel == 0) { lp = 0; rp = 0; }
+        else if (a.kernel == 1) { lp = 0; rp = 1; }
+        else if (a.kernel == 9 || a.kernel == 4) { lp = 2; rp = 3; }
+        const int64_t x0 = trunc_i64(floor(mnx)) - lp, x1 = trunc_i64(floor(mxx)) + rp;
+        const int64_t y0 = trunc_i64(floor(mny)) - lp, y1 = trunc_i64(floor(mxy)) + rp;
+        rx0 = max(x0, (int64_t)0); rx1 = min(x1, (int64_t)a.src_w - 1);
+        ry0 = max(y0, (int64_t)0); ry1 = min(y1, (int64_t)a.src_h - 1);
+    }
 
     __device__ double fill() const {
         if (a.extend == 1) return sizeof(T) == 4 ? 1.0 : (sizeof(T) == 2 ? 65535.0 : 255.0);
@@ -94,6 +131,7 @@ struct AffineCtx {
     __device__ double sb(int64_t ix, int64_t iy, int band) const {
         int64_t rx, ry;
         if (!resolve(ix, a.src_w, &rx) || !resolve(iy, a.src_h, &ry)) return fill();
+        if (rx < rx0 || rx > rx1 || ry < ry0 || ry > ry1) return fill();
         return (double)load_sample<T>(a.in, rx - a.in.x0, ry - a.in.y0, a.bands, band);
     }
     __device__ double sbp(int64_t ix, int64_t iy, int band, int ab, double amax) const {
@@ -170,7 +208,8 @@ struct AffineCtx {
         if (a.kernel == 0) {
             const int64_t ix = trunc_i64(x), iy = trunc_i64(y);
             int64_t rx, ry;
-            if (!resolve(ix, a.src_w, &rx) || !resolve(iy, a.src_h, &ry)) {
+            if (!resolve(ix, a.src_w, &rx) || !resolve(iy, a.src_h, &ry) || rx < rx0 || rx > rx1 || ry < ry0 ||
+                ry > ry1) {
                 for (int b = 0; b < bands; ++b) out[b] = fill();
                 return;
             }
@@ -191,12 +230,6 @@ __device__ __forceinline__ T store_round(double v, bool u8_round_first) {
     return from_f64<T>(v);
 }
 
-__device__ __forceinline__ int64_t tile_origin(int64_t v, int64_t off, int64_t t) {
-    const int64_t d = v - off;
-    const int64_t q = d >= 0 ? d / t : -((-d + t - 1) / t);
-    return off + q * t;
-}
-
 template <typename T>
 __global__ void __launch_bounds__(256) affine_kernel(AffineArgs a) {
     const int64_t npx = (int64_t)a.out.w * a.out.h;
@@ -206,6 +239,7 @@ __global__ void __launch_bounds__(256) affine_kernel(AffineArgs a) {
     const int64_t X = a.out.x0 + lx, Y = a.out.y0 + ly;
     const int bands = a.bands;
     AffineCtx<T> c(a);
+    c.set_tile(X, Y);
     double v[8];
     bool u8_round_first = false;
     const double* m = a.m;

@@ -26,6 +26,7 @@ struct AffineArgs {
     uint32_t total_w = 0, total_h = 0;  // Affine output_w / output_h
     uint32_t tile_w = 128, tile_h = 128;
     int64_t tile_off_x = 0, tile_off_y = 0;  // tile grid origin in affine output coords
+    uint32_t final_w = 0, final_h = 0;       // pipeline output the tile grid covers
     int32_t fast = 0;        // axis-aligned fast path: 0 none, 1 nearest, 2 bilinear, 3 bicubic
     int32_t separable = 0;   // b == c == 0: positions from per-axis tables
     const double* xs = nullptr;  // per output column x_in (separable general path)

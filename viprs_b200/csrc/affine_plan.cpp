@@ -85,6 +85,7 @@ int affine_stage_setup(const PlanNode& n, uint32_t in_w, uint32_t in_h, uint32_t
     if (n.ew > 0 && n.eh > 0) { tw = n.ew; th = n.eh; }  // explicit grid from the caller
     a->tile_w = std::max(tw, 1u); a->tile_h = std::max(th, 1u);
     a->tile_off_x = tile_off_x; a->tile_off_y = tile_off_y;
+    a->final_w = final_w; a->final_h = final_h;
     a->fast = 0;
     if (std::fabs(n.m[1]) <= DBL_EPSILON && std::fabs(n.m[2]) <= DBL_EPSILON) {
         if (n.kernel == Kernel::Nearest) a->fast = 1;

@@ -38,7 +38,7 @@ int32_t cuda_status(cudaError_t e) {
     return VIPRS_ERR_CUDA;
 }
 
-enum class StageType { Shrink, ReduceH, ReduceV, Pixel, Affine };
+enum class StageType { Shrink, ReduceH, ReduceV, Reduce2D, Pixel, Affine };
 
 struct Stage {
     StageType type;
@@ -48,8 +48,10 @@ struct Stage {
     ReduceArgs rd;
     PixelArgs px;
     AffineArgs af;
+    Reduce2DArgs r2;
     // offsets of this stage's tables inside the plan table buffer
     size_t starts_off = 0, phases_off = 0, coeffs_off = 0;
+    size_t starts2_off = 0, phases2_off = 0, coeffs2_off = 0;
 };
 
 struct PlaneInfo {
@@ -187,6 +189,72 @@ int add_reduce_stage(viprs_plan* p, const ReduceKernel& rk, bool horizontal, int
     return VIPRS_OK;
 }
 
+int mode_for(int32_t fmt, bool horizontal, uint32_t bands);
+
+// ReduceH and ReduceV fused into one launch (either order).  `first` produces
+// the mid region `mid`; `second` produces `outr`.  Returns false (and adds
+// nothing) when the tile does not fit in shared memory.
+bool add_reduce2d_stage(viprs_plan* p, const ReduceKernel& first, const ReduceKernel& second, bool hfirst,
+                        int mode_first, int mode_second, const Region& mid, const Region& outr, int in_plane,
+                        int out_plane, bool incremental_h) {
+    Stage st;
+    st.type = StageType::Reduce2D;
+    st.in_plane = in_plane;
+    st.out_plane = out_plane;
+    const ReduceKernel& rh = hfirst ? first : second;
+    const ReduceKernel& rv = hfirst ? second : first;
+    // H tables run over the columns of the H op's output, V tables over the rows of the V op's output
+    const Region& hreg = hfirst ? mid : outr;
+    const Region& vreg = hfirst ? outr : mid;
+    std::vector<int32_t> sh, sv;
+    std::vector<uint8_t> ph, pv;
+    reduce_tables(rh, hreg.x, hreg.w, incremental_h, &sh, &ph);
+    reduce_tables(rv, vreg.y, vreg.h, false, &sv, &pv);
+    Reduce2DArgs& a = st.r2;
+    a.bands = int32_t(p->bands);
+    a.fmt = p->fmt;
+    a.hfirst = hfirst ? 1 : 0;
+    a.mx0 = mid.x; a.my0 = mid.y; a.mw = int32_t(mid.w); a.mh = int32_t(mid.h);
+    a.taps_h = rh.taps; a.taps_v = rv.taps;
+    a.mode_h = hfirst ? mode_first : mode_second;
+    a.mode_v = hfirst ? mode_second : mode_first;
+    a.vector_len = int32_t((hfirst ? outr.w : mid.w) * p->bands / 4 * 4);
+    const double maxv = p->fmt == kU8 ? 255.0 : 65535.0;
+    if (a.mode_h == kReduceFixed && double(rh.max_abs_i16_sum()) * maxv >= 2147483647.0) return false;
+    if (a.mode_v == kReduceFixed && double(rv.max_abs_i16_sum()) * maxv >= 2147483647.0) return false;
+    // tile shape: 16 output rows x 64 columns, shrunk until the mid tile fits
+    a.tile_h = 16; a.tile_w = 64;
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        const std::vector<int32_t>& st2 = hfirst ? sv : sh;
+        const int64_t n2 = hfirst ? outr.h : outr.w;
+        const int64_t tile = hfirst ? a.tile_h : a.tile_w;
+        const int64_t lo = hfirst ? mid.y : mid.x, hi = lo + (hfirst ? mid.h : mid.w) - 1;
+        const int taps2 = hfirst ? rv.taps : rh.taps;
+        int64_t span = 1;
+        for (int64_t t0 = 0; t0 < n2; t0 += tile) {
+            const int64_t t1 = std::min(n2, t0 + tile) - 1;
+            const int64_t a0 = std::max<int64_t>(st2[size_t(t0)], lo);
+            const int64_t a1 = std::min<int64_t>(int64_t(st2[size_t(t1)]) + taps2 - 1, hi);
+            span = std::max(span, a1 - a0 + 1);
+        }
+        a.span_max = int32_t(span);
+        if (launch::reduce2d_smem_bytes(a) != 0) break;
+        if (hfirst) { if (a.tile_w > 8) a.tile_w /= 2; else a.tile_h = std::max(1, a.tile_h / 2); }
+        else { if (a.tile_h > 2) a.tile_h /= 2; else a.tile_w = std::max(1, a.tile_w / 2); }
+    }
+    if (launch::reduce2d_smem_bytes(a) == 0) return false;
+    st.starts_off = push_table(p->host_tables, sh.data(), sh.size() * 4);
+    st.phases_off = push_table(p->host_tables, ph.data(), ph.size());
+    st.starts2_off = push_table(p->host_tables, sv.data(), sv.size() * 4);
+    st.phases2_off = push_table(p->host_tables, pv.data(), pv.size());
+    if (a.mode_h == kReduceFixed) st.coeffs_off = push_table(p->host_tables, rh.coeffs_i16.data(), rh.coeffs_i16.size() * 2);
+    else st.coeffs_off = push_table(p->host_tables, rh.coeffs_f64.data(), rh.coeffs_f64.size() * 8);
+    if (a.mode_v == kReduceFixed) st.coeffs2_off = push_table(p->host_tables, rv.coeffs_i16.data(), rv.coeffs_i16.size() * 2);
+    else st.coeffs2_off = push_table(p->host_tables, rv.coeffs_f64.data(), rv.coeffs_f64.size() * 8);
+    p->stages.push_back(st);
+    return true;
+}
+
 int mode_for(int32_t fmt, bool horizontal, uint32_t bands) {
     if (fmt == kU8 || fmt == kU16) return kReduceFixed;
     // f32: x86 AVX2 order for 1-band H and for V; scalar fma for multi-band H
@@ -270,13 +338,15 @@ int build_chain(viprs_plan* p, const Chain& chain) {
             if (!p->stages.empty() && p->fmt == kU8 && i == n - 1 && cur != 0) {
                 Stage& last = p->stages.back();
                 const bool ok = (last.type == StageType::Shrink && last.sh.hv_order) ||
-                                ((last.type == StageType::ReduceH || last.type == StageType::ReduceV) &&
+                                ((last.type == StageType::ReduceH || last.type == StageType::ReduceV ||
+                                  last.type == StageType::Reduce2D) &&
                                  (256 % p->bands) == 0) ||
                                 last.type == StageType::Affine;
                 if (ok && last.out_plane == cur) {
                     // retarget the previous stage's output to this node's output and
                     // unpremultiply in its store
                     last.sh.unpremul_out = 1; last.rd.unpremul_out = 1; last.af.unpremul_out = 1;
+                    last.r2.unpremul_out = 1;
                     last.out_plane = -1;
                     // the intermediate plane that stage wrote is no longer needed
                     cur = -1; ++i;
@@ -314,6 +384,25 @@ int build_chain(viprs_plan* p, const Chain& chain) {
             cur = st.out_plane; i = last + 1;
             continue;
         }
+        if ((nd.kind == NodeKind::ReduceH || nd.kind == NodeKind::ReduceV) && i + 1 < n &&
+            ((nd.kind == NodeKind::ReduceH && rt[i + 1].n.kind == NodeKind::ReduceV) ||
+             (nd.kind == NodeKind::ReduceV && rt[i + 1].n.kind == NodeKind::ReduceH))) {
+            const bool hfirst = nd.kind == NodeKind::ReduceH;
+            const int op = plane_for(i + 1);
+            if (op < 0) { PlaneInfo dst; dst.r = out[i + 1]; p->planes.push_back(dst); }
+            const int oplane = op < 0 ? int(p->planes.size()) - 1 : op;
+            const bool ok = add_reduce2d_stage(p, rt[i].rk, rt[i + 1].rk, hfirst, mode_for(p->fmt, hfirst, p->bands),
+                                               mode_for(p->fmt, !hfirst, p->bands), out[i], out[i + 1], cur, oplane,
+                                               p->fmt == kU8);
+            if (op < 0) p->planes.pop_back();
+            if (ok) {
+                if (op < 0) p->stages.back().out_plane = -1;
+                if (pending_premul) { p->stages.back().r2.premul_in = 1; pending_premul = false; }
+                cur = op; i += 2;
+                continue;
+            }
+            if (op >= 0) p->planes.pop_back();  // not fusable: fall through to two launches
+        }
         if (nd.kind == NodeKind::ReduceH || nd.kind == NodeKind::ReduceV) {
             const bool h = nd.kind == NodeKind::ReduceH;
             const int op = plane_for(i);
@@ -335,6 +424,20 @@ int build_chain(viprs_plan* p, const Chain& chain) {
             // ReduceOp: H into the intermediate ReduceConfig region, then V (reduce.rs:103-251)
             Region mid = out[i];
             rt[i].rk2.config_required_axis(out[i].y, out[i].h, &mid.y, &mid.h);
+            {
+                const int op = plane_for(i);
+                if (op < 0) { PlaneInfo dst; dst.r = out[i]; p->planes.push_back(dst); }
+                const int oplane = op < 0 ? int(p->planes.size()) - 1 : op;
+                const bool ok = add_reduce2d_stage(p, rt[i].rk, rt[i].rk2, true, kReduceF64Fma, kReduceF64Fma, mid,
+                                                   out[i], cur, oplane, false);
+                if (op < 0) p->planes.pop_back();
+                if (ok) {
+                    if (op < 0) p->stages.back().out_plane = -1;
+                    cur = op; ++i;
+                    continue;
+                }
+                if (op >= 0) p->planes.pop_back();
+            }
             const int midp = add_plane(p, mid, es, &ws);
             int st = add_reduce_stage(p, rt[i].rk, true, kReduceF64Fma, cur, midp, false);
             if (st) return st;
@@ -470,6 +573,17 @@ int execute(viprs_plan* p, const void* src, void* dst, cudaStream_t s, int first
             a.phases = p->d_tables + st.phases_off;
             a.coeffs = p->d_tables + st.coeffs_off;
             e = st.type == StageType::ReduceH ? launch::reduce_h(a, s) : launch::reduce_v(a, s);
+            break;
+        }
+        case StageType::Reduce2D: {
+            Reduce2DArgs a = st.r2; a.in = ia; a.out = oa;
+            a.starts_h = reinterpret_cast<const int32_t*>(p->d_tables + st.starts_off);
+            a.phases_h = p->d_tables + st.phases_off;
+            a.starts_v = reinterpret_cast<const int32_t*>(p->d_tables + st.starts2_off);
+            a.phases_v = p->d_tables + st.phases2_off;
+            a.coeffs_h = p->d_tables + st.coeffs_off;
+            a.coeffs_v = p->d_tables + st.coeffs2_off;
+            e = launch::reduce2d(a, s);
             break;
         }
         case StageType::Pixel: {

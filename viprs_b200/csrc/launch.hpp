@@ -71,6 +71,32 @@ struct ReduceArgs {
     int32_t unpremul_out = 0;
 };
 
+// ReduceH and ReduceV fused (either order): the first op's output tile stays
+// in shared memory.  Tables follow ReduceArgs; the mid plane is the first op's
+// output region.
+struct Reduce2DArgs {
+    PlaneArg in;
+    OutPlaneArg out;
+    int32_t bands = 1;
+    int32_t fmt = kU8;
+    int32_t hfirst = 1;
+    int64_t mx0 = 0, my0 = 0;
+    int32_t mw = 0, mh = 0;
+    int32_t taps_h = 1, taps_v = 1;
+    int32_t mode_h = kReduceFixed, mode_v = kReduceFixed;
+    const int32_t* starts_h = nullptr;
+    const uint8_t* phases_h = nullptr;
+    const int32_t* starts_v = nullptr;
+    const uint8_t* phases_v = nullptr;
+    const void* coeffs_h = nullptr;
+    const void* coeffs_v = nullptr;
+    int32_t vector_len = 0;   // V f32 split, index within a V output row
+    int32_t premul_in = 0;
+    int32_t unpremul_out = 0;
+    int32_t tile_w = 64, tile_h = 16;
+    int32_t span_max = 0;     // largest mid rows (hfirst) or columns (vfirst) one tile reads
+};
+
 struct PixelArgs {
     PlaneArg in;
     OutPlaneArg out;
@@ -83,6 +109,9 @@ namespace launch {
 cudaError_t shrink2d(ShrinkArgs a, cudaStream_t s);
 cudaError_t reduce_h(const ReduceArgs& a, cudaStream_t s);
 cudaError_t reduce_v(const ReduceArgs& a, cudaStream_t s);
+cudaError_t reduce2d(const Reduce2DArgs& a, cudaStream_t s);
+// Shared memory a reduce2d launch needs for its tile shape; 0 if too large.
+size_t reduce2d_smem_bytes(const Reduce2DArgs& a);
 cudaError_t pixel(const PixelArgs& a, cudaStream_t s);
 // Dynamic shared memory a shrink2d launch needs; 0 if the factor is too large.
 size_t shrink2d_smem_bytes(const ShrinkArgs& a, int32_t* nx);

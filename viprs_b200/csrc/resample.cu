@@ -257,22 +257,37 @@ __global__ void __launch_bounds__(kShrinkThreads) shrink2d_kernel(ShrinkArgs a) 
 // column chunk) item is fetched by one thread with a TMA bulk copy into a
 // ring of `stages` shared-memory buffers, so several rows are in flight while
 // the block sums the current one.  Blocks walk items grid-stride; the ring
-// runs across item boundaries.  Every source byte is read once.
+// runs across item boundaries.  Every source byte is read once.  B is the band
+// count (1..4), so that the box sums use immediate shared-memory offsets.
+struct ShrinkCursor {
+    int32_t item;   // item index (row-major over output rows x column chunks)
+    int32_t k;      // source row within the item (0..fv-1)
+    int32_t oy, c;  // item's output row and column chunk
+};
+
+__device__ __forceinline__ void cursor_set(ShrinkCursor& q, int32_t item, int32_t chunks) {
+    q.item = item;
+    q.k = 0;
+    q.oy = item / chunks;
+    q.c = item - q.oy * chunks;
+}
+
+template <int B>
 __global__ void __launch_bounds__(kShrinkThreads) shrink_hv_u8_tma(ShrinkArgs a) {
     extern __shared__ __align__(128) uint8_t smem_tma[];
     uint8_t* smem = smem_tma;
-    const int S = a.stages;
+    constexpr int S = 4;  // ring depth (power of two)
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
     volatile int32_t* flag = reinterpret_cast<volatile int32_t*>(smem + 64);
     uint8_t* bufs = smem + 128;
     uint8_t* ostage = bufs + (size_t)S * a.stage_bytes;
-    const int bands = a.bands;
-    const uint32_t fh = a.fh, fv = a.fv;
-    const int64_t n_items = (int64_t)a.out.h * a.chunks;
-    const int64_t G = gridDim.x;
-    if ((int64_t)blockIdx.x >= n_items) return;
-    const int64_t n_my = (n_items - 1 - blockIdx.x) / G + 1;
-    const int64_t total = n_my * fv;
+    const int32_t fh = int32_t(a.fh), fv = int32_t(a.fv);
+    const int32_t chunks = a.chunks;
+    const int32_t n_items = a.out.h * chunks;
+    const int32_t G = gridDim.x;
+    if ((int32_t)blockIdx.x >= n_items) return;
+    const int32_t n_my = (n_items - 1 - (int32_t)blockIdx.x) / G + 1;
+    const int64_t total = (int64_t)n_my * fv;
     if (threadIdx.x == 0) {
         for (int i = 0; i < S; ++i) mbar_init(&bars[i], 1);
         *flag = 0;
@@ -280,111 +295,117 @@ __global__ void __launch_bounds__(kShrinkThreads) shrink_hv_u8_tma(ShrinkArgs a)
     }
     __syncthreads();
 
-    // geometry of step t (item, source row)
-    auto geom = [&](int64_t t, int64_t* oy, int* lx0, int* ncols, int64_t* as, uint32_t* bytes, int* lead) {
-        const int64_t item = blockIdx.x + (t / fv) * G;
-        const int64_t k = t % fv;
-        *oy = item / a.chunks;
-        const int c = int(item - *oy * a.chunks);
-        *lx0 = a.col_lo + c * a.nxf;
+    // source byte span of (cursor) and its 16-byte aligned cover
+    auto span = [&](const ShrinkCursor& q, int64_t* as, uint32_t* bytes, int32_t* lead, int32_t* lx0, int32_t* ncols) {
+        *lx0 = a.col_lo + q.c * a.nxf;
         *ncols = min(a.nxf, a.col_hi - *lx0);
-        const int64_t X0 = a.out.x0 + *lx0, Y = a.out.y0 + *oy;
-        int64_t ly = Y * (int64_t)fv + k - a.in.y0;
+        const int64_t X0 = a.out.x0 + *lx0, Y = a.out.y0 + q.oy;
+        int64_t ly = Y * fv + q.k - a.in.y0;
         ly = ly < 0 ? 0 : (ly >= a.in.h ? a.in.h - 1 : ly);
-        const int64_t s = ly * a.in.pitch + (X0 * (int64_t)fh - a.in.x0) * bands;
-        const int64_t e = s + (int64_t)(*ncols) * fh * bands;
-        *as = s & ~int64_t(15);
-        *bytes = uint32_t(((e + 15) & ~int64_t(15)) - *as);
-        *lead = int(s - *as);
+        const int64_t s0 = ly * a.in.pitch + (X0 * fh - a.in.x0) * B;
+        const int64_t e0 = s0 + (int64_t)(*ncols) * fh * B;
+        *as = s0 & ~int64_t(15);
+        *bytes = uint32_t(((e0 + 15) & ~int64_t(15)) - *as);
+        *lead = int32_t(s0 - *as);
     };
-    auto issue = [&](int64_t t) {
-        int64_t oy, as; int lx0, ncols, lead; uint32_t bytes;
-        geom(t, &oy, &lx0, &ncols, &as, &bytes, &lead);
-        const int st = int(t % S);
+    auto advance = [&](ShrinkCursor& q) {
+        if (++q.k == fv) cursor_set(q, q.item + G, chunks);
+    };
+    ShrinkCursor prod;  // producer cursor, thread 0 only
+    int64_t issued = 0;
+    auto issue = [&]() {
+        int64_t as; uint32_t bytes; int32_t lead, lx0, ncols;
+        span(prod, &as, &bytes, &lead, &lx0, &ncols);
+        const int st = int(issued & (S - 1));
         mbar_arrive_expect_tx(&bars[st], bytes);
         bulk_load(bufs + (size_t)st * a.stage_bytes, a.in.data + as, bytes, &bars[st]);
+        ++issued;
+        advance(prod);
     };
-    const int64_t first = total < S ? total : (int64_t)S;
-    if (threadIdx.x == 0)
-        for (int64_t t = 0; t < first; ++t) issue(t);
+    if (threadIdx.x == 0) {
+        cursor_set(prod, blockIdx.x, chunks);
+        const int64_t first = total < S ? total : (int64_t)S;
+        for (int64_t t = 0; t < first; ++t) issue();
+    }
 
+    ShrinkCursor cons;
+    cursor_set(cons, blockIdx.x, chunks);
     uint32_t vacc[kShrinkMaxItems];
-    int off[kShrinkMaxItems];
-    int64_t issued = first;
+    int32_t off[kShrinkMaxItems];
     int64_t t_fail = -1;
     for (int64_t t = 0; t < total; ++t) {
-        const int st = int(t % S);
+        const int st = int(t & (S - 1));
         const uint32_t parity = uint32_t((t / S) & 1);
         if (threadIdx.x == 0 && !mbar_wait(&bars[st], parity)) *flag = 1;
         __syncthreads();
         if (*flag) { t_fail = t; break; }
-        int64_t oy, as; int lx0, ncols, lead; uint32_t bytes;
-        geom(t, &oy, &lx0, &ncols, &as, &bytes, &lead);
-        const int64_t k = t % fv;
-        const int nitems = ncols * bands;
-        if (k == 0) {
+        int64_t as; uint32_t bytes; int32_t lead, lx0, ncols;
+        span(cons, &as, &bytes, &lead, &lx0, &ncols);
+        const int32_t nitems = ncols * B;
+        if (cons.k == 0) {
 #pragma unroll
             for (int q = 0; q < kShrinkMaxItems; ++q) {
                 vacc[q] = 0;
-                const int item = threadIdx.x + q * kShrinkThreads;
-                const int x = item / bands;
-                off[q] = x * int(fh) * bands + (item - x * bands);
+                const int32_t item = threadIdx.x + q * kShrinkThreads;
+                const int32_t x = item / B;
+                off[q] = x * fh * B + (item - x * B);
             }
         }
-        const uint8_t* row = bufs + (size_t)st * a.stage_bytes + lead;
+        uint8_t* row = bufs + (size_t)st * a.stage_bytes + lead;
         if (a.premul_in) {
-            premultiply_staged(const_cast<uint8_t*>(row), ncols * int(fh), bands);
+            premultiply_staged(row, ncols * fh, B);
             __syncthreads();
         }
 #pragma unroll
         for (int q = 0; q < kShrinkMaxItems; ++q) {
-            const int item = threadIdx.x + q * kShrinkThreads;
+            const int32_t item = threadIdx.x + q * kShrinkThreads;
             if (item < nitems) {
                 const uint8_t* p = row + off[q];
                 uint32_t sum = 0;
-#pragma unroll 4
-                for (uint32_t j = 0; j < fh; ++j) sum += p[j * bands];
-                vacc[q] += round_mode_u8(sum, a.hmode, fh, a.hmult);
+                int32_t j = 0;
+                for (; j + 8 <= fh; j += 8, p += 8 * B)
+                    sum += (uint32_t)p[0] + p[B] + p[2 * B] + p[3 * B] + p[4 * B] + p[5 * B] + p[6 * B] + p[7 * B];
+                for (; j < fh; ++j, p += B) sum += p[0];
+                vacc[q] += round_mode_u8(sum, a.hmode, uint32_t(fh), a.hmult);
             }
         }
         __syncthreads();  // all reads of this buffer are done
         if (threadIdx.x == 0 && issued < total) {
             fence_proxy_async_smem();
-            issue(issued);
-            ++issued;
+            issue();
         }
-        if (k == fv - 1) {
-            uint8_t* orow = a.out.data + oy * a.out.pitch + (int64_t)lx0 * bands;
+        if (cons.k == fv - 1) {
+            uint8_t* orow = a.out.data + (int64_t)cons.oy * a.out.pitch + (int64_t)lx0 * B;
             if (a.unpremul_out) {
 #pragma unroll
                 for (int q = 0; q < kShrinkMaxItems; ++q) {
-                    const int item = threadIdx.x + q * kShrinkThreads;
-                    if (item < nitems) ostage[item] = (uint8_t)round_mode_u8(vacc[q], a.vmode, fv, a.vmult);
+                    const int32_t item = threadIdx.x + q * kShrinkThreads;
+                    if (item < nitems) ostage[item] = (uint8_t)round_mode_u8(vacc[q], a.vmode, uint32_t(fv), a.vmult);
                 }
                 __syncthreads();
-                const int ab = bands - 1;
-                for (int item = threadIdx.x; item < nitems; item += blockDim.x) {
-                    const int x = item / bands, b = item - x * bands;
+                for (int32_t item = threadIdx.x; item < nitems; item += blockDim.x) {
+                    const int32_t x = item / B, b = item - x * B;
                     uint32_t v = ostage[item];
-                    if (b != ab) v = unpremultiply_u8(v, ostage[x * bands + ab]);
+                    if (b != B - 1) v = unpremultiply_u8(v, ostage[x * B + B - 1]);
                     orow[item] = (uint8_t)v;
                 }
                 __syncthreads();
             } else {
 #pragma unroll
                 for (int q = 0; q < kShrinkMaxItems; ++q) {
-                    const int item = threadIdx.x + q * kShrinkThreads;
-                    if (item < nitems) orow[item] = (uint8_t)round_mode_u8(vacc[q], a.vmode, fv, a.vmult);
+                    const int32_t item = threadIdx.x + q * kShrinkThreads;
+                    if (item < nitems) orow[item] = (uint8_t)round_mode_u8(vacc[q], a.vmode, uint32_t(fv), a.vmult);
                 }
             }
         }
+        advance(cons);
     }
     if (t_fail >= 0) {
         // a copy never completed: record it, then wait (bounded) for the copies
         // this block still has in flight before its shared memory goes away
         if (threadIdx.x == 0) {
             if (a.err) atomicExch(a.err, VIPRS_ERR_TIMEOUT);
-            for (int64_t tt = t_fail + 1; tt < issued; ++tt) mbar_wait(&bars[tt % S], uint32_t((tt / S) & 1));
+            for (int64_t tt = t_fail + 1; tt < issued; ++tt) mbar_wait(&bars[tt & (S - 1)], uint32_t((tt / S) & 1));
         }
         __syncthreads();
     }
@@ -516,6 +537,200 @@ __global__ void __launch_bounds__(256) reduce_v_kernel(ReduceArgs a) {
     store_or_unpremul<T>(a.out.data + oy * a.out.pitch, item, nitems, outv, a.unpremul_out != 0, bands, stage);
 }
 
+// ---------------------------------------------------------------- fused reduce
+
+template <typename T, int MODE>
+__device__ __forceinline__ T reduce_taps_global(const Plane& in, int64_t lx, int64_t ly, bool horizontal,
+                                                int64_t start_local, int taps, int bands, int b,
+                                                const uint8_t* coef, int ph, bool premul, bool simd_lane) {
+    if (MODE == kReduceFixed) {
+        const int16_t* c = reinterpret_cast<const int16_t*>(coef) + ph * taps;
+        int32_t acc = 0;
+        for (int t = 0; t < taps; ++t) {
+            const int64_t x = horizontal ? start_local + t : lx, y = horizontal ? ly : start_local + t;
+            acc += (int32_t)c[t] * (int32_t)load_premul<T>(in, x, y, bands, b, premul);
+        }
+        return from_fixed<T>(acc);
+    } else {
+        const double* c = reinterpret_cast<const double*>(coef) + ph * taps;
+        double acc = 0.0;
+        if (MODE == kReduceF32Simd && horizontal) {
+            int t = 0;
+            for (; t + 4 <= taps; t += 4) {
+                double lanes = as_f64(load_sample<T>(in, start_local + t, ly, bands, b)) * c[t];
+                lanes = lanes + as_f64(load_sample<T>(in, start_local + t + 1, ly, bands, b)) * c[t + 1];
+                lanes = lanes + as_f64(load_sample<T>(in, start_local + t + 2, ly, bands, b)) * c[t + 2];
+                lanes = lanes + as_f64(load_sample<T>(in, start_local + t + 3, ly, bands, b)) * c[t + 3];
+                acc = acc + lanes;
+            }
+            for (; t < taps; ++t) acc = fma(as_f64(load_sample<T>(in, start_local + t, ly, bands, b)), c[t], acc);
+        } else if (MODE == kReduceF32Simd && simd_lane) {
+            for (int t = 0; t < taps; ++t) acc = acc + as_f64(load_sample<T>(in, lx, start_local + t, bands, b)) * c[t];
+        } else {
+            for (int t = 0; t < taps; ++t) {
+                const int64_t x = horizontal ? start_local + t : lx, y = horizontal ? ly : start_local + t;
+                acc = fma(as_f64(load_sample<T>(in, x, y, bands, b)), c[t], acc);
+            }
+        }
+        return from_f64<T>(acc);
+    }
+}
+
+// Second pass over the shared-memory mid tile `m` (row stride `mstride` samples).
+template <typename T, int MODE>
+__device__ __forceinline__ T reduce_taps_smem(const T* m, int64_t first, int64_t lo, int64_t hi, int64_t origin,
+                                              int64_t stride, int taps, const uint8_t* coef, int ph, bool horizontal,
+                                              bool simd_lane) {
+    // tap i reads mid index clamp(first + i, lo, hi) - origin along the pass axis
+    if (MODE == kReduceFixed) {
+        const int16_t* c = reinterpret_cast<const int16_t*>(coef) + ph * taps;
+        int32_t acc = 0;
+        for (int t = 0; t < taps; ++t) {
+            int64_t q = first + t;
+            q = q < lo ? lo : (q > hi ? hi : q);
+            acc += (int32_t)c[t] * (int32_t)m[(q - origin) * stride];
+        }
+        return from_fixed<T>(acc);
+    } else {
+        const double* c = reinterpret_cast<const double*>(coef) + ph * taps;
+        double acc = 0.0;
+        auto val = [&](int t) {
+            int64_t q = first + t;
+            q = q < lo ? lo : (q > hi ? hi : q);
+            return as_f64(m[(q - origin) * stride]);
+        };
+        if (MODE == kReduceF32Simd && horizontal) {
+            int t = 0;
+            for (; t + 4 <= taps; t += 4) {
+                double lanes = val(t) * c[t];
+                lanes = lanes + val(t + 1) * c[t + 1];
+                lanes = lanes + val(t + 2) * c[t + 2];
+                lanes = lanes + val(t + 3) * c[t + 3];
+                acc = acc + lanes;
+            }
+            for (; t < taps; ++t) acc = fma(val(t), c[t], acc);
+        } else if (MODE == kReduceF32Simd && simd_lane) {
+            for (int t = 0; t < taps; ++t) acc = acc + val(t) * c[t];
+        } else {
+            for (int t = 0; t < taps; ++t) acc = fma(val(t), c[t], acc);
+        }
+        return from_f64<T>(acc);
+    }
+}
+
+// One block: an output tile of tile_h rows x tile_w columns.
+template <typename T, int MH, int MV>
+__global__ void __launch_bounds__(256) reduce2d_kernel(Reduce2DArgs a) {
+    extern __shared__ __align__(16) uint8_t smem_r2[];
+    const int bands = a.bands;
+    const int ch_bytes = 65 * a.taps_h * (MH == kReduceFixed ? 2 : 8);
+    const int cv_bytes = 65 * a.taps_v * (MV == kReduceFixed ? 2 : 8);
+    const int chp = (ch_bytes + 15) / 16 * 16, cvp = (cv_bytes + 15) / 16 * 16;
+    uint8_t* ch = smem_r2;
+    uint8_t* cv = smem_r2 + chp;
+    for (int i = threadIdx.x * 4; i < ch_bytes; i += blockDim.x * 4)
+        *reinterpret_cast<uint32_t*>(ch + i) = *reinterpret_cast<const uint32_t*>((const uint8_t*)a.coeffs_h + i);
+    for (int i = threadIdx.x * 4; i < cv_bytes; i += blockDim.x * 4)
+        *reinterpret_cast<uint32_t*>(cv + i) = *reinterpret_cast<const uint32_t*>((const uint8_t*)a.coeffs_v + i);
+    T* mid = reinterpret_cast<T*>(smem_r2 + chp + cvp);
+    const int tx0 = blockIdx.x * a.tile_w, ty0 = blockIdx.y * a.tile_h;
+    const int ncols = min(a.tile_w, a.out.w - tx0), nrows = min(a.tile_h, a.out.h - ty0);
+    uint8_t* stage = reinterpret_cast<uint8_t*>(mid) + (size_t)a.span_max * (a.hfirst ? ncols : nrows) * bands * sizeof(T);
+    stage = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(stage) + 15) & ~uintptr_t(15));
+    __syncthreads();
+    const bool premul = a.premul_in != 0;
+    if (a.hfirst) {
+        // rows of the mid plane this tile's vertical taps read
+        int64_t rlo = a.starts_v[ty0], rhi = (int64_t)a.starts_v[ty0 + nrows - 1] + a.taps_v - 1;
+        const int64_t mlo = a.my0, mhi = a.my0 + a.mh - 1;
+        rlo = rlo < mlo ? mlo : rlo;
+        rhi = rhi > mhi ? mhi : rhi;
+        const int R = int(rhi - rlo + 1);
+        const int per_row = ncols * bands;
+        for (int i = threadIdx.x; i < R * per_row; i += blockDim.x) {
+            const int r = i / per_row, rem = i - r * per_row, x = rem / bands, b = rem - x * bands;
+            const int64_t ly = rlo + r - a.in.y0;
+            const int col = tx0 + x;
+            mid[i] = reduce_taps_global<T, MH>(a.in, 0, ly, true, (int64_t)a.starts_h[col] - a.in.x0, a.taps_h, bands,
+                                               b, ch, a.phases_h[col], premul, false);
+        }
+        __syncthreads();
+        const int n_out = nrows * per_row;
+        for (int base = 0; base < n_out; base += blockDim.x) {
+            const int i = base + threadIdx.x;
+            T v = T(0);
+            if (i < n_out) {
+                const int yy = i / per_row, rem = i - yy * per_row, x = rem / bands, b = rem - x * bands;
+                const int y = ty0 + yy;
+                const int64_t vidx = (int64_t)(tx0 + x) * bands + b;
+                v = reduce_taps_smem<T, MV>(mid + x * bands + b, a.starts_v[y], mlo, mhi, rlo, per_row, a.taps_v, cv,
+                                            a.phases_v[y], false, vidx < a.vector_len);
+            }
+            const int yy = i / per_row;
+            uint8_t* orow = a.out.data + (int64_t)(ty0 + (i < n_out ? yy : 0)) * a.out.pitch;
+            const int64_t col_item = (int64_t)tx0 * bands + (i - yy * per_row);
+            if (a.unpremul_out) {
+                stage[threadIdx.x] = (uint8_t)v;
+                __syncthreads();
+                if (i < n_out) {
+                    const int b = int(col_item % bands);
+                    uint32_t o = stage[threadIdx.x];
+                    if (b != bands - 1) o = unpremultiply_u8(o, stage[threadIdx.x + (bands - 1 - b)]);
+                    orow[col_item] = (uint8_t)o;
+                }
+                __syncthreads();
+            } else if (i < n_out) {
+                reinterpret_cast<T*>(orow)[col_item] = v;
+            }
+        }
+    } else {
+        // columns of the mid plane this tile's horizontal taps read
+        int64_t clo = a.starts_h[tx0], chi = (int64_t)a.starts_h[tx0 + ncols - 1] + a.taps_h - 1;
+        const int64_t mlo = a.mx0, mhi = a.mx0 + a.mw - 1;
+        clo = clo < mlo ? mlo : clo;
+        chi = chi > mhi ? mhi : chi;
+        const int C = int(chi - clo + 1);
+        const int per_row = C * bands;
+        for (int i = threadIdx.x; i < nrows * per_row; i += blockDim.x) {
+            const int yy = i / per_row, rem = i - yy * per_row, c = rem / bands, b = rem - c * bands;
+            const int y = ty0 + yy;
+            const int64_t mcol = clo + c;
+            const int64_t vidx = (mcol - a.mx0) * bands + b;
+            mid[i] = reduce_taps_global<T, MV>(a.in, mcol - a.in.x0, 0, false, (int64_t)a.starts_v[y] - a.in.y0, a.taps_v,
+                                               bands, b, cv, a.phases_v[y], premul, vidx < a.vector_len);
+        }
+        __syncthreads();
+        const int per_out = ncols * bands;
+        const int n_out = nrows * per_out;
+        for (int base = 0; base < n_out; base += blockDim.x) {
+            const int i = base + threadIdx.x;
+            T v = T(0);
+            if (i < n_out) {
+                const int yy = i / per_out, rem = i - yy * per_out, x = rem / bands, b = rem - x * bands;
+                const int col = tx0 + x;
+                v = reduce_taps_smem<T, MH>(mid + yy * per_row + b, a.starts_h[col], mlo, mhi, clo, bands, a.taps_h, ch,
+                                            a.phases_h[col], true, false);
+            }
+            const int yy = i / per_out;
+            uint8_t* orow = a.out.data + (int64_t)(ty0 + (i < n_out ? yy : 0)) * a.out.pitch;
+            const int64_t col_item = (int64_t)tx0 * bands + (i - yy * per_out);
+            if (a.unpremul_out) {
+                stage[threadIdx.x] = (uint8_t)v;
+                __syncthreads();
+                if (i < n_out) {
+                    const int b = int(col_item % bands);
+                    uint32_t o = stage[threadIdx.x];
+                    if (b != bands - 1) o = unpremultiply_u8(o, stage[threadIdx.x + (bands - 1 - b)]);
+                    orow[col_item] = (uint8_t)o;
+                }
+                __syncthreads();
+            } else if (i < n_out) {
+                reinterpret_cast<T*>(orow)[col_item] = v;
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------- pixel ops
 template <typename T>
 __global__ void pixel_kernel(PixelArgs a) {
@@ -645,7 +860,7 @@ cudaError_t shrink2d(ShrinkArgs a, cudaStream_t s) {
         interior_columns(a, &lo, &hi);
         const int64_t iw = hi - lo;
         const int64_t per_col = int64_t(a.fh) * a.bands;
-        if (iw > 0 && per_col <= 16384) {
+        if (iw > 0 && per_col <= 16384 && a.bands <= 4 && int64_t(a.out.h) * iw < (int64_t(1) << 30)) {
             // columns per item: about 4 KB of source per row, at most 1024 outputs per block
             const int64_t target_cols = std::max<int64_t>(1, 4096 / per_col);
             int64_t chunks = std::max<int64_t>(1, (iw + target_cols - 1) / target_cols);
@@ -659,7 +874,9 @@ cudaError_t shrink2d(ShrinkArgs a, cudaStream_t s) {
                 ShrinkArgs f = a;
                 f.col_lo = lo; f.col_hi = hi; f.nxf = int32_t(nxf); f.chunks = int32_t(chunks);
                 f.stages = stages; f.stage_bytes = stage_bytes;
-                auto k = dev::shrink_hv_u8_tma;
+                void (*k)(ShrinkArgs) = a.bands == 1 ? dev::shrink_hv_u8_tma<1>
+                                       : a.bands == 2 ? dev::shrink_hv_u8_tma<2>
+                                       : a.bands == 3 ? dev::shrink_hv_u8_tma<3> : dev::shrink_hv_u8_tma<4>;
                 cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
                 int per_sm = 0;
                 cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, dev::kShrinkThreads, smem);
@@ -727,6 +944,43 @@ static cudaError_t reduce_any(const ReduceArgs& a, cudaStream_t s) {
 
 cudaError_t reduce_h(const ReduceArgs& a, cudaStream_t s) { return reduce_any<true>(a, s); }
 cudaError_t reduce_v(const ReduceArgs& a, cudaStream_t s) { return reduce_any<false>(a, s); }
+
+size_t reduce2d_smem_bytes(const Reduce2DArgs& a) {
+    const int es = fmt_size(a.fmt);
+    const int mh_b = a.mode_h == kReduceFixed ? 2 : 8, mv_b = a.mode_v == kReduceFixed ? 2 : 8;
+    const size_t ch = (65 * a.taps_h * mh_b + 15) / 16 * 16, cv = (65 * a.taps_v * mv_b + 15) / 16 * 16;
+    const size_t mid = size_t(a.span_max) * (a.hfirst ? a.tile_w : a.tile_h) * a.bands * es;
+    const size_t total = ch + cv + (mid + 15) / 16 * 16 + 256 + 16;
+    return total <= 200 * 1024 ? total : 0;
+}
+
+template <typename T, int MH, int MV>
+static cudaError_t r2d(const Reduce2DArgs& a, size_t smem, cudaStream_t s) {
+    auto k = dev::reduce2d_kernel<T, MH, MV>;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    dim3 grid((unsigned)((a.out.w + a.tile_w - 1) / a.tile_w), (unsigned)((a.out.h + a.tile_h - 1) / a.tile_h));
+    k<<<grid, 256, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t reduce2d(const Reduce2DArgs& a, cudaStream_t s) {
+    if (a.out.w <= 0 || a.out.h <= 0) return cudaSuccess;
+    if (a.unpremul_out && (256 % a.bands) != 0) return cudaErrorInvalidValue;
+    const size_t smem = reduce2d_smem_bytes(a);
+    if (smem == 0) return cudaErrorInvalidValue;
+    switch (a.fmt) {
+    case kU8:
+        if (a.mode_h == kReduceFixed) return r2d<uint8_t, kReduceFixed, kReduceFixed>(a, smem, s);
+        return r2d<uint8_t, kReduceF64Fma, kReduceF64Fma>(a, smem, s);
+    case kU16:
+        if (a.mode_h == kReduceFixed) return r2d<uint16_t, kReduceFixed, kReduceFixed>(a, smem, s);
+        return r2d<uint16_t, kReduceF64Fma, kReduceF64Fma>(a, smem, s);
+    default:
+        if (a.mode_h == kReduceF64Fma && a.mode_v == kReduceF64Fma) return r2d<float, kReduceF64Fma, kReduceF64Fma>(a, smem, s);
+        if (a.mode_h == kReduceF64Fma) return r2d<float, kReduceF64Fma, kReduceF32Simd>(a, smem, s);
+        return r2d<float, kReduceF32Simd, kReduceF32Simd>(a, smem, s);
+    }
+}
 
 cudaError_t pixel(const PixelArgs& a, cudaStream_t s) {
     const int64_t npx = (int64_t)a.out.w * a.out.h;
