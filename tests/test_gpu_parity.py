@@ -223,7 +223,7 @@ def test_mapim(oracle, fmt, kernel, bands):
 
 
 def test_errors_are_statuses():
-    t = to_dev(np.zeros((8, 8, 3), np.uint8))
+    t = to_dev(np.zeros((8, 1000, 3), np.uint8))
     with pytest.raises(ViprsError) as e:
         api.reduce_h(t, 0.5)
     assert e.value.status == 1
@@ -235,6 +235,13 @@ def test_errors_are_statuses():
     assert e.value.status == 7
     with pytest.raises(ViprsError) as e:
         api.affine(t, [1, 2, 2, 4], 0, 0, 8, 8)
+    assert e.value.status == 8
+    with pytest.raises(ViprsError) as e:
+        api.reduce_v(t, float("nan"))
+    assert e.value.status == 1
+    with pytest.raises(ViprsError) as e:
+        api.affine(t, [1, 0, 0, 1], float("inf"), 0, 8, 8)
+    assert e.value.status in (1, 8)
     assert e.value.status == 8
     with pytest.raises(ViprsError):
         api.shrink_h(t, 0)

@@ -252,26 +252,130 @@ __global__ void __launch_bounds__(kShrinkThreads) shrink2d_kernel(ShrinkArgs a) 
     }
 }
 
-// ShrinkH then ShrinkV over u8 for the interior output columns, whose source
-// spans lie inside the plane: each source row segment of an (output row,
-// column chunk) item is fetched by one thread with a TMA bulk copy into a
-// ring of `stages` shared-memory buffers, so several rows are in flight while
-// the block sums the current one.  Blocks walk items grid-stride; the ring
-// runs across item boundaries.  Every source byte is read once.  B is the band
-// count (1..4), so that the box sums use immediate shared-memory offsets.
-struct ShrinkCursor {
-    int32_t item;   // item index (row-major over output rows x column chunks)
-    int32_t k;      // source row within the item (0..fv-1)
-    int32_t oy, c;  // item's output row and column chunk
-};
-
-__device__ __forceinline__ void cursor_set(ShrinkCursor& q, int32_t item, int32_t chunks) {
-    q.item = item;
-    q.k = 0;
-    q.oy = item / chunks;
-    q.c = item - q.oy * chunks;
+// Box sums of one output pixel's fh source pixels (B bands, u8) from shared
+// memory at any byte alignment: words are realigned with a funnel shift and
+// the bands are summed four bytes at a time with dp4a masks.  The word after
+// the box is read (the stage buffers carry 32 bytes of slack) but masked out.
+template <int B>
+__device__ __forceinline__ void box_sums_u8(const uint8_t* p, int fh, uint32_t (&sums)[B]) {
+    const int o = int(reinterpret_cast<uintptr_t>(p) & 3);
+    const uint32_t* wp = reinterpret_cast<const uint32_t*>(p - o);
+    const int nbytes = fh * B;
+    const int K = (nbytes + 3) >> 2;
+    const uint32_t sh = 8u * uint32_t(o);
+    const uint32_t tail_mask = (nbytes & 3) ? ((1u << (8 * (nbytes & 3))) - 1u) : 0xFFFFFFFFu;
+#pragma unroll
+    for (int b = 0; b < B; ++b) sums[b] = 0;
+    auto word = [&](int k) {
+        uint32_t w = __funnelshift_r(wp[k], wp[k + 1], sh);
+        return k == K - 1 ? (w & tail_mask) : w;
+    };
+    if (B == 1) {
+        for (int k = 0; k < K; ++k) sums[0] = __dp4a(word(k), 0x01010101u, sums[0]);
+    } else if (B == 2) {
+        for (int k = 0; k < K; ++k) {
+            const uint32_t w = word(k);
+            sums[0] = __dp4a(w, 0x00010001u, sums[0]);
+            sums[B > 1 ? 1 : 0] = __dp4a(w, 0x01000100u, sums[B > 1 ? 1 : 0]);
+        }
+    } else if (B == 3) {
+        // byte j of the realigned stream is band j % 3: masks repeat every 3 words
+        int k = 0;
+        for (; k + 3 <= K; k += 3) {
+            const uint32_t w0 = word(k), w1 = word(k + 1), w2 = word(k + 2);
+            sums[0] = __dp4a(w0, 0x01000001u, sums[0]);
+            sums[1 % B] = __dp4a(w0, 0x00000100u, sums[1 % B]);
+            sums[2 % B] = __dp4a(w0, 0x00010000u, sums[2 % B]);
+            sums[0] = __dp4a(w1, 0x00010000u, sums[0]);
+            sums[1 % B] = __dp4a(w1, 0x01000001u, sums[1 % B]);
+            sums[2 % B] = __dp4a(w1, 0x00000100u, sums[2 % B]);
+            sums[0] = __dp4a(w2, 0x00000100u, sums[0]);
+            sums[1 % B] = __dp4a(w2, 0x00010000u, sums[1 % B]);
+            sums[2 % B] = __dp4a(w2, 0x01000001u, sums[2 % B]);
+        }
+        if (k < K) {
+            const uint32_t w0 = word(k);
+            sums[0] = __dp4a(w0, 0x01000001u, sums[0]);
+            sums[1 % B] = __dp4a(w0, 0x00000100u, sums[1 % B]);
+            sums[2 % B] = __dp4a(w0, 0x00010000u, sums[2 % B]);
+        }
+        if (k + 1 < K) {
+            const uint32_t w1 = word(k + 1);
+            sums[0] = __dp4a(w1, 0x00010000u, sums[0]);
+            sums[1 % B] = __dp4a(w1, 0x01000001u, sums[1 % B]);
+            sums[2 % B] = __dp4a(w1, 0x00000100u, sums[2 % B]);
+        }
+    } else {
+        for (int k = 0; k < K; ++k) {
+            const uint32_t w = word(k);
+#pragma unroll
+            for (int b = 0; b < B; ++b) sums[b] = __dp4a(w, 1u << (8 * b), sums[b]);
+        }
+    }
 }
 
+// Premultiply<U8> in place over `npx` staged pixels of B bands (alpha last).
+template <int B>
+__device__ __forceinline__ void premultiply_pixels(uint8_t* seg, int npx) {
+    for (int p = threadIdx.x; p < npx; p += blockDim.x) {
+        uint8_t* px = seg + p * B;
+        const uint32_t a = px[B - 1];
+#pragma unroll
+        for (int b = 0; b < B - 1; ++b) px[b] = (uint8_t)premultiply_u8(px[b], a);
+    }
+}
+
+// Output columns of the interior whose source boxes lie inside the plane are
+// processed by the bulk-copy ring below; the few edge columns (the reduce
+// halo beyond the image) by this routine: one (output row, column range)
+// item, every source sample read with clamped coordinates.
+template <int B>
+__device__ void shrink_edge_item_u8(const ShrinkArgs& a, int32_t oy, int32_t c0, int32_t c1, uint8_t* buf) {
+    const int32_t fh = int32_t(a.fh), fv = int32_t(a.fv);
+    const int32_t ncols = c1 - c0;
+    const int32_t per_row = ncols * fh * B;
+    const int64_t Y = a.out.y0 + oy;
+    for (int32_t i = threadIdx.x; i < fv * per_row; i += blockDim.x) {
+        const int32_t k = i / per_row, rem = i - k * per_row;
+        const int32_t xb = rem / B, b = rem - xb * B;
+        const int64_t sx = (a.out.x0 + c0) * (int64_t)fh + xb - a.in.x0;
+        buf[i] = load_sample<uint8_t>(a.in, sx, Y * fv + k - a.in.y0, B, b);
+    }
+    __syncthreads();
+    if (a.premul_in) {
+        premultiply_pixels<B>(buf, fv * ncols * fh);
+        __syncthreads();
+    }
+    uint8_t* ob = buf + fv * per_row;
+    for (int32_t item = threadIdx.x; item < ncols * B; item += blockDim.x) {
+        const int32_t x = item / B, b = item - x * B;
+        uint32_t vs = 0;
+        for (int32_t k = 0; k < fv; ++k) {
+            const uint8_t* p = buf + k * per_row + x * fh * B + b;
+            uint32_t hs = 0;
+            for (int32_t j = 0; j < fh; ++j) hs += p[j * B];
+            vs += round_mode_u8(hs, a.hmode, uint32_t(fh), a.hmult);
+        }
+        ob[item] = (uint8_t)round_mode_u8(vs, a.vmode, uint32_t(fv), a.vmult);
+    }
+    __syncthreads();
+    uint8_t* orow = a.out.data + (int64_t)oy * a.out.pitch + (int64_t)c0 * B;
+    for (int32_t item = threadIdx.x; item < ncols * B; item += blockDim.x) {
+        const int32_t x = item / B, b = item - x * B;
+        uint32_t v = ob[item];
+        if (a.unpremul_out && b != B - 1) v = unpremultiply_u8(v, ob[x * B + B - 1]);
+        orow[item] = (uint8_t)v;
+    }
+    __syncthreads();
+}
+
+// ShrinkH then ShrinkV over u8.  Items are (output row, column chunk) of the
+// interior columns; a block owns every G-th item.  One thread per block fetches
+// each source row segment of its items with a TMA bulk copy into a ring of S
+// shared-memory buffers (the ring runs across item boundaries), so S rows are
+// in flight while the block sums the current one; each thread owns one output
+// pixel of the chunk and accumulates its B band sums over the fv rows.
+// Every source byte is read from HBM once.  B is the band count (1..4).
 template <int B>
 __global__ void __launch_bounds__(kShrinkThreads) shrink_hv_u8_tma(ShrinkArgs a) {
     extern __shared__ __align__(128) uint8_t smem_tma[];
@@ -283,8 +387,18 @@ __global__ void __launch_bounds__(kShrinkThreads) shrink_hv_u8_tma(ShrinkArgs a)
     uint8_t* ostage = bufs + (size_t)S * a.stage_bytes;
     const int32_t fh = int32_t(a.fh), fv = int32_t(a.fv);
     const int32_t chunks = a.chunks;
-    const int32_t n_items = a.out.h * chunks;
     const int32_t G = gridDim.x;
+
+    // edge columns first: small, clamped reads
+    {
+        const int32_t nl = a.col_lo > 0 ? a.out.h : 0, nr = a.col_hi < a.out.w ? a.out.h : 0;
+        for (int32_t e = blockIdx.x; e < nl + nr; e += G) {
+            if (e < nl) shrink_edge_item_u8<B>(a, e, 0, a.col_lo, bufs);
+            else shrink_edge_item_u8<B>(a, e - nl, a.col_hi, a.out.w, bufs);
+        }
+    }
+
+    const int32_t n_items = a.out.h * chunks;
     if ((int32_t)blockIdx.x >= n_items) return;
     const int32_t n_my = (n_items - 1 - (int32_t)blockIdx.x) / G + 1;
     const int64_t total = (int64_t)n_my * fv;
@@ -295,111 +409,102 @@ __global__ void __launch_bounds__(kShrinkThreads) shrink_hv_u8_tma(ShrinkArgs a)
     }
     __syncthreads();
 
-    // source byte span of (cursor) and its 16-byte aligned cover
-    auto span = [&](const ShrinkCursor& q, int64_t* as, uint32_t* bytes, int32_t* lead, int32_t* lx0, int32_t* ncols) {
-        *lx0 = a.col_lo + q.c * a.nxf;
-        *ncols = min(a.nxf, a.col_hi - *lx0);
-        const int64_t X0 = a.out.x0 + *lx0, Y = a.out.y0 + q.oy;
-        int64_t ly = Y * fv + q.k - a.in.y0;
+    // per-item geometry: source byte offset of the chunk within a row and its length
+    struct ItemGeom { int32_t oy, lx0, ncols; int64_t sbase, row0; int32_t nbytes; };
+    auto item_geom = [&](int32_t item) {
+        ItemGeom g;
+        g.oy = item / chunks;
+        const int32_t c = item - g.oy * chunks;
+        g.lx0 = a.col_lo + c * a.nxf;
+        g.ncols = min(a.nxf, a.col_hi - g.lx0);
+        g.sbase = ((a.out.x0 + g.lx0) * (int64_t)fh - a.in.x0) * B;
+        g.row0 = (a.out.y0 + g.oy) * (int64_t)fv - a.in.y0;
+        g.nbytes = g.ncols * fh * B;
+        return g;
+    };
+    auto row_span = [&](const ItemGeom& g, int32_t k, int64_t* as, uint32_t* bytes, int32_t* lead) {
+        int64_t ly = g.row0 + k;
         ly = ly < 0 ? 0 : (ly >= a.in.h ? a.in.h - 1 : ly);
-        const int64_t s0 = ly * a.in.pitch + (X0 * fh - a.in.x0) * B;
-        const int64_t e0 = s0 + (int64_t)(*ncols) * fh * B;
+        const int64_t s0 = ly * a.in.pitch + g.sbase;
         *as = s0 & ~int64_t(15);
-        *bytes = uint32_t(((e0 + 15) & ~int64_t(15)) - *as);
+        *bytes = uint32_t(((s0 + g.nbytes + 15) & ~int64_t(15)) - *as);
         *lead = int32_t(s0 - *as);
     };
-    auto advance = [&](ShrinkCursor& q) {
-        if (++q.k == fv) cursor_set(q, q.item + G, chunks);
-    };
-    ShrinkCursor prod;  // producer cursor, thread 0 only
+
+    // producer state (thread 0)
+    int32_t p_item = blockIdx.x, p_k = 0;
+    ItemGeom pg = item_geom(p_item);
     int64_t issued = 0;
     auto issue = [&]() {
-        int64_t as; uint32_t bytes; int32_t lead, lx0, ncols;
-        span(prod, &as, &bytes, &lead, &lx0, &ncols);
+        int64_t as; uint32_t bytes; int32_t lead;
+        row_span(pg, p_k, &as, &bytes, &lead);
         const int st = int(issued & (S - 1));
         mbar_arrive_expect_tx(&bars[st], bytes);
         bulk_load(bufs + (size_t)st * a.stage_bytes, a.in.data + as, bytes, &bars[st]);
         ++issued;
-        advance(prod);
+        if (++p_k == fv) {
+            p_k = 0;
+            p_item += G;
+            if (p_item < n_items) pg = item_geom(p_item);
+        }
     };
     if (threadIdx.x == 0) {
-        cursor_set(prod, blockIdx.x, chunks);
         const int64_t first = total < S ? total : (int64_t)S;
         for (int64_t t = 0; t < first; ++t) issue();
     }
 
-    ShrinkCursor cons;
-    cursor_set(cons, blockIdx.x, chunks);
-    uint32_t vacc[kShrinkMaxItems];
-    int32_t off[kShrinkMaxItems];
+    int32_t c_item = blockIdx.x, c_k = 0;
+    ItemGeom cg = item_geom(c_item);
+    uint32_t vacc[B];
+#pragma unroll
+    for (int b = 0; b < B; ++b) vacc[b] = 0;
     int64_t t_fail = -1;
+    const int32_t x = threadIdx.x;  // this thread's output pixel within the chunk (nxf <= blockDim)
     for (int64_t t = 0; t < total; ++t) {
         const int st = int(t & (S - 1));
         const uint32_t parity = uint32_t((t / S) & 1);
         if (threadIdx.x == 0 && !mbar_wait(&bars[st], parity)) *flag = 1;
         __syncthreads();
         if (*flag) { t_fail = t; break; }
-        int64_t as; uint32_t bytes; int32_t lead, lx0, ncols;
-        span(cons, &as, &bytes, &lead, &lx0, &ncols);
-        const int32_t nitems = ncols * B;
-        if (cons.k == 0) {
-#pragma unroll
-            for (int q = 0; q < kShrinkMaxItems; ++q) {
-                vacc[q] = 0;
-                const int32_t item = threadIdx.x + q * kShrinkThreads;
-                const int32_t x = item / B;
-                off[q] = x * fh * B + (item - x * B);
-            }
-        }
+        int64_t as; uint32_t bytes; int32_t lead;
+        row_span(cg, c_k, &as, &bytes, &lead);
         uint8_t* row = bufs + (size_t)st * a.stage_bytes + lead;
         if (a.premul_in) {
-            premultiply_staged(row, ncols * fh, B);
+            premultiply_pixels<B>(row, cg.ncols * fh);
             __syncthreads();
         }
+        if (x < cg.ncols) {
+            uint32_t sums[B];
+            box_sums_u8<B>(row + x * fh * B, fh, sums);
 #pragma unroll
-        for (int q = 0; q < kShrinkMaxItems; ++q) {
-            const int32_t item = threadIdx.x + q * kShrinkThreads;
-            if (item < nitems) {
-                const uint8_t* p = row + off[q];
-                uint32_t sum = 0;
-                int32_t j = 0;
-                for (; j + 8 <= fh; j += 8, p += 8 * B)
-                    sum += (uint32_t)p[0] + p[B] + p[2 * B] + p[3 * B] + p[4 * B] + p[5 * B] + p[6 * B] + p[7 * B];
-                for (; j < fh; ++j, p += B) sum += p[0];
-                vacc[q] += round_mode_u8(sum, a.hmode, uint32_t(fh), a.hmult);
-            }
+            for (int b = 0; b < B; ++b) vacc[b] += round_mode_u8(sums[b], a.hmode, uint32_t(fh), a.hmult);
         }
         __syncthreads();  // all reads of this buffer are done
         if (threadIdx.x == 0 && issued < total) {
             fence_proxy_async_smem();
             issue();
         }
-        if (cons.k == fv - 1) {
-            uint8_t* orow = a.out.data + (int64_t)cons.oy * a.out.pitch + (int64_t)lx0 * B;
+        if (++c_k == fv) {
+            uint8_t o[B];
+#pragma unroll
+            for (int b = 0; b < B; ++b) o[b] = (uint8_t)round_mode_u8(vacc[b], a.vmode, uint32_t(fv), a.vmult);
             if (a.unpremul_out) {
 #pragma unroll
-                for (int q = 0; q < kShrinkMaxItems; ++q) {
-                    const int32_t item = threadIdx.x + q * kShrinkThreads;
-                    if (item < nitems) ostage[item] = (uint8_t)round_mode_u8(vacc[q], a.vmode, uint32_t(fv), a.vmult);
-                }
-                __syncthreads();
-                for (int32_t item = threadIdx.x; item < nitems; item += blockDim.x) {
-                    const int32_t x = item / B, b = item - x * B;
-                    uint32_t v = ostage[item];
-                    if (b != B - 1) v = unpremultiply_u8(v, ostage[x * B + B - 1]);
-                    orow[item] = (uint8_t)v;
-                }
-                __syncthreads();
-            } else {
-#pragma unroll
-                for (int q = 0; q < kShrinkMaxItems; ++q) {
-                    const int32_t item = threadIdx.x + q * kShrinkThreads;
-                    if (item < nitems) orow[item] = (uint8_t)round_mode_u8(vacc[q], a.vmode, uint32_t(fv), a.vmult);
-                }
+                for (int b = 0; b < B - 1; ++b) o[b] = (uint8_t)unpremultiply_u8(o[b], o[B - 1]);
             }
+            if (x < cg.ncols) {
+                uint8_t* dst = a.out.data + (int64_t)cg.oy * a.out.pitch + (int64_t)(cg.lx0 + x) * B;
+#pragma unroll
+                for (int b = 0; b < B; ++b) dst[b] = o[b];
+            }
+#pragma unroll
+            for (int b = 0; b < B; ++b) vacc[b] = 0;
+            c_k = 0;
+            c_item += G;
+            if (c_item < n_items) cg = item_geom(c_item);
         }
-        advance(cons);
     }
+    (void)ostage;
     if (t_fail >= 0) {
         // a copy never completed: record it, then wait (bounded) for the copies
         // this block still has in flight before its shared memory goes away
@@ -855,49 +960,33 @@ cudaError_t shrink2d(ShrinkArgs a, cudaStream_t s) {
     if (a.out.w <= 0 || a.out.h <= 0) return cudaSuccess;
     round_consts(a.fh, a.bands, true, &a.hmode, &a.hmult);
     round_consts(a.fv, a.bands, false, &a.vmode, &a.vmult);
-    if (a.fmt == kU8 && a.hv_order && (reinterpret_cast<uintptr_t>(a.in.data) & 15) == 0) {
+    if (a.fmt == kU8 && a.hv_order && (reinterpret_cast<uintptr_t>(a.in.data) & 15) == 0 && a.bands <= 4) {
         int32_t lo, hi;
         interior_columns(a, &lo, &hi);
         const int64_t iw = hi - lo;
         const int64_t per_col = int64_t(a.fh) * a.bands;
-        if (iw > 0 && per_col <= 16384 && a.bands <= 4 && int64_t(a.out.h) * iw < (int64_t(1) << 30)) {
-            // columns per item: about 4 KB of source per row, at most 1024 outputs per block
-            const int64_t target_cols = std::max<int64_t>(1, 4096 / per_col);
-            int64_t chunks = std::max<int64_t>(1, (iw + target_cols - 1) / target_cols);
-            int64_t nxf = (iw + chunks - 1) / chunks;
-            nxf = std::min<int64_t>(nxf, (int64_t)dev::kShrinkMaxItems * dev::kShrinkThreads / a.bands);
-            chunks = (iw + nxf - 1) / nxf;
-            const int stages = 4;
-            const uint32_t stage_bytes = uint32_t((nxf * per_col + 32 + 127) / 128 * 128);
-            const size_t smem = 128 + size_t(stages) * stage_bytes + size_t(nxf * a.bands + 16);
-            if (smem <= 200 * 1024) {
-                ShrinkArgs f = a;
-                f.col_lo = lo; f.col_hi = hi; f.nxf = int32_t(nxf); f.chunks = int32_t(chunks);
-                f.stages = stages; f.stage_bytes = stage_bytes;
-                void (*k)(ShrinkArgs) = a.bands == 1 ? dev::shrink_hv_u8_tma<1>
-                                       : a.bands == 2 ? dev::shrink_hv_u8_tma<2>
-                                       : a.bands == 3 ? dev::shrink_hv_u8_tma<3> : dev::shrink_hv_u8_tma<4>;
-                cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                int per_sm = 0;
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, dev::kShrinkThreads, smem);
-                const int64_t items = int64_t(a.out.h) * chunks;
-                const int64_t grid = std::min<int64_t>(items, int64_t(std::max(per_sm, 1)) * sm_count());
-                k<<<(unsigned)grid, dev::kShrinkThreads, smem, s>>>(f);
-                cudaError_t e = cudaGetLastError();
-                if (e != cudaSuccess) return e;
-                // the edge columns whose source spans leave the plane
-                ShrinkArgs g = a;
-                if (lo > 0) {
-                    g.col_lo = 0; g.col_hi = lo;
-                    e = shrink_typed<uint8_t>(g, s);
-                    if (e != cudaSuccess) return e;
-                }
-                if (hi < a.out.w) {
-                    g.col_lo = hi; g.col_hi = a.out.w;
-                    e = shrink_typed<uint8_t>(g, s);
-                }
-                return e;
-            }
+        // one output pixel per thread: chunks of at most 256 columns, about 16 KB per row
+        int64_t nxf = std::min<int64_t>(dev::kShrinkThreads, std::max<int64_t>(1, 16384 / std::max<int64_t>(per_col, 1)));
+        const int64_t chunks = iw > 0 ? (iw + nxf - 1) / nxf : 0;
+        if (chunks > 0) nxf = (iw + chunks - 1) / chunks;
+        const int64_t edge_cols = std::max<int64_t>(lo, a.out.w - hi);
+        const int64_t edge_bytes = int64_t(a.fv) * edge_cols * per_col + edge_cols * a.bands + 64;
+        const uint32_t stage_bytes = uint32_t((std::max<int64_t>(nxf * per_col, 1) + 32 + 127) / 128 * 128);
+        const size_t smem = 128 + std::max<size_t>(size_t(4) * stage_bytes, size_t(edge_bytes)) + 16;
+        if (iw > 0 && per_col <= 16384 && smem <= 200 * 1024 && int64_t(a.out.h) * chunks < (int64_t(1) << 30)) {
+            ShrinkArgs f = a;
+            f.col_lo = lo; f.col_hi = hi; f.nxf = int32_t(nxf); f.chunks = int32_t(chunks);
+            f.stages = 4; f.stage_bytes = stage_bytes;
+            void (*k)(ShrinkArgs) = a.bands == 1 ? dev::shrink_hv_u8_tma<1>
+                                   : a.bands == 2 ? dev::shrink_hv_u8_tma<2>
+                                   : a.bands == 3 ? dev::shrink_hv_u8_tma<3> : dev::shrink_hv_u8_tma<4>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            int per_sm = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, dev::kShrinkThreads, smem);
+            const int64_t items = std::max<int64_t>(int64_t(a.out.h) * chunks, 2 * int64_t(a.out.h));
+            const int64_t grid = std::min<int64_t>(items, int64_t(std::max(per_sm, 1)) * sm_count());
+            k<<<(unsigned)grid, dev::kShrinkThreads, smem, s>>>(f);
+            return cudaGetLastError();
         }
     }
     switch (a.fmt) {
