@@ -77,6 +77,18 @@ SIGNATURES = {
     "viprs_plan_execute_stages": (_I, [_P, _I, _I, _P, _P, _P]),
     "viprs_plan_execute_host": (_I, [_P, _P, _P, _P]),
     "viprs_plan_destroy": (None, [_P]),
+    "viprs_thumbnail_batch_create": (_I, [_I, _P, _P, _P, _I, _U, _U, _I, _I, ctypes.POINTER(_P)]),
+    "viprs_batch_output_size": (_I, [_P, _I, ctypes.POINTER(_U), ctypes.POINTER(_U)]),
+    "viprs_batch_work_items": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "viprs_batch_launch_count": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "viprs_batch_execute": (_I, [_P, _P, _P, _P]),
+    "viprs_batch_execute_graph": (_I, [_P, _P, _P, _P]),
+    "viprs_batch_execute_per_image": (_I, [_P, _P, _P, _P]),
+    "viprs_batch_autotune": (_I, [_P, _P, _P, _P, _I, ctypes.POINTER(ctypes.c_float)]),
+    "viprs_batch_set_config": (_I, [_P, _U, _I, _I]),
+    "viprs_batch_get_config": (_I, [_P, ctypes.POINTER(_U), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "viprs_batch_status": (_I, [_P, _P]),
+    "viprs_batch_destroy": (None, [_P]),
 }
 
 

@@ -372,3 +372,105 @@ def sm_count():
 
 
 
+
+
+class ThumbnailBatch:
+    """Thumbnails of many u8 images of uneven size (FitBox etc.), run either as
+    one persistent launch over a device work list (optionally through a CUDA
+    graph) or image by image through per-image plans."""
+
+    def __init__(self, shapes, target="fitbox", target_width=256, target_height=256, kernel="lanczos3",
+                 crop=False):
+        L = N.lib()
+        n = len(shapes)
+        hs = (ctypes.c_uint32 * n)(*[int(s[0]) for s in shapes])
+        ws = (ctypes.c_uint32 * n)(*[int(s[1]) for s in shapes])
+        bs = (ctypes.c_uint32 * n)(*[int(s[2]) for s in shapes])
+        t = TARGETS[target] if isinstance(target, str) else int(target)
+        h = ctypes.c_void_p()
+        N.check(L.viprs_thumbnail_batch_create(n, ws, hs, bs, t, target_width, target_height, _kernel(kernel),
+                                               int(crop), ctypes.byref(h)), "thumbnail_batch_create")
+        self._h = h
+        self.shapes = [tuple(int(v) for v in s) for s in shapes]
+        self.out_shapes = []
+        for i in range(n):
+            w = ctypes.c_uint32()
+            hh = ctypes.c_uint32()
+            N.check(L.viprs_batch_output_size(self._h, i, ctypes.byref(w), ctypes.byref(hh)), "batch_output_size")
+            self.out_shapes.append((hh.value, w.value, self.shapes[i][2]))
+        self._ptr_cache = None
+
+    def work(self):
+        items = ctypes.c_int32()
+        stages = ctypes.c_int32()
+        grid = ctypes.c_int32()
+        N.check(N.lib().viprs_batch_work_items(self._h, ctypes.byref(items), ctypes.byref(stages),
+                                               ctypes.byref(grid)), "batch_work_items")
+        return items.value, stages.value, grid.value
+
+    def launches(self):
+        b = ctypes.c_int32()
+        p = ctypes.c_int32()
+        N.check(N.lib().viprs_batch_launch_count(self._h, ctypes.byref(b), ctypes.byref(p)), "batch_launch_count")
+        return b.value, p.value
+
+    def alloc_outputs(self, device="cuda"):
+        return [torch.empty(s, dtype=torch.uint8, device=device) for s in self.out_shapes]
+
+    def pointer_arrays(self, srcs, dsts):
+        """Device arrays of the buffers' addresses (cached for the same buffers)."""
+        key = (tuple(t.data_ptr() for t in srcs), tuple(t.data_ptr() for t in dsts))
+        if self._ptr_cache is None or self._ptr_cache[0] != key:
+            dev = srcs[0].device
+            ps = torch.tensor([t.data_ptr() for t in srcs], dtype=torch.int64, device=dev)
+            pd = torch.tensor([t.data_ptr() for t in dsts], dtype=torch.int64, device=dev)
+            self._ptr_cache = (key, ps, pd)
+        return self._ptr_cache[1], self._ptr_cache[2]
+
+    def run(self, srcs, dsts=None, graph=False):
+        dsts = self.alloc_outputs(srcs[0].device) if dsts is None else dsts
+        ps, pd = self.pointer_arrays(srcs, dsts)
+        fn = N.lib().viprs_batch_execute_graph if graph else N.lib().viprs_batch_execute
+        N.check(fn(self._h, ctypes.c_void_p(ps.data_ptr()), ctypes.c_void_p(pd.data_ptr()), _stream()),
+                "batch_execute")
+        return dsts
+
+    def run_per_image(self, srcs, dsts=None):
+        dsts = self.alloc_outputs(srcs[0].device) if dsts is None else dsts
+        hs = (ctypes.c_uint64 * len(srcs))(*[t.data_ptr() for t in srcs])
+        hd = (ctypes.c_uint64 * len(dsts))(*[t.data_ptr() for t in dsts])
+        N.check(N.lib().viprs_batch_execute_per_image(self._h, hs, hd, _stream()), "batch_execute_per_image")
+        return dsts
+
+    def status(self):
+        return int(N.lib().viprs_batch_status(self._h, _stream()))
+
+    def autotune(self, srcs, dsts, repeats=3):
+        ps, pd = self.pointer_arrays(srcs, dsts)
+        best = ctypes.c_float()
+        N.check(N.lib().viprs_batch_autotune(self._h, ctypes.c_void_p(ps.data_ptr()), ctypes.c_void_p(pd.data_ptr()),
+                                             _stream(), int(repeats), ctypes.byref(best)), "batch_autotune")
+        return self.config(), best.value
+
+    def config(self):
+        r = ctypes.c_uint32()
+        lag = ctypes.c_int32()
+        cap = ctypes.c_int32()
+        N.check(N.lib().viprs_batch_get_config(self._h, ctypes.byref(r), ctypes.byref(lag), ctypes.byref(cap)),
+                "batch_get_config")
+        return {"ring_bytes": r.value, "lag_blocks": lag.value, "blocks_per_sm": cap.value}
+
+    def set_config(self, ring_bytes, lag_blocks, blocks_per_sm):
+        N.check(N.lib().viprs_batch_set_config(self._h, int(ring_bytes), int(lag_blocks), int(blocks_per_sm)),
+                "batch_set_config")
+
+    def close(self):
+        if self._h:
+            N.lib().viprs_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

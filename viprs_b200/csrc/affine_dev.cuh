@@ -1,0 +1,410 @@
+// affine_dev.cuh -- device code of the affine and mapim interpolators (see
+// affine.cu for the viprs files it follows).  Included by affine.cu and batch.cu.
+#pragma once
+
+#include "affine_launch.hpp"
+#include "common.cuh"
+
+namespace viprs {
+namespace dev {
+
+__device__ __forceinline__ int64_t trunc_i64(double v) {
+    // Rust `as i64` for the finite, moderate values reaching here
+    return (int64_t)v;
+}
+
+__device__ __forceinline__ double bicubic_w(double x) {
+    x = fabs(x);
+    if (x < 1.0) return fma(2.5 * x, -x, 1.5 * x * x * x) + 1.0;
+    if (x < 2.0) return fma(4.0, -x, fma(2.5 * x, x, -0.5 * x * x * x)) + 2.0;
+    return 0.0;
+}
+
+// InterpolationKernel::interpolate (kernel.rs:133-214)
+__device__ __forceinline__ double kernel_w(int k, double x) {
+    const double eps = 2.220446049250313e-16;
+    const double pi = 3.141592653589793;
+    switch (k) {
+    case 0: return fabs(x) < 0.5 ? 1.0 : 0.0;
+    case 1: x = fabs(x); return x < 1.0 ? 1.0 - x : 0.0;
+    case 2: case 7: case 5: return bicubic_w(x);
+    case 3:
+        x = fabs(x);
+        if (x < 0.5) return fma(2.0 * x, -x, 1.0);
+        if (x < 1.5) return fma(2.5, -x, x * x) + 1.5;
+        return 0.0;
+    case 8: {
+        x = fabs(x);
+        if (x < eps) return 1.0;
+        if (x < 2.0) { const double p = pi * x; return 2.0 * sin(p) * sin(p / 2.0) / (p * p); }
+        return 0.0;
+    }
+    case 9: {
+        x = fabs(x);
+        if (x < eps) return 1.0;
+        if (x < 3.0) { const double p = pi * x; return 3.0 * sin(p) * sin(p / 3.0) / (p * p); }
+        return 0.0;
+    }
+    default: return 0.0;
+    }
+}
+
+__device__ __forceinline__ int64_t tile_origin(int64_t v, int64_t off, int64_t t) {
+    const int64_t d = v - off;
+    const int64_t q = d >= 0 ? d / t : -((-d + t - 1) / t);
+    return off + q * t;
+}
+
+template <typename T>
+struct AffineCtx {
+    const AffineArgs& a;
+    // the scheduler tile's input region (Affine::required_input_region clipped
+    // to the source bounds): viprs samples outside it read the fill value
+    int64_t rx0 = 0, rx1 = -1, ry0 = 0, ry1 = -1;
+    __device__ AffineCtx(const AffineArgs& args) : a(args) {}
+
+    __device__ void set_tile(int64_t X, int64_t Y) {
+        rx0 = 0; rx1 = (int64_t)a.src_w - 1; ry0 = 0; ry1 = (int64_t)a.src_h - 1;
+        if (X < a.tile_off_x || X >= a.tile_off_x + (int64_t)a.final_w || Y < a.tile_off_y ||
+            Y >= a.tile_off_y + (int64_t)a.final_h)
+            return;  // outside the tile grid (a downstream halo): image bounds only
+        const int64_t X0 = tile_origin(X, a.tile_off_x, a.tile_w), Y0 = tile_origin(Y, a.tile_off_y, a.tile_h);
+        const int64_t TW = min((int64_t)a.tile_w, a.tile_off_x + (int64_t)a.final_w - X0);
+        const int64_t TH = min((int64_t)a.tile_h, a.tile_off_y + (int64_t)a.final_h - Y0);
+        const double* m = a.m;
+        const double xs[2] = {(double)X0, (double)X0 + (double)(TW - 1)};
+        const double ys[2] = {(double)Y0, (double)Y0 + (double)(TH - 1)};
+        double mnx = 0, mxx = 0, mny = 0, mxy = 0;
+        for (int i = 0; i < 4; ++i) {
+            const double x = xs[i & 1], y = ys[i >> 1];
+            const double cx = fma(m[1], y, m[0] * x) + a.tx, cy = fma(m[3], y, m[2] * x) + a.ty;
+            if (i == 0) { mnx = mxx = cx; mny = mxy = cy; }
+            else { mnx = fmin(mnx, cx); mxx = fmax(mxx, cx); mny = fmin(mny, cy); mxy = fmax(mxy, cy); }
+        }
+        int lp = 1, rp = 2;
+        if (a.kernel == 0) { lp = 0; rp = 0; }
+        else if (a.kernel == 1) { lp = 0; rp = 1; }
+        else if (a.kernel == 9 || a.kernel == 4) { lp = 2; rp = 3; }
+        const int64_t x0 = trunc_i64(floor(mnx)) - lp, x1 = trunc_i64(floor(mxx)) + rp;
+        const int64_t y0 = trunc_i64(floor(mny)) - lp, y1 = trunc_i64(floor(mxy)) + rp;
+        rx0 = max(x0, (int64_t)0); rx1 = min(x1, (int64_t)a.src_w - 1);
+        ry0 = max(y0, (int64_t)0); ry1 = min(y1, (int64_t)a.src_h - 1);
+    }
+
+    __device__ double fill() const {
+        if (a.extend == 1) return sizeof(T) == 4 ? 1.0 : (sizeof(T) == 2 ? 65535.0 : 255.0);
+        if (a.extend == 2) return a.background;
+        return 0.0;
+    }
+    __device__ bool resolve(int64_t c, int64_t size, int64_t* r) const {
+        if (size <= 0) return false;
+        if (c >= 0 && c < size) { *r = c; return true; }
+        switch (a.extend) {
+        case 3: *r = c < 0 ? 0 : size - 1; return true;
+        case 4: { int64_t m = c % size; if (m < 0) m += size; *r = m; return true; }
+        case 5: {
+            const int64_t p = size * 2;
+            int64_t w = c % p;
+            if (w < 0) w += p;
+            *r = w < size ? w : p - 1 - w;
+            return true;
+        }
+        default: return false;
+        }
+    }
+    // Affine::sample_band: extend against the source bounds, read the plane
+    __device__ double sb(int64_t ix, int64_t iy, int band) const {
+        int64_t rx, ry;
+        if (!resolve(ix, a.src_w, &rx) || !resolve(iy, a.src_h, &ry)) return fill();
+        if (rx < rx0 || rx > rx1 || ry < ry0 || ry > ry1) return fill();
+        return (double)load_sample<T>(a.in, rx - a.in.x0, ry - a.in.y0, a.bands, band);
+    }
+    __device__ double sbp(int64_t ix, int64_t iy, int band, int ab, double amax) const {
+        const double v = sb(ix, iy, band);
+        if (band == ab) return v;
+        return v * (sb(ix, iy, ab) / amax);
+    }
+    __device__ double sample(double x, double y, int band, bool pm, int ab, double amax) const {
+        if (!isfinite(x) || !isfinite(y)) return fill();
+        const int k = a.kernel;
+        if (k == 0) {
+            const int64_t ix = trunc_i64(x), iy = trunc_i64(y);
+            return pm ? sbp(ix, iy, band, ab, amax) : sb(ix, iy, band);
+        }
+        if (k == 1) {
+            const int64_t x0 = trunc_i64(x), y0 = trunc_i64(y);
+            const double fx = x - (double)x0, fy = y - (double)y0;
+            double p00, p01, p10, p11;
+            if (pm) {
+                p00 = sbp(x0, y0, band, ab, amax); p01 = sbp(x0 + 1, y0, band, ab, amax);
+                p10 = sbp(x0, y0 + 1, band, ab, amax); p11 = sbp(x0 + 1, y0 + 1, band, ab, amax);
+            } else {
+                p00 = sb(x0, y0, band); p01 = sb(x0 + 1, y0, band);
+                p10 = sb(x0, y0 + 1, band); p11 = sb(x0 + 1, y0 + 1, band);
+            }
+            const double top = fma(p01, fx, p00 * (1.0 - fx));
+            const double bottom = fma(p11, fx, p10 * (1.0 - fx));
+            return top * (1.0 - fy) + bottom * fy;
+        }
+        const int64_t support = k == 9 ? 3 : 2;
+        const int64_t cx = trunc_i64(floor(x)), cy = trunc_i64(floor(y));
+        double acc = 0.0, wsum = 0.0;
+        for (int64_t ky = -(support - 1); ky <= support; ++ky) {
+            const int64_t iy = cy + ky;
+            const double wy = kernel_w(k, fabs((double)iy - y));
+            if (wy != 0.0) {
+                for (int64_t kx = -(support - 1); kx <= support; ++kx) {
+                    const int64_t ix = cx + kx;
+                    const double wx = kernel_w(k, fabs((double)ix - x));
+                    if (wx != 0.0) {
+                        const double w = wx * wy;
+                        wsum += w;
+                        acc = fma(pm ? sbp(ix, iy, band, ab, amax) : sb(ix, iy, band), w, acc);
+                    }
+                }
+            }
+        }
+        return wsum > 0.0 ? acc / wsum : fill();
+    }
+    // Affine::sample_pixel_at into out[0..bands)
+    __device__ void pixel(double x, double y, double* out) const {
+        const int bands = a.bands;
+        if (bands == 4 && !a.premultiplied) {
+            if (!isfinite(x) || !isfinite(y)) {
+                for (int b = 0; b < bands; ++b) out[b] = fill();
+                return;
+            }
+            const int ab = bands - 1;
+            const double amax = sizeof(T) == 4 ? 1.0 : (sizeof(T) == 2 ? 65535.0 : 255.0);
+            double alpha = sample(x, y, ab, true, ab, amax);
+            alpha = alpha < 0.0 ? 0.0 : (alpha > amax ? amax : alpha);
+            const double na = alpha / amax;
+            for (int b = 0; b < ab; ++b) {
+                const double p = sample(x, y, b, true, ab, amax);
+                out[b] = na > 0.0 ? p / na : 0.0;
+            }
+            out[ab] = alpha;
+            return;
+        }
+        if (!isfinite(x) || !isfinite(y)) {
+            for (int b = 0; b < bands; ++b) out[b] = fill();
+            return;
+        }
+        if (a.kernel == 0) {
+            const int64_t ix = trunc_i64(x), iy = trunc_i64(y);
+            int64_t rx, ry;
+            if (!resolve(ix, a.src_w, &rx) || !resolve(iy, a.src_h, &ry) || rx < rx0 || rx > rx1 || ry < ry0 ||
+                ry > ry1) {
+                for (int b = 0; b < bands; ++b) out[b] = fill();
+                return;
+            }
+            for (int b = 0; b < bands; ++b) out[b] = (double)load_sample<T>(a.in, rx - a.in.x0, ry - a.in.y0, bands, b);
+            return;
+        }
+        for (int b = 0; b < bands; ++b) out[b] = sample(x, y, b, false, 0, 1.0);
+    }
+};
+
+template <typename T>
+__device__ __forceinline__ T store_round(double v, bool u8_round_first) {
+    if (sizeof(T) == 1 && u8_round_first) {
+        double r = round(v);
+        r = r < 0.0 ? 0.0 : (r > 255.0 ? 255.0 : r);
+        return (T)(uint32_t)r;
+    }
+    return from_f64<T>(v);
+}
+
+// One output pixel (lx, ly) of the plane a.out.
+template <typename T>
+__device__ void affine_pixel(const AffineArgs& a, int64_t lx, int64_t ly) {
+    const int64_t X = a.out.x0 + lx, Y = a.out.y0 + ly;
+    const int bands = a.bands;
+    AffineCtx<T> c(a);
+    c.set_tile(X, Y);
+    double v[8];
+    bool u8_round_first = false;
+    const double* m = a.m;
+    // fast paths and per-axis tables cover the affine's own output rectangle; a
+    // region requested beyond it (a downstream op's halo) takes the general walk
+    const bool inside = X >= 0 && X < (int64_t)a.total_w && Y >= 0 && Y < (int64_t)a.total_h;
+    const int fast = inside ? a.fast : 0;
+    if (fast == 1) {
+        // process_region_nearest_fast (core.rs:1097-1143)
+        const int64_t xc = trunc_i64(fma(m[0], (double)X, a.tx)), yc = trunc_i64(fma(m[3], (double)Y, a.ty));
+        if (yc < 0 || yc >= (int64_t)a.src_h || xc < 0 || xc >= (int64_t)a.src_w) {
+            for (int b = 0; b < bands; ++b) v[b] = c.fill();
+        } else {
+            for (int b = 0; b < bands; ++b) v[b] = (double)load_sample<T>(a.in, xc - a.in.x0, yc - a.in.y0, bands, b);
+        }
+    } else if (fast == 2) {
+        // process_region_bilinear_fast (core.rs:1145-1219)
+        const double cxr = fma(m[0], (double)X, a.tx), cyr = fma(m[3], (double)Y, a.ty);
+        const int64_t xs = trunc_i64(cxr), ys = trunc_i64(cyr);
+        const double wx1 = cxr - (double)xs, wx0 = 1.0 - wx1;
+        const double wy1 = cyr - (double)ys, wy0 = 1.0 - wy1;
+        if (ys < 0 || ys + 1 >= (int64_t)a.src_h || xs < 0 || xs + 1 >= (int64_t)a.src_w) {
+            for (int b = 0; b < bands; ++b) v[b] = c.sample((double)xs + wx1, (double)ys + wy1, b, false, 0, 1.0);
+        } else {
+            for (int b = 0; b < bands; ++b) {
+                const int64_t bx = xs - a.in.x0, by = ys - a.in.y0;
+                const double p00 = (double)load_sample<T>(a.in, bx, by, bands, b);
+                const double p01 = (double)load_sample<T>(a.in, bx + 1, by, bands, b);
+                const double p10 = (double)load_sample<T>(a.in, bx, by + 1, bands, b);
+                const double p11 = (double)load_sample<T>(a.in, bx + 1, by + 1, bands, b);
+                const double top = fma(p01, wx1, p00 * wx0), bottom = fma(p11, wx1, p10 * wx0);
+                v[b] = fma(bottom, wy1, top * wy0);
+            }
+        }
+    } else if (fast == 3) {
+        // process_region_bicubic_fast[_u8] (core.rs:1221-1513), build_cubic_axis (:163-189)
+        const double cxr = fma(m[0], (double)X, a.tx), cyr = fma(m[3], (double)Y, a.ty);
+        const int64_t xs = trunc_i64(floor(cxr)) - 1, ys = trunc_i64(floor(cyr)) - 1;
+        u8_round_first = true;
+        if (ys < 0 || ys + 3 >= (int64_t)a.src_h || xs < 0 || xs + 3 >= (int64_t)a.src_w) {
+            if (sizeof(T) == 1) {
+                for (int b = 0; b < bands; ++b) v[b] = c.sample(cxr, cyr, b, false, 0, 1.0);
+            } else {
+                c.pixel(cxr, cyr, v);
+                u8_round_first = false;
+            }
+        } else {
+            double wx[4], wy[4], sx = 0.0, sy = 0.0;
+            for (int t = 0; t < 4; ++t) {
+                wx[t] = bicubic_w(fabs((double)(xs + t) - cxr));
+                wy[t] = bicubic_w(fabs((double)(ys + t) - cyr));
+            }
+            for (int t = 0; t < 4; ++t) { sx += wx[t]; sy += wy[t]; }
+            if (sx > 0.0) for (int t = 0; t < 4; ++t) wx[t] /= sx;
+            if (sy > 0.0) for (int t = 0; t < 4; ++t) wy[t] /= sy;
+            const int64_t bx = xs - a.in.x0, by = ys - a.in.y0;
+            for (int b = 0; b < bands; ++b) {
+                double acc = 0.0;
+                for (int r = 0; r < 4; ++r) {
+                    const double p0 = (double)load_sample<T>(a.in, bx, by + r, bands, b);
+                    const double p1 = (double)load_sample<T>(a.in, bx + 1, by + r, bands, b);
+                    const double p2 = (double)load_sample<T>(a.in, bx + 2, by + r, bands, b);
+                    const double p3 = (double)load_sample<T>(a.in, bx + 3, by + r, bands, b);
+                    const double ra = fma(p3, wx[3], fma(p2, wx[2], fma(p1, wx[1], p0 * wx[0])));
+                    acc = fma(ra, wy[r], acc);
+                }
+                v[b] = acc;
+            }
+        }
+    } else {
+        double x_in, y_in;
+        if (a.separable && a.xs != nullptr && inside) {
+            x_in = a.xs[X];
+            y_in = a.ys[Y];
+        } else {
+            const int64_t X0 = tile_origin(X, a.tile_off_x, a.tile_w), Y0 = tile_origin(Y, a.tile_off_y, a.tile_h);
+            double rx = fma(m[1], (double)Y0, m[0] * (double)X0) + a.tx;
+            double ry = fma(m[3], (double)Y0, m[2] * (double)X0) + a.ty;
+            for (int64_t r = Y0; r < Y; ++r) { rx += m[1]; ry += m[3]; }
+            x_in = rx; y_in = ry;
+            for (int64_t q = X0; q < X; ++q) { x_in += m[0]; y_in += m[2]; }
+        }
+        c.pixel(x_in, y_in, v);
+    }
+    T* dst = reinterpret_cast<T*>(a.out.data + ly * a.out.pitch) + lx * bands;
+    T o[8];
+    for (int b = 0; b < bands; ++b) o[b] = store_round<T>(v[b], u8_round_first);
+    if (sizeof(T) == 1 && a.unpremul_out && bands >= 2) {
+        const uint32_t al = (uint32_t)o[bands - 1];
+        for (int b = 0; b < bands - 1; ++b) o[b] = (T)unpremultiply_u8((uint32_t)o[b], al);
+    }
+    for (int b = 0; b < bands; ++b) dst[b] = o[b];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) affine_kernel(AffineArgs a) {
+    const int64_t npx = (int64_t)a.out.w * a.out.h;
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npx) return;
+    const int64_t ly = p / a.out.w, lx = p - ly * a.out.w;
+    affine_pixel<T>(a, lx, ly);
+}
+
+// ---------------------------------------------------------------- mapim
+template <typename T>
+__device__ __forceinline__ double mp_band(const MapimArgs& a, int64_t ix, int64_t iy, int band) {
+    int64_t x, y;
+    if (!a.extend_copy) {
+        if (ix < 0 || ix >= (int64_t)a.src_w || iy < 0 || iy >= (int64_t)a.src_h) return a.background;
+        x = ix; y = iy;
+    } else {
+        int lp = 1, rp = 2;
+        if (a.kernel == 0) { lp = 0; rp = 0; }
+        else if (a.kernel == 1) { lp = 0; rp = 1; }
+        else if (a.kernel == 9 || a.kernel == 4) { lp = 2; rp = 3; }
+        if (ix < -(int64_t)(lp + 1) || ix > (int64_t)a.src_w + rp || iy < -(int64_t)(lp + 1) || iy > (int64_t)a.src_h + rp)
+            return a.background;
+        x = clampi64(ix, 0, (int64_t)a.src_w - 1);
+        y = clampi64(iy, 0, (int64_t)a.src_h - 1);
+    }
+    return (double)load_sample<T>(a.src, x, y, a.bands, band);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) mapim_kernel(MapimArgs a) {
+    const int64_t npx = (int64_t)a.out.w * a.out.h;
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npx) return;
+    const int64_t ly = p / a.out.w, lx = p - ly * a.out.w;
+    const float2 idx = *reinterpret_cast<const float2*>(a.index.data + ly * a.index.pitch + lx * 8);
+    const double rx = (double)idx.x, ry = (double)idx.y;
+    const int bands = a.bands;
+    T* dst = reinterpret_cast<T*>(a.out.data + ly * a.out.pitch) + lx * bands;
+    if (!isfinite(rx) || !isfinite(ry)) {
+        for (int b = 0; b < bands; ++b) dst[b] = from_f64<T>(a.background);
+        return;
+    }
+    if (a.kernel == 0) {
+        const int64_t x0 = trunc_i64(floor(rx)), y0 = trunc_i64(floor(ry));
+        for (int b = 0; b < bands; ++b) dst[b] = from_f64<T>(mp_band<T>(a, x0, y0, b));
+        return;
+    }
+    if (a.kernel == 1) {
+        const int64_t x0 = trunc_i64(floor(rx)), y0 = trunc_i64(floor(ry));
+        const double fx = rx - (double)x0, fy = ry - (double)y0;
+        const bool interior = x0 >= 0 && x0 + 1 < (int64_t)a.src_w && y0 >= 0 && y0 + 1 < (int64_t)a.src_h;
+        for (int b = 0; b < bands; ++b) {
+            const double p00 = mp_band<T>(a, x0, y0, b), p01 = mp_band<T>(a, x0 + 1, y0, b);
+            const double p10 = mp_band<T>(a, x0, y0 + 1, b), p11 = mp_band<T>(a, x0 + 1, y0 + 1, b);
+            double top, bottom;
+            if (interior) { top = fma(p01, fx, p00 * (1.0 - fx)); bottom = fma(p11, fx, p10 * (1.0 - fx)); }
+            else { top = fma(p00, 1.0 - fx, p01 * fx); bottom = p10 * (1.0 - fx) + p11 * fx; }
+            dst[b] = from_f64<T>(top * (1.0 - fy) + bottom * fy);
+        }
+        return;
+    }
+    // Affine sampler with Background(bg) over the source read region (mapim.rs:1178-1186, 1250-1271)
+    const int k = a.kernel;
+    const int64_t support = k == 9 ? 3 : 2;
+    const int64_t cx = trunc_i64(floor(rx)), cy = trunc_i64(floor(ry));
+    for (int b = 0; b < bands; ++b) {
+        double acc = 0.0, wsum = 0.0;
+        for (int64_t ky = -(support - 1); ky <= support; ++ky) {
+            const int64_t iy = cy + ky;
+            const double wy = kernel_w(k, fabs((double)iy - ry));
+            if (wy != 0.0) {
+                for (int64_t kx = -(support - 1); kx <= support; ++kx) {
+                    const int64_t ix = cx + kx;
+                    const double wx = kernel_w(k, fabs((double)ix - rx));
+                    if (wx != 0.0) {
+                        const double w = wx * wy;
+                        wsum += w;
+                        double s = a.background;
+                        if (ix >= 0 && ix < (int64_t)a.src_w && iy >= 0 && iy < (int64_t)a.src_h)
+                            s = (double)load_sample<T>(a.src, ix, iy, bands, b);
+                        acc = fma(s, w, acc);
+                    }
+                }
+            }
+        }
+        dst[b] = from_f64<T>(wsum > 0.0 ? acc / wsum : a.background);
+    }
+}
+
+}  // namespace dev
+}  // namespace viprs

@@ -1,0 +1,68 @@
+// batch_launch.hpp -- descriptors of the persistent batched-thumbnail kernel.
+//
+// A batch is many thumbnail plans (one per image) executed by ONE persistent
+// launch that walks a device work list.  Every stage of every image plan
+// becomes a BatchStage; its work is split into items (shrink: output row x
+// column chunk; fused reduce: output tile; affine / pixel: output row).  A
+// stage that consumes another stage's output waits (bounded) until that
+// stage's completion counter reaches its item count.  The list is ordered so
+// that every item a stage waits for precedes it: blocks claim items in list
+// order, so every awaited item is already owned by a running block.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "affine_launch.hpp"
+#include "launch.hpp"
+
+namespace viprs {
+
+enum : int32_t { kBatchShrink = 1, kBatchReduce2D = 2, kBatchPixel = 3, kBatchAffine = 4,
+                 kBatchReduceH = 5, kBatchReduceV = 6 };
+
+struct BatchStage {
+    int32_t type = 0;
+    int32_t image = 0;
+    int32_t in_src = 0;    // the input plane is the image's source buffer
+    int32_t out_dst = 0;   // the output plane is the image's destination buffer
+    int32_t n_items = 0;
+    int32_t dep = -1;      // stage whose completion this stage waits for
+    int32_t dep_items = 0; // that stage's item count
+    // shrink items: chunk layout over the output columns
+    int32_t lo = 0, hi = 0, chunk_cols = 1, n_chunks = 1;
+    // reduce h/v items: samples per item
+    int32_t per_item = 256;
+    ShrinkArgs sh;
+    Reduce2DArgs r2;
+    PixelArgs px;
+    AffineArgs af;
+    ReduceArgs rd;
+};
+
+struct WorkItem {
+    int32_t stage;
+    int32_t index;
+};
+
+struct BatchArgs {
+    const BatchStage* stages = nullptr;
+    const WorkItem* items = nullptr;
+    int32_t n_items = 0;
+    int32_t* counters = nullptr;  // one per stage, zeroed before each launch
+    int32_t* cursor = nullptr;    // work-list cursor, zeroed before each launch
+    int32_t* err = nullptr;       // first error (timeout) seen by any block
+    const uint64_t* srcs = nullptr;  // device array: source pointer of each image
+    const uint64_t* dsts = nullptr;  // device array: destination pointer of each image
+    uint32_t ring_stage_bytes = 0;   // shrink ring buffer size
+    uint32_t smem_bytes = 0;
+};
+
+namespace launch {
+// Launch the persistent kernel on `grid` blocks.
+cudaError_t batch(const BatchArgs& a, int grid, cudaStream_t s);
+// Largest resident block count per SM for `smem` bytes of shared memory.
+int batch_blocks_per_sm(size_t smem);
+}  // namespace launch
+
+}  // namespace viprs

@@ -1,0 +1,431 @@
+// batch_plan.cpp -- batched thumbnails: one plan per image, executed either
+// as ONE persistent launch over a device work list (optionally captured in a
+// CUDA graph) or image by image (the plain per-image GPU path).
+//
+// Each image's plan is PipelineBuilder::thumbnail over an in-memory source
+// (builder/resample.rs:871-979); the persistent kernel runs exactly the same
+// stages with the same tables, so both paths give identical bytes.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <new>
+#include <numeric>
+#include <vector>
+
+#include "batch_launch.hpp"
+#include "chain.hpp"
+#include "viprs_b200.h"
+
+using namespace viprs;
+
+struct viprs_batch {
+    int n = 0;
+    std::vector<uint32_t> w, h, bands;
+    std::vector<viprs_plan*> plans;
+    // knobs (autotuned)
+    uint32_t ring_target = 8192;  // source bytes per shrink row segment
+    int32_t lag_blocks = 2;       // work-list lag between an image's stages, in grids
+    int32_t blocks_per_sm = 0;    // 0 = occupancy maximum
+    // device work list
+    std::vector<BatchStage> stages;
+    std::vector<WorkItem> items;
+    BatchStage* d_stages = nullptr;
+    WorkItem* d_items = nullptr;
+    int32_t* d_counters = nullptr;
+    int32_t* d_ctrl = nullptr;  // [0] cursor, [1] error
+    size_t counters_cap = 0, stages_cap = 0, items_cap = 0;
+    uint32_t ring_stage_bytes = 0;
+    size_t smem = 0;
+    int grid = 0;
+    // captured graph
+    cudaGraphExec_t graph = nullptr;
+    const uint64_t* graph_srcs = nullptr;
+    const uint64_t* graph_dsts = nullptr;
+};
+
+namespace {
+
+int sm_count() {
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 148;
+}
+
+void free_list(viprs_batch* b) {
+    if (b->d_stages) cudaFree(b->d_stages);
+    if (b->d_items) cudaFree(b->d_items);
+    if (b->d_counters) cudaFree(b->d_counters);
+    b->d_stages = nullptr; b->d_items = nullptr; b->d_counters = nullptr;
+    b->stages_cap = b->items_cap = b->counters_cap = 0;
+}
+
+void drop_graph(viprs_batch* b) {
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+    b->graph_srcs = b->graph_dsts = nullptr;
+}
+
+// Convert one image's plan into batch stages; returns status.
+int plan_stages(viprs_batch* b, int image, std::vector<std::vector<BatchStage>>* per_image) {
+    viprs_plan* p = b->plans[size_t(image)];
+    std::vector<BatchStage> out;
+    const int last_plane = int(p->planes.size()) - 1;
+    for (size_t si = 0; si < p->stages.size(); ++si) {
+        const Stage& st = p->stages[si];
+        BatchStage bs;
+        bs.image = image;
+        bs.in_src = st.in_plane == 0 ? 1 : 0;
+        bs.out_dst = st.out_plane == last_plane ? 1 : 0;
+        const PlaneArg in = plane_in_arg(p, st.in_plane, nullptr);
+        const OutPlaneArg outp = plane_out_arg(p, st.out_plane, nullptr);
+        switch (st.type) {
+        case StageType::Shrink: {
+            if (p->fmt != kU8 || !st.sh.hv_order || p->bands > 4) return VIPRS_ERR_UNSUPPORTED_FORMAT;
+            bs.type = kBatchShrink;
+            bs.sh = st.sh;
+            bs.sh.in = in;
+            bs.sh.out = outp;
+            int32_t lo, hi;
+            launch::shrink_prepare(&bs.sh, &lo, &hi);
+            bs.lo = lo; bs.hi = hi;
+            const int64_t per_col = int64_t(bs.sh.fh) * p->bands;
+            bs.chunk_cols = int32_t(std::max<int64_t>(1, std::min<int64_t>(256, b->ring_target / std::max<int64_t>(per_col, 1))));
+            const int32_t n_int = hi > lo ? (hi - lo + bs.chunk_cols - 1) / bs.chunk_cols : 0;
+            bs.n_chunks = (lo > 0 ? 1 : 0) + n_int + (hi < outp.w ? 1 : 0);
+            bs.n_items = outp.h * bs.n_chunks;
+            const uint32_t need = uint32_t((bs.chunk_cols * per_col + 32 + 127) / 128 * 128);
+            b->ring_stage_bytes = std::max(b->ring_stage_bytes, need);
+            break;
+        }
+        case StageType::Reduce2D: {
+            if (p->fmt != kU8 || st.r2.mode_h != kReduceFixed || st.r2.mode_v != kReduceFixed)
+                return VIPRS_ERR_UNSUPPORTED_FORMAT;
+            bs.type = kBatchReduce2D;
+            bs.r2 = st.r2;
+            bs.r2.in = in;
+            bs.r2.out = outp;
+            bs.r2.starts_h = reinterpret_cast<const int32_t*>(p->d_tables + st.starts_off);
+            bs.r2.phases_h = p->d_tables + st.phases_off;
+            bs.r2.starts_v = reinterpret_cast<const int32_t*>(p->d_tables + st.starts2_off);
+            bs.r2.phases_v = p->d_tables + st.phases2_off;
+            bs.r2.coeffs_h = p->d_tables + st.coeffs_off;
+            bs.r2.coeffs_v = p->d_tables + st.coeffs2_off;
+            const int nbx = (outp.w + bs.r2.tile_w - 1) / bs.r2.tile_w;
+            const int nby = (outp.h + bs.r2.tile_h - 1) / bs.r2.tile_h;
+            bs.n_items = nbx * nby;
+            break;
+        }
+        case StageType::Affine: {
+            bs.type = kBatchAffine;
+            bs.af = st.af;
+            bs.af.in = in;
+            bs.af.out = outp;
+            if (bs.af.separable && !bs.af.fast) {
+                bs.af.xs = reinterpret_cast<const double*>(p->d_tables + st.starts_off);
+                bs.af.ys = reinterpret_cast<const double*>(p->d_tables + st.phases_off);
+            }
+            bs.n_items = outp.h;
+            break;
+        }
+        case StageType::Pixel: {
+            bs.type = kBatchPixel;
+            bs.px = st.px;
+            bs.px.in = in;
+            bs.px.out = outp;
+            bs.n_items = outp.h;
+            break;
+        }
+        default:
+            return VIPRS_ERR_UNSUPPORTED_FORMAT;
+        }
+        out.push_back(bs);
+    }
+    (*per_image)[size_t(image)] = std::move(out);
+    return VIPRS_OK;
+}
+
+size_t reduce2d_need(const Reduce2DArgs& a) { return launch::reduce2d_smem_bytes(a); }
+
+// Build the device work list for the current knobs.
+int build_list(viprs_batch* b) {
+    b->ring_stage_bytes = 0;
+    std::vector<std::vector<BatchStage>> per(size_t(b->n));
+    for (int i = 0; i < b->n; ++i) {
+        const int st = plan_stages(b, i, &per);
+        if (st) return st;
+    }
+    b->ring_stage_bytes = std::max<uint32_t>(b->ring_stage_bytes, 256);
+    // shared memory: ring buffers, edge scratch, fused-reduce tiles
+    size_t work = size_t(4) * b->ring_stage_bytes;
+    for (auto& v : per)
+        for (auto& s : v)
+            if (s.type == kBatchReduce2D) work = std::max(work, reduce2d_need(s.r2));
+    b->smem = 128 + (sizeof(BatchStage) + 127) / 128 * 128 + work + 64;
+    if (b->smem > 200 * 1024) return VIPRS_ERR_INVALID_ARGUMENT;
+    int per_sm = launch::batch_blocks_per_sm(b->smem);
+    if (per_sm <= 0) return VIPRS_ERR_INVALID_ARGUMENT;
+    if (b->blocks_per_sm > 0) per_sm = std::min(per_sm, b->blocks_per_sm);
+    b->grid = per_sm * sm_count();
+
+    // flatten: global stage index, dependency on the image's previous stage
+    b->stages.clear();
+    std::vector<std::vector<int>> gidx(size_t(b->n));
+    for (int i = 0; i < b->n; ++i) {
+        for (size_t j = 0; j < per[size_t(i)].size(); ++j) {
+            BatchStage s = per[size_t(i)][j];
+            if (j > 0) {
+                s.dep = gidx[size_t(i)][j - 1];
+                s.dep_items = b->stages[size_t(s.dep)].n_items;
+            }
+            gidx[size_t(i)].push_back(int(b->stages.size()));
+            b->stages.push_back(s);
+        }
+    }
+    // work list: images large first; an image's next stage is emitted once
+    // `lag` further items have been emitted after its previous stage, so that
+    // a block claiming it rarely waits and the producer's output is still in L2
+    std::vector<int> order(size_t(b->n));
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        return uint64_t(b->w[size_t(x)]) * b->h[size_t(x)] * b->bands[size_t(x)] >
+               uint64_t(b->w[size_t(y)]) * b->h[size_t(y)] * b->bands[size_t(y)];
+    });
+    const int64_t lag = int64_t(std::max(b->lag_blocks, 0)) * b->grid;
+    struct Pending { int image; size_t j; int64_t ready_at; };
+    std::deque<Pending> pending;
+    b->items.clear();
+    auto emit = [&](int image, size_t j) {
+        const int g = gidx[size_t(image)][j];
+        for (int32_t k = 0; k < b->stages[size_t(g)].n_items; ++k) b->items.push_back(WorkItem{g, k});
+        if (j + 1 < gidx[size_t(image)].size())
+            pending.push_back(Pending{image, j + 1, int64_t(b->items.size()) + lag});
+    };
+    auto flush = [&](bool all) {
+        while (!pending.empty() && (all || pending.front().ready_at <= int64_t(b->items.size()))) {
+            Pending q = pending.front();
+            pending.pop_front();
+            emit(q.image, q.j);
+        }
+    };
+    for (int image : order) {
+        if (!gidx[size_t(image)].empty()) emit(image, 0);
+        flush(false);
+    }
+    flush(true);
+
+    // upload
+    if (b->stages.size() > b->stages_cap || b->items.size() > b->items_cap || b->stages.size() > b->counters_cap) {
+        free_list(b);
+        b->stages_cap = std::max<size_t>(b->stages.size(), 1);
+        b->items_cap = std::max<size_t>(b->items.size(), 1);
+        b->counters_cap = b->stages_cap;
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->d_stages), b->stages_cap * sizeof(BatchStage));
+        if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&b->d_items), b->items_cap * sizeof(WorkItem));
+        if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&b->d_counters), b->counters_cap * sizeof(int32_t));
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    cudaError_t e = cudaMemcpy(b->d_stages, b->stages.data(), b->stages.size() * sizeof(BatchStage), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_items, b->items.data(), b->items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice);
+    return cuda_status(e);
+}
+
+int launch_batch(viprs_batch* b, const uint64_t* d_srcs, const uint64_t* d_dsts, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(b->d_counters, 0, b->stages.size() * sizeof(int32_t), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_ctrl, 0, 2 * sizeof(int32_t), s);
+    if (e != cudaSuccess) return cuda_status(e);
+    BatchArgs a;
+    a.stages = b->d_stages;
+    a.items = b->d_items;
+    a.n_items = int32_t(b->items.size());
+    a.counters = b->d_counters;
+    a.cursor = b->d_ctrl;
+    a.err = b->d_ctrl + 1;
+    a.srcs = d_srcs;
+    a.dsts = d_dsts;
+    a.ring_stage_bytes = b->ring_stage_bytes;
+    a.smem_bytes = uint32_t(b->smem);
+    return cuda_status(launch::batch(a, b->grid, s));
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t viprs_thumbnail_batch_create(int32_t n, const uint32_t* widths, const uint32_t* heights,
+                                     const uint32_t* bands, int32_t target, uint32_t tw, uint32_t th,
+                                     int32_t kernel, int32_t crop, viprs_batch** out) {
+    if (!out || !widths || !heights || !bands) return VIPRS_ERR_NULL_POINTER;
+    *out = nullptr;
+    if (n <= 0 || target < 0 || target > 3) return VIPRS_ERR_INVALID_ARGUMENT;
+    if (kernel < 0 || kernel > 9) return VIPRS_ERR_INVALID_KERNEL;
+    std::unique_ptr<viprs_batch> b(new (std::nothrow) viprs_batch());
+    if (!b) return VIPRS_ERR_OUT_OF_MEMORY;
+    b->n = n;
+    b->w.assign(widths, widths + n);
+    b->h.assign(heights, heights + n);
+    b->bands.assign(bands, bands + n);
+    b->plans.assign(size_t(n), nullptr);
+    int st = VIPRS_OK;
+    for (int i = 0; i < n && st == VIPRS_OK; ++i) {
+        Chain c;
+        st = builder_thumbnail_chain(widths[i], heights[i], bands[i], ThumbTarget(target), tw, th, Kernel(kernel),
+                                     crop != 0, &c);
+        if (st == VIPRS_OK) st = create_chain_plan(widths[i], heights[i], bands[i], VIPRS_U8, c, &b->plans[size_t(i)]);
+    }
+    if (st == VIPRS_OK) {
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->d_ctrl), 4 * sizeof(int32_t));
+        st = cuda_status(e);
+    }
+    if (st == VIPRS_OK) st = build_list(b.get());
+    if (st != VIPRS_OK) {
+        viprs_batch_destroy(b.release());
+        return st;
+    }
+    *out = b.release();
+    return VIPRS_OK;
+}
+
+int32_t viprs_batch_output_size(const viprs_batch* b, int32_t i, uint32_t* w, uint32_t* h) {
+    if (!b || !w || !h) return VIPRS_ERR_NULL_POINTER;
+    if (i < 0 || i >= b->n) return VIPRS_ERR_INVALID_ARGUMENT;
+    *w = b->plans[size_t(i)]->out_w;
+    *h = b->plans[size_t(i)]->out_h;
+    return VIPRS_OK;
+}
+
+int32_t viprs_batch_work_items(const viprs_batch* b, int32_t* items, int32_t* stages, int32_t* grid) {
+    if (!b) return VIPRS_ERR_NULL_POINTER;
+    if (items) *items = int32_t(b->items.size());
+    if (stages) *stages = int32_t(b->stages.size());
+    if (grid) *grid = b->grid;
+    return VIPRS_OK;
+}
+
+int32_t viprs_batch_execute(viprs_batch* b, const uint64_t* d_srcs, const uint64_t* d_dsts, void* stream) {
+    if (!b || !d_srcs || !d_dsts) return VIPRS_ERR_NULL_POINTER;
+    return launch_batch(b, d_srcs, d_dsts, static_cast<cudaStream_t>(stream));
+}
+
+int32_t viprs_batch_execute_graph(viprs_batch* b, const uint64_t* d_srcs, const uint64_t* d_dsts, void* stream) {
+    if (!b || !d_srcs || !d_dsts) return VIPRS_ERR_NULL_POINTER;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (!b->graph || b->graph_srcs != d_srcs || b->graph_dsts != d_dsts) {
+        drop_graph(b);
+        cudaStream_t cs;
+        cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return cuda_status(e);
+        cudaGraph_t g = nullptr;
+        e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        int st = VIPRS_OK;
+        if (e == cudaSuccess) st = launch_batch(b, d_srcs, d_dsts, cs);
+        cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+        if (e == cudaSuccess) e = e2;
+        if (e == cudaSuccess && st == VIPRS_OK) e = cudaGraphInstantiate(&b->graph, g, 0);
+        if (g) cudaGraphDestroy(g);
+        cudaStreamDestroy(cs);
+        if (st != VIPRS_OK) return st;
+        if (e != cudaSuccess) { b->graph = nullptr; return cuda_status(e); }
+        b->graph_srcs = d_srcs;
+        b->graph_dsts = d_dsts;
+    }
+    return cuda_status(cudaGraphLaunch(b->graph, s));
+}
+
+int32_t viprs_batch_execute_per_image(viprs_batch* b, const uint64_t* h_srcs, const uint64_t* h_dsts, void* stream) {
+    if (!b || !h_srcs || !h_dsts) return VIPRS_ERR_NULL_POINTER;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    for (int i = 0; i < b->n; ++i) {
+        const int st = execute_plan(b->plans[size_t(i)], reinterpret_cast<const void*>(h_srcs[i]),
+                                    reinterpret_cast<void*>(h_dsts[i]), s);
+        if (st) return st;
+    }
+    return VIPRS_OK;
+}
+
+int32_t viprs_batch_launch_count(const viprs_batch* b, int32_t* batched, int32_t* per_image) {
+    if (!b) return VIPRS_ERR_NULL_POINTER;
+    if (batched) *batched = 1;
+    if (per_image) {
+        int32_t n = 0;
+        for (auto* p : b->plans) n += int32_t(p->stages.size());
+        *per_image = n;
+    }
+    return VIPRS_OK;
+}
+
+int32_t viprs_batch_set_config(viprs_batch* b, uint32_t ring_bytes, int32_t lag_blocks, int32_t blocks_per_sm) {
+    if (!b) return VIPRS_ERR_NULL_POINTER;
+    if (ring_bytes < 256 || ring_bytes > 32768 || lag_blocks < 0 || blocks_per_sm < 0) return VIPRS_ERR_INVALID_ARGUMENT;
+    b->ring_target = ring_bytes;
+    b->lag_blocks = lag_blocks;
+    b->blocks_per_sm = blocks_per_sm;
+    drop_graph(b);
+    return build_list(b);
+}
+
+int32_t viprs_batch_get_config(const viprs_batch* b, uint32_t* ring_bytes, int32_t* lag_blocks, int32_t* blocks_per_sm) {
+    if (!b) return VIPRS_ERR_NULL_POINTER;
+    if (ring_bytes) *ring_bytes = b->ring_target;
+    if (lag_blocks) *lag_blocks = b->lag_blocks;
+    if (blocks_per_sm) *blocks_per_sm = b->blocks_per_sm;
+    return VIPRS_OK;
+}
+
+int32_t viprs_batch_autotune(viprs_batch* b, const uint64_t* d_srcs, const uint64_t* d_dsts, void* stream,
+                             int32_t repeats, float* best_ms) {
+    if (!b || !d_srcs || !d_dsts) return VIPRS_ERR_NULL_POINTER;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const uint32_t rings[] = {4096, 8192, 16384};
+    const int32_t lags[] = {1, 2, 4};
+    const int32_t caps[] = {0, 3};
+    float best = 1e30f;
+    uint32_t br = b->ring_target;
+    int32_t bl = b->lag_blocks, bc = b->blocks_per_sm;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    repeats = std::max(repeats, 1);
+    for (uint32_t r : rings)
+        for (int32_t l : lags)
+            for (int32_t c : caps) {
+                if (viprs_batch_set_config(b, r, l, c) != VIPRS_OK) continue;
+                if (launch_batch(b, d_srcs, d_dsts, s) != VIPRS_OK) continue;  // warm
+                cudaEventRecord(e0, s);
+                for (int k = 0; k < repeats; ++k) launch_batch(b, d_srcs, d_dsts, s);
+                cudaEventRecord(e1, s);
+                cudaEventSynchronize(e1);
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                ms /= float(repeats);
+                if (ms < best) { best = ms; br = r; bl = l; bc = c; }
+            }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (best_ms) *best_ms = best;
+    return viprs_batch_set_config(b, br, bl, bc);
+}
+
+int32_t viprs_batch_status(viprs_batch* b, void* stream) {
+    if (!b) return VIPRS_ERR_NULL_POINTER;
+    cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_status(e);
+    int32_t h[2] = {0, 0};
+    e = cudaMemcpy(h, b->d_ctrl, sizeof(h), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_status(e);
+    return h[1];
+}
+
+void viprs_batch_destroy(viprs_batch* b) {
+    if (!b) return;
+    drop_graph(b);
+    free_list(b);
+    if (b->d_ctrl) cudaFree(b->d_ctrl);
+    for (auto* p : b->plans) free_plan(p);
+    delete b;
+}
+
+}  // extern "C"

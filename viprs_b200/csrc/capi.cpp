@@ -20,66 +20,21 @@
 #include <new>
 #include <vector>
 
-#include "affine_launch.hpp"
-#include "launch.hpp"
-#include "plan.hpp"
+#include "chain.hpp"
 #include "viprs_b200.h"
 
 using namespace viprs;
 
 namespace {
-
 thread_local int32_t g_last_cuda_error = 0;
+}  // namespace
 
-int32_t cuda_status(cudaError_t e) {
+int32_t viprs::cuda_status(cudaError_t e) {
     if (e == cudaSuccess) return VIPRS_OK;
     g_last_cuda_error = int32_t(e);
     if (e == cudaErrorMemoryAllocation) return VIPRS_ERR_OUT_OF_MEMORY;
     return VIPRS_ERR_CUDA;
 }
-
-enum class StageType { Shrink, ReduceH, ReduceV, Reduce2D, Pixel, Affine };
-
-struct Stage {
-    StageType type;
-    int in_plane = 0;   // index into planes; 0 = source
-    int out_plane = 0;  // index into planes; last = destination
-    ShrinkArgs sh;
-    ReduceArgs rd;
-    PixelArgs px;
-    AffineArgs af;
-    Reduce2DArgs r2;
-    // offsets of this stage's tables inside the plan table buffer
-    size_t starts_off = 0, phases_off = 0, coeffs_off = 0;
-    size_t starts2_off = 0, phases2_off = 0, coeffs2_off = 0;
-};
-
-struct PlaneInfo {
-    Region r;
-    size_t offset = 0;  // workspace offset (intermediates)
-    int64_t pitch = 0;
-};
-
-}  // namespace
-
-struct viprs_plan {
-    int device = 0;
-    uint32_t in_w = 0, in_h = 0, bands = 0;
-    int32_t fmt = 0;
-    uint32_t out_w = 0, out_h = 0;
-    int64_t in_pitch = 0, out_pitch = 0;
-    std::vector<PlaneInfo> planes;
-    std::vector<Stage> stages;
-    std::vector<uint8_t> host_tables;
-    uint8_t* d_tables = nullptr;
-    uint8_t* d_work = nullptr;
-    size_t work_bytes = 0;
-    bool stream_ordered_alloc = false;
-    cudaStream_t alloc_stream = nullptr;
-    // execute_host staging
-    uint8_t* d_in = nullptr;
-    uint8_t* d_out = nullptr;
-};
 
 namespace {
 
@@ -515,7 +470,7 @@ int alloc_plan(viprs_plan* p, cudaStream_t stream, bool stream_ordered) {
     return cuda_status(e);
 }
 
-void free_plan(viprs_plan* p) {
+void free_plan_a(viprs_plan* p) {
     if (!p) return;
     if (p->stream_ordered_alloc) {
         if (p->d_tables) cudaFreeAsync(p->d_tables, p->alloc_stream);
@@ -529,7 +484,7 @@ void free_plan(viprs_plan* p) {
     delete p;
 }
 
-PlaneArg in_arg(const viprs_plan* p, int idx, const uint8_t* src) {
+PlaneArg in_arg_a(const viprs_plan* p, int idx, const uint8_t* src) {
     const PlaneInfo& pi = p->planes[idx];
     PlaneArg a;
     a.x0 = pi.r.x; a.y0 = pi.r.y; a.w = int32_t(pi.r.w); a.h = int32_t(pi.r.h);
@@ -541,7 +496,7 @@ PlaneArg in_arg(const viprs_plan* p, int idx, const uint8_t* src) {
     return a;
 }
 
-OutPlaneArg out_arg(const viprs_plan* p, int idx, uint8_t* dst) {
+OutPlaneArg out_arg_a(const viprs_plan* p, int idx, uint8_t* dst) {
     const PlaneInfo& pi = p->planes[idx];
     OutPlaneArg a;
     a.x0 = pi.r.x; a.y0 = pi.r.y; a.w = int32_t(pi.r.w); a.h = int32_t(pi.r.h);
@@ -550,15 +505,15 @@ OutPlaneArg out_arg(const viprs_plan* p, int idx, uint8_t* dst) {
     return a;
 }
 
-int execute(viprs_plan* p, const void* src, void* dst, cudaStream_t s, int first = 0, int count = -1) {
+int execute_a(viprs_plan* p, const void* src, void* dst, cudaStream_t s, int first = 0, int count = -1) {
     const uint8_t* in = static_cast<const uint8_t*>(src);
     uint8_t* out = static_cast<uint8_t*>(dst);
     const int nst = int(p->stages.size());
     const int last = count < 0 ? nst : std::min(nst, first + count);
     for (int si = std::max(first, 0); si < last; ++si) {
         Stage& st = p->stages[size_t(si)];
-        const PlaneArg ia = in_arg(p, st.in_plane, in);
-        const OutPlaneArg oa = out_arg(p, st.out_plane, out);
+        const PlaneArg ia = in_arg_a(p, st.in_plane, in);
+        const OutPlaneArg oa = out_arg_a(p, st.out_plane, out);
         cudaError_t e = cudaSuccess;
         switch (st.type) {
         case StageType::Shrink: {
@@ -622,10 +577,24 @@ int64_t pitch_of(const viprs_image* im) {
 int run_single(const viprs_image* in, const viprs_image* out, const PlanNode& node, void* stream) {
     int st = check_image(in);
     if (st) return st;
+    if (in->width == 0 || in->height == 0) return VIPRS_ERR_INVALID_ARGUMENT;
+    {
+        // parameter errors first (BuildError happens before any pixel is touched)
+        uint32_t ow, oh;
+        st = node_output_dims(node, in->width, in->height, &ow, &oh);
+        if (st) return st;
+        if (node.kind == NodeKind::ReduceH || node.kind == NodeKind::ReduceV || node.kind == NodeKind::Reduce) {
+            ReduceKernel rk;
+            st = rk.init(node.factor, node.kernel);
+            if (st == VIPRS_OK && node.kind == NodeKind::Reduce) st = rk.init(node.vfactor, node.kernel);
+            if (st) return st;
+        }
+    }
+    if (!out) return VIPRS_ERR_NULL_POINTER;
+    if (out->width == 0 || out->height == 0) return VIPRS_ERR_SIZE_MISMATCH;
     st = check_image(out);
     if (st) return st;
     if (in->format != out->format || in->bands != out->bands) return VIPRS_ERR_SIZE_MISMATCH;
-    if (in->width == 0 || in->height == 0) return VIPRS_ERR_INVALID_ARGUMENT;
     std::unique_ptr<viprs_plan> p(new (std::nothrow) viprs_plan());
     if (!p) return VIPRS_ERR_OUT_OF_MEMORY;
     p->in_w = in->width; p->in_h = in->height; p->bands = in->bands; p->fmt = in->format;
@@ -638,12 +607,12 @@ int run_single(const viprs_image* in, const viprs_image* out, const PlanNode& no
     if (p->out_w != out->width || p->out_h != out->height) return VIPRS_ERR_SIZE_MISMATCH;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     st = alloc_plan(p.get(), s, true);
-    if (st == VIPRS_OK) st = execute(p.get(), in->data, out->data, s);
-    free_plan(p.release());
+    if (st == VIPRS_OK) st = execute_a(p.get(), in->data, out->data, s);
+    free_plan_a(p.release());
     return st;
 }
 
-int create_chain_plan(uint32_t w, uint32_t h, uint32_t bands, int32_t format, const Chain& chain,
+int create_chain_plan_a(uint32_t w, uint32_t h, uint32_t bands, int32_t format, const Chain& chain,
                       viprs_plan** out) {
     if (!out) return VIPRS_ERR_NULL_POINTER;
     *out = nullptr;
@@ -658,12 +627,24 @@ int create_chain_plan(uint32_t w, uint32_t h, uint32_t bands, int32_t format, co
     p->out_pitch = int64_t(p->out_w) * bands * format_size(Format(format));
     p->planes.back().pitch = p->out_pitch;
     st = alloc_plan(p.get(), nullptr, false);
-    if (st) { free_plan(p.release()); return st; }
+    if (st) { free_plan_a(p.release()); return st; }
     *out = p.release();
     return VIPRS_OK;
 }
 
 }  // namespace
+
+namespace viprs {
+int create_chain_plan(uint32_t w, uint32_t h, uint32_t bands, int32_t format, const Chain& chain, viprs_plan** out) {
+    return create_chain_plan_a(w, h, bands, format, chain, out);
+}
+int execute_plan(viprs_plan* p, const void* src, void* dst, cudaStream_t s, int first, int count) {
+    return execute_a(p, src, dst, s, first, count);
+}
+void free_plan(viprs_plan* p) { free_plan_a(p); }
+PlaneArg plane_in_arg(const viprs_plan* p, int idx, const uint8_t* src) { return in_arg_a(p, idx, src); }
+OutPlaneArg plane_out_arg(const viprs_plan* p, int idx, uint8_t* dst) { return out_arg_a(p, idx, dst); }
+}  // namespace viprs
 
 extern "C" {
 
@@ -844,7 +825,7 @@ int32_t viprs_chain_plan_create(uint32_t w, uint32_t h, uint32_t bands, int32_t 
         n.demand = Demand(v.demand_hint);
         c.nodes.push_back(n);
     }
-    return create_chain_plan(w, h, bands, format, c, out);
+    return create_chain_plan_a(w, h, bands, format, c, out);
 }
 
 int32_t viprs_thumbnail_plan_create(uint32_t w, uint32_t h, uint32_t bands, int32_t format, int32_t target,
@@ -854,7 +835,7 @@ int32_t viprs_thumbnail_plan_create(uint32_t w, uint32_t h, uint32_t bands, int3
     Chain c;
     int st = builder_thumbnail_chain(w, h, bands, ThumbTarget(target), tw, th, Kernel(kernel), crop != 0, &c);
     if (st) return st;
-    return create_chain_plan(w, h, bands, format, c, out);
+    return create_chain_plan_a(w, h, bands, format, c, out);
 }
 
 int32_t viprs_resize_plan_create(uint32_t w, uint32_t h, uint32_t bands, int32_t format, double hscale,
@@ -863,7 +844,7 @@ int32_t viprs_resize_plan_create(uint32_t w, uint32_t h, uint32_t bands, int32_t
     Chain c;
     int st = builder_resize_chain(w, h, bands, hscale, vscale, Kernel(kernel), &c);
     if (st) return st;
-    return create_chain_plan(w, h, bands, format, c, out);
+    return create_chain_plan_a(w, h, bands, format, c, out);
 }
 
 int32_t viprs_plan_output_size(const viprs_plan* p, uint32_t* w, uint32_t* h) {
@@ -886,14 +867,14 @@ int32_t viprs_plan_launch_count(const viprs_plan* p, int32_t* launches) {
 
 int32_t viprs_plan_execute(viprs_plan* p, const void* src, void* dst, void* stream) {
     if (!p || !src || !dst) return VIPRS_ERR_NULL_POINTER;
-    return execute(p, src, dst, static_cast<cudaStream_t>(stream));
+    return execute_a(p, src, dst, static_cast<cudaStream_t>(stream));
 }
 
 int32_t viprs_plan_execute_stages(viprs_plan* p, int32_t first, int32_t count, const void* src, void* dst,
                                   void* stream) {
     if (!p || !src || !dst) return VIPRS_ERR_NULL_POINTER;
     if (first < 0 || count < 0) return VIPRS_ERR_INVALID_ARGUMENT;
-    return execute(p, src, dst, static_cast<cudaStream_t>(stream), first, count);
+    return execute_a(p, src, dst, static_cast<cudaStream_t>(stream), first, count);
 }
 
 int32_t viprs_plan_execute_host(viprs_plan* p, const void* hsrc, void* hdst, void* stream) {
@@ -908,13 +889,13 @@ int32_t viprs_plan_execute_host(viprs_plan* p, const void* hsrc, void* hdst, voi
     if (e != cudaSuccess) return cuda_status(e);
     e = cudaMemcpyAsync(p->d_in, hsrc, in_bytes, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return cuda_status(e);
-    int st = execute(p, p->d_in, p->d_out, s);
+    int st = execute_a(p, p->d_in, p->d_out, s);
     if (st) return st;
     e = cudaMemcpyAsync(hdst, p->d_out, out_bytes, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     return cuda_status(e);
 }
 
-void viprs_plan_destroy(viprs_plan* p) { free_plan(p); }
+void viprs_plan_destroy(viprs_plan* p) { free_plan_a(p); }
 
 }  // extern "C"

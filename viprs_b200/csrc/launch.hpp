@@ -115,6 +115,9 @@ size_t reduce2d_smem_bytes(const Reduce2DArgs& a);
 cudaError_t pixel(const PixelArgs& a, cudaStream_t s);
 // Dynamic shared memory a shrink2d launch needs; 0 if the factor is too large.
 size_t shrink2d_smem_bytes(const ShrinkArgs& a, int32_t* nx);
+// Set the u8 rounding constants of `a` and return its interior output columns
+// [lo, hi) (source boxes inside the plane, aligned spans inside the buffer).
+void shrink_prepare(ShrinkArgs* a, int32_t* lo, int32_t* hi);
 }  // namespace launch
 
 }  // namespace viprs

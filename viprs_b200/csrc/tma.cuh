@@ -12,7 +12,14 @@
 namespace viprs {
 namespace dev {
 
-constexpr uint32_t kMaxPolls = 1u << 26;
+constexpr uint32_t kMaxPolls = 1u << 26;           // hard cap on polls
+constexpr uint64_t kWaitLimitNs = 2000000000ull;   // and on wall time: 2 s
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -43,10 +50,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait; returns false on timeout.
+// Bounded wait (poll count and wall time); returns false on timeout.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    for (uint32_t i = 0; i < kMaxPolls; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (uint32_t i = 0; i < kMaxPolls; ++i) {
         if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 255) == 255 && global_ns() - t0 > kWaitLimitNs) return false;
+    }
     return false;
 }
 
