@@ -97,8 +97,11 @@ int plan_stages(viprs_batch* b, int image, std::vector<std::vector<BatchStage>>*
             const int32_t n_int = hi > lo ? (hi - lo + bs.chunk_cols - 1) / bs.chunk_cols : 0;
             bs.n_chunks = (lo > 0 ? 1 : 0) + n_int + (hi < outp.w ? 1 : 0);
             bs.n_items = outp.h * bs.n_chunks;
-            const uint32_t need = uint32_t((bs.chunk_cols * per_col + 32 + 127) / 128 * 128);
+            const uint32_t need = uint32_t((bs.chunk_cols * per_col + 32 + 15 + 127) / 128 * 128);
             b->ring_stage_bytes = std::max(b->ring_stage_bytes, need);
+            // the edge routine stages fv x fh source pixels of one output column in the ring
+            const int64_t edge = int64_t(bs.sh.fv) * per_col + p->bands + 64;
+            b->ring_stage_bytes = std::max(b->ring_stage_bytes, uint32_t((edge / 4 + 1 + 127) / 128 * 128));
             break;
         }
         case StageType::Reduce2D: {
