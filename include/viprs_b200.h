@@ -262,6 +262,46 @@ int32_t viprs_batch_get_config(const viprs_batch *batch, uint32_t *ring_bytes,
 int32_t viprs_batch_status(viprs_batch *batch, void *stream);
 void viprs_batch_destroy(viprs_batch *batch);
 
+/* ---- adjoints (backward passes), f32 images ---------------------------------
+   viprs's resample operators are forward only, so these have no reference
+   counterpart; each is the exact transpose / derivative of the forward entry
+   point named beside it, as this library evaluates it (same coefficient
+   tables, positions and extend rules).  Scratch is allocated stream-ordered on
+   `stream`.  Gradients are overwritten, not accumulated. */
+
+/* Transpose of viprs_reduceh (horizontal != 0) / viprs_reducev on f32: for
+   every input sample, a gather over the outputs whose taps read it; taps that
+   the clamp-to-edge source read folds onto sample 0 / n-1 are folded there. */
+int32_t viprs_reduce_adjoint(const viprs_image *grad_out, const viprs_image *grad_in,
+                             double factor, int32_t kernel, int32_t horizontal, void *stream);
+/* Transpose of viprs_reduce (ReduceH then ReduceV over the virtual plane):
+   V^T into a mid plane, then H^T folding the mid rows that lie beyond the
+   image onto its edge rows. */
+int32_t viprs_reduce_hv_adjoint(const viprs_image *grad_out, const viprs_image *grad_in,
+                                double hfactor, double vfactor, int32_t kernel, void *stream);
+/* Gradient of viprs_affine_backward_matrix (bilinear) wrt its input image
+   (grad_in, may be NULL; f32 atomics, or with `deterministic` a fixed-point
+   2^-32 accumulator whose integer adds make the result independent of order)
+   and wrt the backward matrix and translation (grad_matrix[6] =
+   d/d(b0, b1, b2, b3, tx, ty), HOST memory, may be NULL; the call then
+   synchronises `stream`).  4-band images without `premultiplied` take the
+   alpha-premultiplying sampler's derivative. */
+int32_t viprs_affine_grad(const viprs_image *in, const viprs_image *grad_out,
+                          const viprs_image *grad_in, const double backward[4], double tx,
+                          double ty, int32_t kernel, int32_t extend, double background,
+                          int32_t premultiplied, uint32_t tile_w, uint32_t tile_h,
+                          int32_t deterministic, double *grad_matrix, void *stream);
+/* Gradient of viprs_mapim on f32 wrt the source image (grad_src, scatter as in
+   viprs_affine_grad) and wrt the 2-band coordinates (grad_index: derivative of
+   the interpolation weights, with the quotient rule through their
+   renormalisation); either output may be NULL.  2/4-band sources need
+   `premultiplied` (the alpha-premultiplying sampler is forward only). */
+int32_t viprs_mapim_grad(const viprs_image *src, const viprs_image *index,
+                         const viprs_image *grad_out, const viprs_image *grad_src,
+                         const viprs_image *grad_index, int32_t kernel, int32_t extend_copy,
+                         double background, int32_t premultiplied, int32_t deterministic,
+                         void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -186,8 +186,10 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchArgs g) {
             BatchStage& s = *sst;
             const uint8_t* in = reinterpret_cast<const uint8_t*>(g.srcs[s.image]);
             uint8_t* out = reinterpret_cast<uint8_t*>(g.dsts[s.image]);
-            if (s.in_src) { s.sh.in.data = in; s.r2.in.data = in; s.px.in.data = in; s.af.in.data = in; }
-            if (s.out_dst) { s.sh.out.data = out; s.r2.out.data = out; s.px.out.data = out; s.af.out.data = out; }
+            if (s.in_src) { s.sh.in.data = in; s.r2.in.data = in; s.px.in.data = in; s.af.in.data = in; s.rd.in.data = in; }
+            if (s.out_dst) {
+                s.sh.out.data = out; s.r2.out.data = out; s.px.out.data = out; s.af.out.data = out; s.rd.out.data = out;
+            }
             if (s.dep >= 0) {
                 bool done = ld_acquire_i32(g.counters + s.dep) >= s.dep_items;
                 const uint64_t t0 = global_ns();
@@ -223,6 +225,14 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchArgs g) {
         case kBatchAffine:
             for (int32_t x = threadIdx.x; x < s.af.out.w; x += blockDim.x) affine_pixel<uint8_t>(s.af, x, it.index);
             break;
+        case kBatchReduceH:
+        case kBatchReduceV: {
+            const int32_t chunks = (s.rd.out.w * s.rd.bands + 255) / 256;
+            const int32_t oy = it.index / chunks, ch = it.index - oy * chunks;
+            if (s.type == kBatchReduceH) reduce_h_chunk<uint8_t, kReduceFixed>(s.rd, ch, oy, work);
+            else reduce_v_chunk<uint8_t, kReduceFixed>(s.rd, ch, oy, work);
+            break;
+        }
         default:
             batch_pixel_row(s.px, it.index);
             break;

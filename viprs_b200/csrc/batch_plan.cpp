@@ -134,6 +134,19 @@ int plan_stages(viprs_batch* b, int image, std::vector<std::vector<BatchStage>>*
             bs.n_items = outp.h;
             break;
         }
+        case StageType::ReduceH:
+        case StageType::ReduceV: {
+            if (p->fmt != kU8 || st.rd.mode != kReduceFixed) return VIPRS_ERR_UNSUPPORTED_FORMAT;
+            bs.type = st.type == StageType::ReduceH ? kBatchReduceH : kBatchReduceV;
+            bs.rd = st.rd;
+            bs.rd.in = in;
+            bs.rd.out = outp;
+            bs.rd.starts = reinterpret_cast<const int32_t*>(p->d_tables + st.starts_off);
+            bs.rd.phases = p->d_tables + st.phases_off;
+            bs.rd.coeffs = p->d_tables + st.coeffs_off;
+            bs.n_items = outp.h * ((outp.w * int32_t(p->bands) + 255) / 256);
+            break;
+        }
         case StageType::Pixel: {
             bs.type = kBatchPixel;
             bs.px = st.px;
@@ -167,6 +180,8 @@ int build_list(viprs_batch* b) {
     for (auto& v : per)
         for (auto& s : v)
             if (s.type == kBatchReduce2D) work = std::max(work, reduce2d_need(s.r2));
+            else if (s.type == kBatchReduceH || s.type == kBatchReduceV)
+                work = std::max(work, size_t(65 * s.rd.taps * 2 + 15) / 16 * 16 + 256);
     b->smem = 128 + (sizeof(BatchStage) + 127) / 128 * 128 + work + 64;
     if (b->smem > 200 * 1024) return VIPRS_ERR_INVALID_ARGUMENT;
     int per_sm = launch::batch_blocks_per_sm(b->smem);

@@ -576,9 +576,9 @@ __device__ __forceinline__ void store_or_unpremul(uint8_t* orow, int64_t item, i
     }
 }
 
+// One chunk of blockDim.x output samples (`chunk`) of output row `oy`.
 template <typename T, int MODE>
-__global__ void __launch_bounds__(256) reduce_h_kernel(ReduceArgs a) {
-    extern __shared__ __align__(16) uint8_t smem[];
+__device__ void reduce_h_chunk(const ReduceArgs& a, int64_t chunk, int64_t oy, uint8_t* smem) {
     const int taps = a.taps, bands = a.bands;
     const int coef_bytes = 65 * taps * (MODE == kReduceFixed ? 2 : 8);
     const bool coef_in_smem = coef_bytes <= 48 * 1024;
@@ -591,8 +591,7 @@ __global__ void __launch_bounds__(256) reduce_h_kernel(ReduceArgs a) {
     }
     uint8_t* stage = smem + ((coef_in_smem ? coef_bytes : 0) + 15) / 16 * 16;
     const int nitems = a.out.w * bands;
-    const int64_t item = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t oy = blockIdx.y;
+    const int64_t item = chunk * blockDim.x + threadIdx.x;
     const int64_t ly = a.out.y0 + oy - a.in.y0;
     T outv = T(0);
     if (item < nitems) {
@@ -630,8 +629,13 @@ __global__ void __launch_bounds__(256) reduce_h_kernel(ReduceArgs a) {
 }
 
 template <typename T, int MODE>
-__global__ void __launch_bounds__(256) reduce_v_kernel(ReduceArgs a) {
+__global__ void __launch_bounds__(256) reduce_h_kernel(ReduceArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
+    reduce_h_chunk<T, MODE>(a, blockIdx.x, blockIdx.y, smem);
+}
+
+template <typename T, int MODE>
+__device__ void reduce_v_chunk(const ReduceArgs& a, int64_t chunk, int64_t oy, uint8_t* smem) {
     const int taps = a.taps, bands = a.bands;
     const int coef_bytes = 65 * taps * (MODE == kReduceFixed ? 2 : 8);
     const bool coef_in_smem = coef_bytes <= 48 * 1024;
@@ -644,8 +648,7 @@ __global__ void __launch_bounds__(256) reduce_v_kernel(ReduceArgs a) {
     }
     uint8_t* stage = smem + ((coef_in_smem ? coef_bytes : 0) + 15) / 16 * 16;
     const int nitems = a.out.w * bands;
-    const int64_t item = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t oy = blockIdx.y;
+    const int64_t item = chunk * blockDim.x + threadIdx.x;
     const int64_t base = (int64_t)a.starts[oy] - a.in.y0;
     const int ph = a.phases[oy];
     T outv = T(0);
@@ -670,6 +673,12 @@ __global__ void __launch_bounds__(256) reduce_v_kernel(ReduceArgs a) {
         }
     }
     store_or_unpremul<T>(a.out.data + oy * a.out.pitch, item, nitems, outv, a.unpremul_out != 0, bands, stage);
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) reduce_v_kernel(ReduceArgs a) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    reduce_v_chunk<T, MODE>(a, blockIdx.x, blockIdx.y, smem);
 }
 
 // ---------------------------------------------------------------- fused reduce
