@@ -274,9 +274,9 @@ void viprs_batch_destroy(viprs_batch *batch);
    the clamp-to-edge source read folds onto sample 0 / n-1 are folded there. */
 int32_t viprs_reduce_adjoint(const viprs_image *grad_out, const viprs_image *grad_in,
                              double factor, int32_t kernel, int32_t horizontal, void *stream);
-/* Transpose of viprs_reduce (ReduceH then ReduceV over the virtual plane):
-   V^T into a mid plane, then H^T folding the mid rows that lie beyond the
-   image onto its edge rows. */
+/* Transpose of the ReduceH -> ReduceV chain (PipelineBuilder::reduce_h(..)
+   .reduce_v(..), one fused stage of a chain plan): V^T into a mid plane, then
+   H^T folding the mid rows that lie beyond the image onto its edge rows. */
 int32_t viprs_reduce_hv_adjoint(const viprs_image *grad_out, const viprs_image *grad_in,
                                 double hfactor, double vfactor, int32_t kernel, void *stream);
 /* Gradient of viprs_affine_backward_matrix (bilinear) wrt its input image

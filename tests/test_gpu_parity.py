@@ -241,8 +241,7 @@ def test_errors_are_statuses():
     assert e.value.status == 1
     with pytest.raises(ViprsError) as e:
         api.affine(t, [1, 0, 0, 1], float("inf"), 0, 8, 8)
-    assert e.value.status in (1, 8)
-    assert e.value.status == 8
+    assert e.value.status == 1  # InvalidAffineMatrix: non-finite translation
     with pytest.raises(ViprsError):
         api.shrink_h(t, 0)
 

@@ -100,7 +100,8 @@ def reduce(t, hfactor, vfactor, kernel="lanczos3"):
 def shrink_h(t, factor, ceil=False):
     t = _as_hwc(t)
     h, w, b = t.shape
-    ow = -(-w // factor) if ceil else w // factor
+    # factor 0 is rejected by the library (InvalidShrinkParameters), not here
+    ow = 0 if factor <= 0 else (-(-w // factor) if ceil else w // factor)
     out = _empty(h, ow, b, t)
     N.check(N.lib().viprs_shrinkh(image(t), image(out), int(factor), int(ceil), _stream()), "shrink_h")
     return out
@@ -109,7 +110,7 @@ def shrink_h(t, factor, ceil=False):
 def shrink_v(t, factor, ceil=False):
     t = _as_hwc(t)
     h, w, b = t.shape
-    oh = -(-h // factor) if ceil else h // factor
+    oh = 0 if factor <= 0 else (-(-h // factor) if ceil else h // factor)
     out = _empty(oh, w, b, t)
     N.check(N.lib().viprs_shrinkv(image(t), image(out), int(factor), int(ceil), _stream()), "shrink_v")
     return out
@@ -118,7 +119,7 @@ def shrink_v(t, factor, ceil=False):
 def shrink(t, hfactor, vfactor):
     t = _as_hwc(t)
     h, w, b = t.shape
-    out = _empty(h // vfactor, w // hfactor, b, t)
+    out = _empty(h // vfactor if vfactor > 0 else 0, w // hfactor if hfactor > 0 else 0, b, t)
     N.check(N.lib().viprs_shrink(image(t), image(out), int(hfactor), int(vfactor), _stream()), "shrink")
     return out
 

@@ -62,9 +62,10 @@ __global__ void __launch_bounds__(256) reduce_adjoint_kernel(ReduceAdjArgs a) {
     a.g_in[idx] = (float)acc;
 }
 
+// Image-gradient scatter; both targets null = the image gradient was not requested.
 __device__ __forceinline__ void scatter(float* g, unsigned long long* fx, double scale, int64_t idx, double v) {
     if (fx) atomicAdd(fx + idx, (unsigned long long)(long long)llrint(v * scale));
-    else atomicAdd(g + idx, (float)v);
+    else if (g) atomicAdd(g + idx, (float)v);
 }
 
 // Bilinear forward of one band with derivative, from four samples.
