@@ -45,7 +45,8 @@ typedef enum {
     VIPRS_ERR_INVALID_KERNEL = 7,
     VIPRS_ERR_DEGENERATE_AFFINE = 8,
     VIPRS_ERR_NULL_POINTER = 9,
-    VIPRS_ERR_SIZE_MISMATCH = 10
+    VIPRS_ERR_SIZE_MISMATCH = 10,
+    VIPRS_ERR_SCRATCH_LIMIT = 11  /* viprs_reduce_noalloc: tables + planes exceed its static scratch */
 } viprs_status;
 
 /* BandFormatId subset on this path (crates/viprs-core/src/format.rs). */
@@ -261,6 +262,27 @@ int32_t viprs_batch_get_config(const viprs_batch *batch, uint32_t *ring_bytes,
    if a bounded wait gave up), 0 if none. */
 int32_t viprs_batch_status(viprs_batch *batch, void *stream);
 void viprs_batch_destroy(viprs_batch *batch);
+
+/* ---- no device allocation ----------------------------------------------------
+   No counterpart in the reference: viprs runs on the CPU and has no device
+   memory to manage.  Same operation, arguments and result as viprs_reduce,
+   but the call allocates no device memory (no cudaMalloc, cudaMallocAsync or
+   cudaFree, no library allocator): its coefficient and position tables, and
+   the intermediate plane when the fused tile does not fit in shared memory,
+   live in one static device array of VIPRS_NOALLOC_SCRATCH_BYTES that every
+   GPU loading this library holds until the process exits.  It is for callers
+   that cannot allocate device memory: a host framework whose allocator owns
+   the GPU's memory, a plugin inside another program's processing callback,
+   a latency-bound loop that must not let cudaMalloc/cudaFree synchronise the
+   device.  Work needing more than the array returns VIPRS_ERR_SCRATCH_LIMIT
+   before touching the GPU.  The first call on each device (with that device
+   current) looks up the array's device address and may load this library's
+   device code there: make it before any stream capture begins.  All calls on
+   a device share the array, so calls whose GPU work overlaps (different
+   streams or threads without ordering between them) race; order them. */
+#define VIPRS_NOALLOC_SCRATCH_BYTES (4u << 20)
+int32_t viprs_reduce_noalloc(const viprs_image *in, const viprs_image *out, double hfactor,
+                             double vfactor, int32_t kernel, void *stream);
 
 /* ---- adjoints (backward passes), f32 images ---------------------------------
    viprs's resample operators are forward only, so these have no reference

@@ -14,6 +14,7 @@ STATUS = {
     4: "out of device memory", 5: "CUDA error", 6: "device wait timed out",
     7: "interpolation kernel not valid for this op", 8: "affine matrix determinant is singular",
     9: "null pointer", 10: "image size, bands or format mismatch",
+    11: "work exceeds the static scratch of the no-alloc entry point",
 }
 
 
@@ -89,6 +90,7 @@ SIGNATURES = {
     "viprs_batch_get_config": (_I, [_P, ctypes.POINTER(_U), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "viprs_batch_status": (_I, [_P, _P]),
     "viprs_batch_destroy": (None, [_P]),
+    "viprs_reduce_noalloc": (_I, [_IMG, _IMG, _D, _D, _I, _P]),
     "viprs_reduce_adjoint": (_I, [_IMG, _IMG, _D, _I, _I, _P]),
     "viprs_reduce_hv_adjoint": (_I, [_IMG, _IMG, _D, _D, _I, _P]),
     "viprs_affine_grad": (_I, [_IMG, _IMG, _IMG, ctypes.POINTER(_D), _D, _D, _I, _I, _D, _I, _U, _U, _I,

@@ -18,7 +18,7 @@ OBJ_DIR = os.path.join(ROOT, "_build", "obj")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
-CU_SOURCES = ["resample.cu", "affine.cu", "adjoint.cu", "batch.cu"]
+CU_SOURCES = ["resample.cu", "affine.cu", "adjoint.cu", "batch.cu", "noalloc.cu"]
 CPP_SOURCES = ["plan.cpp", "affine_plan.cpp", "capi.cpp", "batch_plan.cpp", "adjoint_plan.cpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -644,6 +644,39 @@ int execute_plan(viprs_plan* p, const void* src, void* dst, cudaStream_t s, int 
 void free_plan(viprs_plan* p) { free_plan_a(p); }
 PlaneArg plane_in_arg(const viprs_plan* p, int idx, const uint8_t* src) { return in_arg_a(p, idx, src); }
 OutPlaneArg plane_out_arg(const viprs_plan* p, int idx, uint8_t* dst) { return out_arg_a(p, idx, dst); }
+
+// Host-side planning of a one-node chain for `in` -> `out`, with the same
+// checks, in the same order, as the allocating single-op entry points; the
+// plan's device pointers are left null for the caller to point at memory it
+// already has.
+int plan_single_node(const viprs_image* in, const viprs_image* out, const PlanNode& node, viprs_plan* p) {
+    int st = check_image(in);
+    if (st) return st;
+    if (in->width == 0 || in->height == 0) return VIPRS_ERR_INVALID_ARGUMENT;
+    uint32_t ow, oh;
+    st = node_output_dims(node, in->width, in->height, &ow, &oh);
+    if (st) return st;
+    if (node.kind == NodeKind::ReduceH || node.kind == NodeKind::ReduceV || node.kind == NodeKind::Reduce) {
+        ReduceKernel rk;
+        st = rk.init(node.factor, node.kernel);
+        if (st == VIPRS_OK && node.kind == NodeKind::Reduce) st = rk.init(node.vfactor, node.kernel);
+        if (st) return st;
+    }
+    if (!out) return VIPRS_ERR_NULL_POINTER;
+    if (out->width == 0 || out->height == 0) return VIPRS_ERR_SIZE_MISMATCH;
+    st = check_image(out);
+    if (st) return st;
+    if (in->format != out->format || in->bands != out->bands) return VIPRS_ERR_SIZE_MISMATCH;
+    p->in_w = in->width; p->in_h = in->height; p->bands = in->bands; p->fmt = in->format;
+    p->in_pitch = pitch_of(in);
+    p->out_pitch = pitch_of(out);
+    Chain c;
+    c.nodes.push_back(node);
+    st = build_chain(p, c);
+    if (st) return st;
+    if (p->out_w != out->width || p->out_h != out->height) return VIPRS_ERR_SIZE_MISMATCH;
+    return VIPRS_OK;
+}
 }  // namespace viprs
 
 extern "C" {
@@ -661,6 +694,7 @@ const char* viprs_status_string(int32_t status) {
     case VIPRS_ERR_DEGENERATE_AFFINE: return "affine matrix determinant is singular";
     case VIPRS_ERR_NULL_POINTER: return "null pointer";
     case VIPRS_ERR_SIZE_MISMATCH: return "image size, bands or format mismatch";
+    case VIPRS_ERR_SCRATCH_LIMIT: return "work exceeds the static scratch of the no-alloc entry point";
     default: return "unknown status";
     }
 }

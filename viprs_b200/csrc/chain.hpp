@@ -11,6 +11,7 @@
 #include "affine_launch.hpp"
 #include "launch.hpp"
 #include "plan.hpp"
+#include "viprs_b200.h"
 
 namespace viprs {
 
@@ -70,5 +71,7 @@ void free_plan(viprs_plan* p);
 PlaneArg plane_in_arg(const viprs_plan* p, int idx, const uint8_t* src);
 OutPlaneArg plane_out_arg(const viprs_plan* p, int idx, uint8_t* dst);
 int32_t cuda_status(cudaError_t e);
+// Host-side plan of a one-node chain (no device memory touched); status 0 on success.
+int plan_single_node(const viprs_image* in, const viprs_image* out, const PlanNode& node, viprs_plan* p);
 
 }  // namespace viprs
