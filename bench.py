@@ -1,22 +1,41 @@
 """Benchmark of the resample hot path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--no-cpu] [--no-others] [--cpu-seconds S]
 
-Workload (N=1 default): thumbnail of one 8192x8192x3 u8 image to 400 px width
-(in-memory plan: ShrinkH 19 -> ShrinkV 19 -> ReduceH/ReduceV 1.0779 Lanczos3).
-A step is one execution of the plan on device-resident input; the 201 MB
-input exceeds the 126 MB L2, so no flush is needed between steps.
+Headline workload (the metric "input Mpix/s batched vs per-image GPU (bit-exact
+u8); fwd+bwd GB/s vs HBM"): thumbnails of 512 u8 images of uneven size (width
+log-uniform in 256..6000, aspect w/h uniform in 0.5..2, 3 or 4 bands with
+p = 0.5) to a 256 px FitBox with Lanczos3 — per image the in-memory thumbnail
+chain (premultiply for 4 bands, box shrink, residual Lanczos3 reduce,
+unpremultiply).  A step is one run of the whole batch: ONE persistent kernel
+over a device work list, launched through a CUDA graph, inputs resident in
+HBM (about 9.4 GB, far above the 126 MB L2: no flush needed).  The plain
+per-image GPU path (each image's plan launched in turn) is timed on the same
+images, and the batch output is checked bit-exact against it.
 
-Prints one JSON line.  `value` is input Mpix/s over all ranks (each rank runs
-its own replica: the single-image workload does not shard).  `e2e` is the same
-metric through the public plan API with host buffers (pinned host -> device
-copy of the input and device -> host copy of the thumbnail inside the timed
-region).  `roofline` is the shrink kernel's algorithmic HBM bytes per launch
-divided by its CUDA-event launch time, against the measured copy bandwidth.
-`cpu_baseline` is the CPU restatement of viprs on this host's cores.
+Every rank runs its own 512-image batch (different seeds): `value` is the
+input Mpix/s of all ranks over the max-over-ranks time, scaling "weak"; no
+data crosses between GPUs.
+
+`e2e` is the same batch through ThumbnailBatch.run_host: pinned host images
+copied in, the graph run, thumbnails copied out, every step.  `roofline` is the
+batch kernel's algorithmic bytes (each image's input read once + output written
+once) over its CUDA-event time per launch, against MEASURED_PEAKS.json.
+`cpu_baseline` is the oracle (the C restatement of viprs's CPU path) on all
+host cores over a bounded sample of the batch.  `others` holds the remaining
+configurations: the 8192x8192x3 thumbnail, the 1024x768x3 reduce, the f32
+6000x4000x4 resize, and the fwd+bwd GB/s of the reduce+affine and mapim
+gradient workloads.
+
+`--impl reference` times the reference arm: viprs's CPU path as restated in C
+(viprs itself needs a Rust toolchain this image lacks), all host cores, on a
+bounded sample of the same batch per step.
 """
 import argparse
+import ctypes
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -29,6 +48,12 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 FALLBACK_HBM_GBS = 6650.0
+METRIC = "input Mpix/s batched vs per-image GPU (bit-exact u8); fwd+bwd GB/s vs HBM"
+BATCH_N = 512
+BATCH_SEED = 0x5EED0003
+BATCH_BOX = 256
+WORKLOAD = (f"{BATCH_N} uneven u8 images (w log-U[256,6000], w/h U[0.5,2], 3|4 bands) -> "
+            f"thumbnail FitBox {BATCH_BOX}x{BATCH_BOX} Lanczos3, one persistent launch via CUDA graph")
 
 
 def measured_hbm_peak():
@@ -58,7 +83,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except Exception:
@@ -127,144 +152,366 @@ def max_over_ranks(x, ws):
     return float(t.item())
 
 
-def cpu_baseline_thumbnail(img_np, target_w, seconds=10.0):
-    """The CPU restatement of viprs (oracle port) on all host cores, on the same image."""
+def sum_over_ranks(x, ws):
+    if ws <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def timed(fn, steps, warmup, stream):
+    """Mean CUDA-event ms of fn() over `steps` launches after `warmup`."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for a, b in evs:
+        a.record(stream)
+        fn()
+        b.record(stream)
+    torch.cuda.synchronize()
+    return statistics.mean(a.elapsed_time(b) for a, b in evs)
+
+
+# ----------------------------------------------------------------------------- headline: batched thumbnails
+
+def make_batch_images(seed, n=BATCH_N, device="cuda"):
+    from viprs_b200 import synth
+    shapes = synth.uneven_batch_shapes(BATCH_N, seed)[:n]
+    imgs = [synth.smooth_u8(h, w, b, seed * 1000 + i, device=device) for i, (h, w, b) in enumerate(shapes)]
+    return shapes, imgs
+
+
+def cpu_baseline_batch(host_imgs, seconds):
+    """The oracle (CPU restatement of viprs) on all host cores, image by image
+    over the batch in order, until `seconds` of work."""
     from oracle import oracle as O
     threads = os.cpu_count() or 1
-    O.thumbnail(img_np, "width", target_w, 0, threads=threads)  # warm
-    n = 0
+    O.thumbnail(host_imgs[0], "fitbox", BATCH_BOX, BATCH_BOX, threads=threads)  # warm
+    n, mpix = 0, 0.0
     t0 = time.perf_counter()
     while True:
-        O.thumbnail(img_np, "width", target_w, 0, threads=threads)
+        img = host_imgs[n % len(host_imgs)]
+        O.thumbnail(img, "fitbox", BATCH_BOX, BATCH_BOX, threads=threads)
         n += 1
+        mpix += img.shape[0] * img.shape[1] / 1e6
         el = time.perf_counter() - t0
         if el >= seconds:
             break
-    mpix = img_np.shape[0] * img_np.shape[1] / 1e6
-    return {"value": round(mpix * n / el, 3), "unit": "Mpix/s", "cores": threads, "kind": "port",
-            "sample": f"{n} thumbnails of the same {img_np.shape[1]}x{img_np.shape[0]}x{img_np.shape[2]} u8 "
-                      f"image in {el:.1f} s"}
+    return {"value": round(mpix / el, 3), "unit": "Mpix/s", "cores": threads, "kind": "port",
+            "sample": f"{n} images of the batch ({mpix:.1f} Mpix), one after another, each on all {threads} "
+                      f"threads, {el:.1f} s"}
 
 
-def run_thumbnail(args, rank, ws, local):
+def run_batch(args, rank, ws, local):
     import numpy as np
     import torch
 
-    from viprs_b200 import api, synth
+    from viprs_b200 import api
 
-    H = W = 8192
-    B = 3
-    TW = 400
     torch.cuda.set_device(local)
-    img = synth.smooth_u8(H, W, B, 0x5EED0001 + rank)
-    plan = api.thumbnail_plan(W, H, B, torch.uint8, "width", TW)
-    out = torch.empty(plan.out_shape, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
+    shapes, srcs = make_batch_images(BATCH_SEED + 7919 * rank, args.images)
+    batch = api.ThumbnailBatch(shapes, "fitbox", BATCH_BOX, BATCH_BOX)
+    dsts = batch.alloc_outputs()
+    in_bytes = sum(h * w * b for h, w, b in shapes)
+    out_bytes = sum(h * w * b for h, w, b in batch.out_shapes)
+    mpix = sum(h * w for h, w, _ in shapes) / 1e6
+
+    # the project's autotuner picks the ring size, work-list lag and blocks per SM
+    tuned = batch.autotune(srcs, dsts, repeats=2)[0] if not args.no_autotune else batch.config()
+    items, stages, grid = batch.work()
+
+    # plain per-image GPU path, timed on the same images
+    per = batch.alloc_outputs()
+    per_ms = timed(lambda: batch.run_per_image(srcs, per), max(3, args.steps // 4), 2, stream)
+    _, per_launches = batch.launches()
+
+    # batched: warm-up (captures the graph), then K timed graph launches
     for _ in range(args.warmup):
-        plan(img, out)
+        batch.run(srcs, dsts, graph=True)
     torch.cuda.synchronize()
-    n_st = plan.launches
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
-           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    assert batch.status() == 0, "batch kernel reported an error"
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     sampler = ClockSampler(local)
     sampler.start()
-    time.sleep(0.3)
+    time.sleep(0.25)
     barrier(ws)
     torch.cuda.synchronize()
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
     start.record(stream)
-    for k in range(args.steps):
-        e0, e1, e2 = ev[k]
-        e0.record(stream)
-        plan.run_stages(img, out, 0, 1)
-        e1.record(stream)
-        plan.run_stages(img, out, 1, n_st - 1)
-        e2.record(stream)
+    for a, b in evs:
+        a.record(stream)
+        batch.run(srcs, dsts, graph=True)
+        b.record(stream)
     end.record(stream)
     torch.cuda.synchronize()
     barrier(ws)
     clocks = sampler.stop()
-    total_ms = start.elapsed_time(end)
-    total_ms = max_over_ranks(total_ms, ws)
-    shrink_ms = statistics.mean(e0.elapsed_time(e1) for e0, e1, _ in ev)
-    mpix = H * W / 1e6
-    value = mpix * args.steps * ws / (total_ms / 1e3)
+    assert batch.status() == 0, "batch kernel reported an error"
+    total_ms = max_over_ranks(start.elapsed_time(end), ws)
+    kernel_ms = statistics.mean(a.elapsed_time(b) for a, b in evs)
+    all_mpix = sum_over_ranks(mpix, ws)
+    value = all_mpix * args.steps / (total_ms / 1e3)
+    per_value = mpix / (per_ms / 1e3)
 
-    # algorithmic bytes of the shrink launch: the 8189x8189 source pixels the
-    # 19x19 box shrink needs, read once, plus the shrunk plane written once
-    fh = 19
-    need = (W // fh) * fh
-    shrink_bytes = need * need * B + (W // fh) * (H // fh) * B
-    achieved = shrink_bytes / (shrink_ms / 1e3) / 1e9
-    peak, peak_kind = measured_hbm_peak()
+    same = all(torch.equal(a, b) for a, b in zip(dsts, per))
 
-    # end to end through the public API from pinned host memory
-    host_in = img.cpu().pin_memory()
-    host_out = torch.empty(plan.out_shape, dtype=torch.uint8).pin_memory()
-    for _ in range(max(1, args.warmup)):
-        plan.execute_host(host_in, host_out)
+    # end to end from pinned host memory through ThumbnailBatch.run_host
+    host_srcs = [s.cpu().pin_memory() for s in srcs]
+    host_dsts = [torch.empty(s, dtype=torch.uint8).pin_memory() for s in batch.out_shapes]
+    e2e_steps = max(3, min(args.steps, 10))
+    batch.run_host(host_srcs, host_dsts, srcs, dsts)
     barrier(ws)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        plan.execute_host(host_in, host_out)
-    torch.cuda.synchronize()
+    for _ in range(e2e_steps):
+        batch.run_host(host_srcs, host_dsts, srcs, dsts)
     e2e_s = max_over_ranks(time.perf_counter() - t0, ws)
-    e2e_value = mpix * args.steps * ws / e2e_s
+    e2e_value = all_mpix * e2e_steps / e2e_s
+    same = same and all(torch.equal(h, d.cpu()) for h, d in zip(host_dsts, dsts))
 
-    ok = np.array_equal(out.cpu().numpy(), host_out.numpy())
+    peak, peak_kind = measured_hbm_peak()
+    alg = in_bytes + out_bytes
+    achieved = alg / (kernel_ms / 1e3) / 1e9
     line = {
-        "metric": "thumbnail input Mpix/s (8192x8192x3 u8 -> 400 px, bit-exact vs viprs CPU path)",
-        "value": round(value, 2), "unit": "Mpix/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded smooth sinusoids + noise, generated on device)",
-        "config": {"workload": "thumbnail 8192x8192x3 u8 -> 400x400 (shrink 19 + Lanczos3 reduce 1.0779)",
-                   "parallelism": f"replicas x{ws}", "l2": "input 201 MB > 126 MB L2 (no flush needed)"},
-        "gpu_launches": n_st * args.steps,
-        "e2e": {"value": round(e2e_value, 2), "unit": "Mpix/s", "h2d_bytes_per_step": H * W * B,
-                "d2h_bytes_per_step": int(np.prod(plan.out_shape))},
+        "metric": METRIC, "value": round(value, 2), "unit": "Mpix/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded smooth sinusoids + uniform noise, generated on device)",
+        "config": {"workload": WORKLOAD if args.images == BATCH_N else f"first {args.images} images of: {WORKLOAD}",
+                   "images_per_gpu": args.images, "input_bytes_per_gpu": in_bytes,
+                   "input_mpix_per_gpu": round(mpix, 2), "parallelism": f"independent batch per GPU x{ws}",
+                   "l2": f"inputs {in_bytes / 1e9:.1f} GB >> 126 MB L2 (no flush needed)",
+                   "autotuned": tuned, "work_items": items, "stages": stages, "grid": grid},
+        "gpu_launches": args.steps,
+        "per_image": {"value": round(per_value, 2), "unit": "Mpix/s", "ms_per_step": round(per_ms, 4),
+                      "launches_per_step": per_launches},
+        "batched_over_per_image": round(value / ws / per_value, 3),
+        "e2e": {"value": round(e2e_value, 2), "unit": "Mpix/s", "h2d_bytes_per_step": in_bytes,
+                "d2h_bytes_per_step": out_bytes, "path": "ThumbnailBatch.run_host (pinned host buffers)"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
-                     "kernel": "shrink2d_kernel<u8,HV>", "kernel_ms": round(shrink_ms, 4),
-                     "algorithmic_bytes": shrink_bytes},
+                     "kernel": "batch_kernel", "kernel_ms": round(kernel_ms, 4), "algorithmic_bytes": alg},
         "clocks": clocks,
-        "parity": "device result equals host-path result" if ok else "MISMATCH",
+        "parity": "batched == per-image path (bit-exact)" if same else "MISMATCH",
     }
     if rank == 0 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_baseline_thumbnail(img.cpu().numpy(), TW, args.cpu_seconds)
+        sample = [s.cpu().numpy() for s in srcs[:64]]
+        line["cpu_baseline"] = cpu_baseline_batch(sample, args.cpu_seconds)
+    del host_srcs, host_dsts
     return line
 
 
+# ----------------------------------------------------------------------------- the other configurations
+
+def other_thumbnail_8192(stream, steps):
+    import torch
+
+    from viprs_b200 import api, synth
+    H = W = 8192
+    img = synth.smooth_u8(H, W, 3, 0x5EED0001)
+    plan = api.thumbnail_plan(W, H, 3, torch.uint8, "width", 400)
+    out = torch.empty(plan.out_shape, dtype=torch.uint8, device="cuda")
+    total = timed(lambda: plan(img, out), steps, 3, stream)
+    shrink = timed(lambda: plan.run_stages(img, out, 0, 1), steps, 3, stream)
+    need = (W // 19) * 19
+    sb = need * need * 3 + (W // 19) * (H // 19) * 3
+    peak, _ = measured_hbm_peak()
+    return {"workload": "thumbnail 8192x8192x3 u8 -> 400 px (shrink 19 + Lanczos3 1.0779)",
+            "mpix_per_s": round(H * W / 1e6 / (total / 1e3), 1), "ms": round(total, 4), "launches": plan.launches,
+            "shrink_kernel": {"ms": round(shrink, 4), "algorithmic_bytes": sb,
+                              "gbs": round(sb / (shrink / 1e3) / 1e9, 1),
+                              "frac": round(sb / (shrink / 1e3) / 1e9 / peak, 4)}}
+
+
+def other_reduce_1024(stream, steps):
+    import torch
+
+    from viprs_b200 import api, synth
+    img = synth.smooth_u8(768, 1024, 3, 0x5EED0000)
+    plan = api.PipelineBuilder(1024, 768, 3, torch.uint8).reduce_h(4.0).reduce_v(4.0).build()
+    out = torch.empty(plan.out_shape, dtype=torch.uint8, device="cuda")
+    ms = timed(lambda: plan(img, out), steps, 3, stream)
+    b = 1024 * 768 * 3 + 256 * 192 * 3
+    return {"workload": "reduce_h(4)+reduce_v(4) Lanczos3 1024x768x3 u8 (single launch, latency-bound)",
+            "mpix_per_s": round(0.786432 / (ms / 1e3), 1), "us": round(ms * 1e3, 2), "algorithmic_bytes": b,
+            "gbs": round(b / (ms / 1e3) / 1e9, 1)}
+
+
+def other_resize_f32(stream, steps):
+    import torch
+
+    from viprs_b200 import api, synth
+    img = synth.uniform_f32(4000, 6000, 4, 0x5EED0002)
+    plan = api.resize_plan(6000, 4000, 4, torch.float32, 0.37)
+    out = torch.empty(plan.out_shape, dtype=torch.float32, device="cuda")
+    ms = timed(lambda: plan(img, out), steps, 3, stream)
+    b = 6000 * 4000 * 16 + out.numel() * 4
+    peak, _ = measured_hbm_peak()
+    return {"workload": "resize 0.37 Lanczos3 6000x4000x4 f32 (ReduceV+ReduceH 2.7027 fused)",
+            "mpix_per_s": round(24.0 / (ms / 1e3), 1), "ms": round(ms, 4), "algorithmic_bytes": b,
+            "gbs": round(b / (ms / 1e3) / 1e9, 1), "frac": round(b / (ms / 1e3) / 1e9 / peak, 4),
+            "launches": plan.launches}
+
+
+def other_reduce_affine_grad(stream, steps):
+    """16 x 1024^2 x 4 f32: reduce_h(2)+reduce_v(2) -> affine bilinear 512^2 (alpha path), fwd + bwd."""
+    import torch
+
+    from viprs_b200 import _native as N
+    from viprs_b200 import api, synth
+    n = 16
+    g = torch.Generator().manual_seed(0x5EED0004)
+    xs = [synth.uniform_f32(1024, 1024, 4, 0x5EED0004 + i) for i in range(n)]
+    gys = [torch.randn((512, 512, 4), device="cuda") for _ in range(n)]
+    plan = api.PipelineBuilder(1024, 1024, 4, torch.float32).reduce_h(2.0).reduce_v(2.0).build()
+    zs = [torch.empty(plan.out_shape, device="cuda") for _ in range(n)]
+    ys = [torch.empty((512, 512, 4), device="cuda") for _ in range(n)]
+    gzs = [torch.empty(plan.out_shape, device="cuda") for _ in range(n)]
+    gxs = [torch.empty((1024, 1024, 4), device="cuda") for _ in range(n)]
+    gms = torch.empty((n, 6), dtype=torch.float64, device="cuda")
+    mats = []
+    for _ in range(n):
+        th = math.radians(-30 + 60 * float(torch.rand(1, generator=g)))
+        s = 0.8 + 0.6 * float(torch.rand(1, generator=g))
+        t = (-20 + 40 * torch.rand(2, generator=g)).tolist()
+        M = [s * math.cos(th), -s * math.sin(th), s * math.sin(th), s * math.cos(th)]
+        # about the image centre: output centre = M (input centre) + translation
+        c = 256.0
+        tx = c + t[0] - (M[0] * c + M[1] * c)
+        ty = c + t[1] - (M[2] * c + M[3] * c)
+        bm, btx, bty = api.forward_affine_to_backward(M, tx, ty)
+        mats.append(((ctypes.c_double * 4)(*bm), btx, bty))
+    L = N.lib()
+    sp = api._stream()
+
+    def fwd():
+        for i in range(n):
+            plan(xs[i], zs[i])
+            m, btx, bty = mats[i]
+            N.check(L.viprs_affine_backward_matrix(api.image(zs[i]), api.image(ys[i]), m, btx, bty, 1, 2, 0.0, 0,
+                                                   0, 0, sp), "affine")
+
+    def bwd():
+        for i in range(n):
+            m, btx, bty = mats[i]
+            N.check(L.viprs_affine_grad(api.image(zs[i]), api.image(gys[i]), api.image(gzs[i]), m, btx, bty, 1, 2,
+                                        0.0, 0, 0, 0, 0, ctypes.c_void_p(gms[i].data_ptr()), sp), "affine_grad")
+            N.check(L.viprs_reduce_hv_adjoint(api.image(gzs[i]), api.image(gxs[i]), 2.0, 2.0, 9, sp),
+                    "reduce_hv_adjoint")
+
+    fwd_ms = timed(fwd, steps, 3, stream)
+    bwd_ms = timed(bwd, steps, 3, stream)
+    alg = 738197504
+    peak, _ = measured_hbm_peak()
+    gbs = alg / ((fwd_ms + bwd_ms) / 1e3) / 1e9
+    return {"workload": "16 x 1024^2x4 f32: reduce_h(2)+reduce_v(2) L3 -> affine(s R(theta), t) bilinear 512^2, "
+                        "fwd + bwd (image and matrix gradients, f32-atomic scatter)",
+            "fwd_ms": round(fwd_ms, 4), "bwd_ms": round(bwd_ms, 4), "algorithmic_bytes_fwd_bwd": alg,
+            "gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}
+
+
+def other_mapim_grad(stream, steps):
+    """4096^2 f32 source, identity grid + smooth displacement (max 8 px), bicubic, fwd + bwd."""
+    import torch
+    import torch.nn.functional as F
+
+    from viprs_b200 import _native as N
+    from viprs_b200 import api, synth
+    S = 4096
+    src = synth.uniform_f32(S, S, 1, 0x5EED0005)
+    g = torch.Generator(device="cuda").manual_seed(0x5EED0005)
+    noise = torch.randn((2, 1, S, S), generator=g, device="cuda")
+    sigma, r = 32.0, 96
+    k = torch.exp(-0.5 * (torch.arange(-r, r + 1, device="cuda", dtype=torch.float32) / sigma) ** 2)
+    k = (k / k.sum()).view(1, 1, 1, -1)
+    d = F.conv2d(F.conv2d(noise, k, padding=(0, r)), k.view(1, 1, -1, 1), padding=(r, 0))[:, 0]
+    d = d * (8.0 / d.abs().max())
+    yy, xx = torch.meshgrid(torch.arange(S, device="cuda", dtype=torch.float32),
+                            torch.arange(S, device="cuda", dtype=torch.float32), indexing="ij")
+    index = torch.stack([xx + d[0], yy + d[1]], dim=2).contiguous()
+    out = torch.empty((S, S, 1), device="cuda")
+    gy = torch.randn((S, S, 1), device="cuda")
+    gs = torch.empty_like(src)
+    gi = torch.empty_like(index)
+    L = N.lib()
+    sp = api._stream()
+
+    def fwd():
+        N.check(L.viprs_mapim(api.image(src), api.image(index), api.image(out), 2, 0, 0.0, 0, sp), "mapim")
+
+    def bwd(det):
+        N.check(L.viprs_mapim_grad(api.image(src), api.image(index), api.image(gy), api.image(gs), api.image(gi),
+                                   2, 0, 0.0, 0, det, sp), "mapim_grad")
+
+    fwd_ms = timed(fwd, steps, 3, stream)
+    bwd_ms = timed(lambda: bwd(0), steps, 3, stream)
+    det_ms = timed(lambda: bwd(1), steps, 3, stream)
+    alg = 738197504
+    peak, _ = measured_hbm_peak()
+    gbs = alg / ((fwd_ms + bwd_ms) / 1e3) / 1e9
+    return {"workload": "mapim bicubic 4096^2x1 f32, index = identity + Gaussian(sigma 32)-smoothed displacement "
+                        "(max 8 px), fwd + bwd (image and coordinate gradients)",
+            "fwd_ms": round(fwd_ms, 4), "bwd_ms_atomic": round(bwd_ms, 4), "bwd_ms_deterministic": round(det_ms, 4),
+            "algorithmic_bytes_fwd_bwd": alg, "gbs": round(gbs, 1), "frac": round(gbs / peak, 4),
+            "forward_only_gbs": round(268435456 / (fwd_ms / 1e3) / 1e9, 1)}
+
+
+def run_others(steps):
+    import torch
+    stream = torch.cuda.current_stream()
+    out = {}
+    for name, fn in (("thumbnail_8192", other_thumbnail_8192), ("reduce_1024x768", other_reduce_1024),
+                     ("resize_f32_6000x4000", other_resize_f32), ("reduce_affine_fwd_bwd", other_reduce_affine_grad),
+                     ("mapim_fwd_bwd", other_mapim_grad)):
+        try:
+            out[name] = fn(stream, steps)
+        except Exception as e:  # reported, never hidden
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        torch.cuda.empty_cache()
+    return out
+
+
+# ----------------------------------------------------------------------------- reference arm
+
 def run_reference(args, rank, ws):
     """Reference arm: viprs's CPU path restated in C (viprs itself needs a Rust
-    toolchain that this image lacks), on all host cores, same workload."""
-    import numpy as np
+    toolchain that this image lacks), on all host cores.  Each step is a bounded
+    sample of the batch: 16 of its images, generated on the host."""
     if rank != 0:
         return None
     from oracle import oracle as O
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    rng = np.random.default_rng(0x5EED0001)
-    # a host-generated image of the workload's shape and distribution
-    from gpu_helpers import smooth_image
-    img = smooth_image(rng, 8192, 8192, 3)
+    from viprs_b200 import synth
+    shapes = synth.uneven_batch_shapes(BATCH_N, BATCH_SEED)
+    picks = list(range(0, BATCH_N, BATCH_N // 16))[:16]
+    imgs = [synth.smooth_u8(*shapes[i], BATCH_SEED * 1000 + i, device="cpu").numpy() for i in picks]
+    mpix = sum(im.shape[0] * im.shape[1] for im in imgs) / 1e6
     threads = os.cpu_count() or 1
+
+    def step():
+        for im in imgs:
+            O.thumbnail(im, "fitbox", BATCH_BOX, BATCH_BOX, threads=threads)
+
     for _ in range(args.warmup):
-        O.thumbnail(img, "width", 400, 0, threads=threads)
+        step()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        O.thumbnail(img, "width", 400, 0, threads=threads)
+        step()
     el = time.perf_counter() - t0
-    v = 8192 * 8192 / 1e6 * args.steps / el
+    v = mpix * args.steps / el
+    sample = f"16 of the 512 batch images ({mpix:.1f} Mpix) per step, each on all {threads} threads"
     return {
-        "metric": "thumbnail input Mpix/s (8192x8192x3 u8 -> 400 px, bit-exact vs viprs CPU path)",
-        "value": round(v, 3), "unit": "Mpix/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(el * 1e3 / args.steps, 3), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded smooth sinusoids + noise)",
-        "config": {"workload": "thumbnail 8192x8192x3 u8 -> 400x400 (shrink 19 + Lanczos3 reduce 1.0779)",
-                   "parallelism": "host threads"},
+        "metric": METRIC, "value": round(v, 3), "unit": "Mpix/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(el * 1e3 / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded smooth sinusoids + noise)",
+        "config": {"workload": WORKLOAD, "parallelism": "host threads", "sample": sample},
         "impl": "reference",
-        "cpu_baseline": {"value": round(v, 3), "unit": "Mpix/s", "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} thumbnails of one 8192x8192x3 u8 image"},
+        "cpu_baseline": {"value": round(v, 3), "unit": "Mpix/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": round(v, 3), "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -276,9 +523,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-others", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--images", type=int, default=BATCH_N, help="first N images of the batch (profiling cases)")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default kernel configuration")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    args.steps = max(args.steps, 1)
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))
         ws = int(os.environ.get("WORLD_SIZE", "1"))
@@ -287,7 +538,9 @@ def main():
             print(json.dumps(line), flush=True)
         return
     rank, ws, local = dist_setup()
-    line = run_thumbnail(args, rank, ws, local)
+    line = run_batch(args, rank, ws, local)
+    if rank == 0 and not args.no_others:
+        line["others"] = run_others(10)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:

@@ -305,9 +305,10 @@ int32_t viprs_reduce_hv_adjoint(const viprs_image *grad_out, const viprs_image *
    (grad_in, may be NULL; f32 atomics, or with `deterministic` a fixed-point
    2^-32 accumulator whose integer adds make the result independent of order)
    and wrt the backward matrix and translation (grad_matrix[6] =
-   d/d(b0, b1, b2, b3, tx, ty), HOST memory, may be NULL; the call then
-   synchronises `stream`).  4-band images without `premultiplied` take the
-   alpha-premultiplying sampler's derivative. */
+   d/d(b0, b1, b2, b3, tx, ty), DEVICE memory, may be NULL; written on
+   `stream` by a fixed-order reduction of per-block partial sums).  4-band
+   images without `premultiplied` take the alpha-premultiplying sampler's
+   derivative. */
 int32_t viprs_affine_grad(const viprs_image *in, const viprs_image *grad_out,
                           const viprs_image *grad_in, const double backward[4], double tx,
                           double ty, int32_t kernel, int32_t extend, double background,

@@ -170,13 +170,13 @@ def _rot_backward(theta, s, in_w, in_h, out_w, out_h):
 
 def _affine_grad_raw(x, gy, bm, bt, extend, bg, premul, det, want_x=True):
     gx = torch.empty_like(x) if want_x else None
-    g6 = (ctypes.c_double * 6)()
+    g6 = torch.empty(6, dtype=torch.float64, device=x.device)
     mm = (ctypes.c_double * 4)(*bm)
     st = N.lib().viprs_affine_grad(api.image(x), api.image(gy), api.image(gx) if want_x else None, mm, bt[0],
-                                   bt[1], 1, api.EXTEND[extend], bg, int(premul), 0, 0, int(det), g6,
-                                   api._stream())
+                                   bt[1], 1, api.EXTEND[extend], bg, int(premul), 0, 0, int(det),
+                                   ctypes.c_void_p(g6.data_ptr()), api._stream())
     N.check(st, "affine_grad")
-    return gx, list(g6)
+    return gx, g6.cpu().tolist()
 
 
 AFFINE_GEOMS = {

@@ -93,8 +93,7 @@ SIGNATURES = {
     "viprs_reduce_noalloc": (_I, [_IMG, _IMG, _D, _D, _I, _P]),
     "viprs_reduce_adjoint": (_I, [_IMG, _IMG, _D, _I, _I, _P]),
     "viprs_reduce_hv_adjoint": (_I, [_IMG, _IMG, _D, _D, _I, _P]),
-    "viprs_affine_grad": (_I, [_IMG, _IMG, _IMG, ctypes.POINTER(_D), _D, _D, _I, _I, _D, _I, _U, _U, _I,
-                               ctypes.POINTER(_D), _P]),
+    "viprs_affine_grad": (_I, [_IMG, _IMG, _IMG, ctypes.POINTER(_D), _D, _D, _I, _I, _D, _I, _U, _U, _I, _P, _P]),
     "viprs_mapim_grad": (_I, [_IMG, _IMG, _IMG, _IMG, _IMG, _I, _I, _D, _I, _I, _P]),
 }
 

@@ -436,6 +436,18 @@ class ThumbnailBatch:
                 "batch_execute")
         return dsts
 
+    def run_host(self, host_srcs, host_dsts, dev_srcs, dev_dsts, graph=True):
+        """Host buffers in and out: copy every (pinned) host image to its device
+        buffer, run the batch, copy the thumbnails back, all on the current
+        stream, then synchronise."""
+        for h, d in zip(host_srcs, dev_srcs):
+            d.copy_(h, non_blocking=True)
+        self.run(dev_srcs, dev_dsts, graph=graph)
+        for d, h in zip(dev_dsts, host_dsts):
+            h.copy_(d, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return host_dsts
+
     def run_per_image(self, srcs, dsts=None):
         dsts = self.alloc_outputs(srcs[0].device) if dsts is None else dsts
         hs = (ctypes.c_uint64 * len(srcs))(*[t.data_ptr() for t in srcs])

@@ -116,12 +116,13 @@ class _AffineBackwardFn(torch.autograd.Function):
         need_x = ctx.needs_input_grad[0]
         need_m = ctx.needs_input_grad[1] or ctx.needs_input_grad[2]
         gx = torch.empty_like(x) if need_x else None
-        gm = (ctypes.c_double * 6)()
+        gm = torch.empty(6, dtype=torch.float64, device=x.device) if need_m else None
         mm = (ctypes.c_double * 4)(*m)
         N.check(N.lib().viprs_affine_grad(_img(x), _img(gy), _img(gx) if need_x else None, mm, t[0], t[1],
                                           api.KERNELS["bilinear"], extend, bg, premul, 0, 0, det,
-                                          gm if need_m else None, api._stream()), "affine_grad")
-        g6 = torch.tensor(list(gm), dtype=mdt, device=mdev) if need_m else None
+                                          ctypes.c_void_p(gm.data_ptr()) if need_m else None, api._stream()),
+                "affine_grad")
+        g6 = gm.to(device=mdev, dtype=mdt) if need_m else None
         return (gx, g6[:4] if need_m else None, g6[4:] if need_m else None, None, None, None, None, None, None)
 
 

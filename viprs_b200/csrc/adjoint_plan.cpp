@@ -265,12 +265,7 @@ int32_t viprs_affine_grad(const viprs_image* in, const viprs_image* grad_out, co
     e = launch::affine_grad(g, blocks, s);
     if (e == cudaSuccess && grad_in && deterministic)
         e = launch::fixed_to_f32(g.g_fixed, static_cast<float*>(grad_in->data), n_in, 1.0 / g.fixed_scale, s);
-    if (e == cudaSuccess && grad_matrix) {
-        double* d6 = sc.alloc<double>(6, &e);
-        if (e == cudaSuccess) e = launch::sum_partials(g.partial, blocks, d6, s);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(grad_matrix, d6, 6 * sizeof(double), cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    }
+    if (e == cudaSuccess && grad_matrix) e = launch::sum_partials(g.partial, blocks, grad_matrix, s);
     return cuda_status(e);
 }
 
