@@ -26,16 +26,20 @@ __device__ __forceinline__ int32_t ld_acquire_i32(const int32_t* p) {
 
 constexpr int kRing = 4;
 
-// One interior (output row, column chunk) shrink item through the TMA ring.
-// `pos` counts ring loads issued so far by this block (identical in every
-// thread).  Returns false on a timed-out copy.
+// One interior shrink item -- output rows [oy0, oy1) of a column chunk --
+// through the TMA ring.  The item's source rows are consecutive plane rows
+// (oy0 * fv + k), so the ring streams them without a break at output-row
+// boundaries.  `pos` counts ring loads issued so far by this block (identical
+// in every thread).  Returns false on a timed-out copy.
 template <int B>
-__device__ bool batch_shrink_interior(const ShrinkArgs& a, int32_t oy, int32_t c0, int32_t ncols, uint64_t* bars,
-                                      uint8_t* bufs, uint32_t stage_bytes, int64_t& pos, volatile int32_t* flag) {
+__device__ bool batch_shrink_interior(const ShrinkArgs& a, int32_t oy0, int32_t oy1, int32_t c0, int32_t ncols,
+                                      uint64_t* bars, uint8_t* bufs, uint32_t stage_bytes, int64_t& pos,
+                                      volatile int32_t* flag) {
     const int32_t fh = int32_t(a.fh), fv = int32_t(a.fv);
     const int64_t sbase = ((a.out.x0 + c0) * (int64_t)fh - a.in.x0) * B;
-    const int64_t row0 = (a.out.y0 + oy) * (int64_t)fv - a.in.y0;
+    const int64_t row0 = (a.out.y0 + oy0) * (int64_t)fv - a.in.y0;
     const int32_t nbytes = ncols * fh * B;
+    const int32_t total = (oy1 - oy0) * fv;
     auto span = [&](int32_t k, int64_t* as, uint32_t* bytes, int32_t* lead) {
         int64_t ly = row0 + k;
         ly = ly < 0 ? 0 : (ly >= a.in.h ? a.in.h - 1 : ly);
@@ -51,16 +55,18 @@ __device__ bool batch_shrink_interior(const ShrinkArgs& a, int32_t oy, int32_t c
         mbar_arrive_expect_tx(&bars[st], bytes);
         bulk_load(bufs + (size_t)st * stage_bytes, a.in.data + as, bytes, &bars[st]);
     };
-    const int32_t first = fv < kRing ? fv : kRing;
+    const int32_t first = total < kRing ? total : kRing;
     if (threadIdx.x == 0)
         for (int32_t k = 0; k < first; ++k) issue(k);
     uint32_t vacc[B];
 #pragma unroll
     for (int b = 0; b < B; ++b) vacc[b] = 0;
     const int32_t x = threadIdx.x;
+    const uint32_t hhalf = uint32_t(fh) / 2;
+    const bool hmult = a.hmode == 3;
     bool ok = true;
-    int32_t k = 0;
-    for (; k < fv; ++k) {
+    int32_t k = 0, kv = 0, oy = oy0;
+    for (; k < total; ++k) {
         const int st = int((pos + k) & (kRing - 1));
         const uint32_t parity = uint32_t(((pos + k) / kRing) & 1);
         if (threadIdx.x == 0 && !mbar_wait(&bars[st], parity)) *flag = 1;
@@ -76,46 +82,58 @@ __device__ bool batch_shrink_interior(const ShrinkArgs& a, int32_t oy, int32_t c
         if (x < ncols) {
             uint32_t sums[B];
             box_sums_u8<B>(row + x * fh * B, fh, sums);
+            if (hmult) {
 #pragma unroll
-            for (int b = 0; b < B; ++b) vacc[b] += round_mode_u8(sums[b], a.hmode, uint32_t(fh), a.hmult);
+                for (int b = 0; b < B; ++b) vacc[b] += round_mult_u8(sums[b], hhalf, a.hmult);
+            } else {
+#pragma unroll
+                for (int b = 0; b < B; ++b) vacc[b] += round_mode_u8(sums[b], a.hmode, uint32_t(fh), a.hmult);
+            }
         }
         __syncthreads();
-        if (threadIdx.x == 0 && k + kRing < fv) {
+        if (threadIdx.x == 0 && k + kRing < total) {
             fence_proxy_async_smem();
             issue(k + kRing);
+        }
+        if (++kv == fv) {
+            if (x < ncols) {
+                uint8_t o[B];
+#pragma unroll
+                for (int b = 0; b < B; ++b) o[b] = (uint8_t)round_mode_u8(vacc[b], a.vmode, uint32_t(fv), a.vmult);
+                if (a.unpremul_out) {
+#pragma unroll
+                    for (int b = 0; b < B - 1; ++b) o[b] = (uint8_t)unpremultiply_u8(o[b], o[B - 1]);
+                }
+                uint8_t* dst = a.out.data + (int64_t)oy * a.out.pitch + (int64_t)(c0 + x) * B;
+#pragma unroll
+                for (int b = 0; b < B; ++b) dst[b] = o[b];
+            }
+#pragma unroll
+            for (int b = 0; b < B; ++b) vacc[b] = 0;
+            kv = 0;
+            ++oy;
         }
     }
     if (!ok) {
         // wait (bounded) for the copies of this item still in flight
         if (threadIdx.x == 0) {
-            const int32_t last = (k + kRing < fv) ? k + kRing : fv;
+            const int32_t last = (k + kRing < total) ? k + kRing : total;
             for (int32_t kk = k + 1; kk < last; ++kk)
                 mbar_wait(&bars[(pos + kk) & (kRing - 1)], uint32_t(((pos + kk) / kRing) & 1));
         }
         __syncthreads();
         return false;
     }
-    pos += fv;
-    if (x < ncols) {
-        uint8_t o[B];
-#pragma unroll
-        for (int b = 0; b < B; ++b) o[b] = (uint8_t)round_mode_u8(vacc[b], a.vmode, uint32_t(fv), a.vmult);
-        if (a.unpremul_out) {
-#pragma unroll
-            for (int b = 0; b < B - 1; ++b) o[b] = (uint8_t)unpremultiply_u8(o[b], o[B - 1]);
-        }
-        uint8_t* dst = a.out.data + (int64_t)oy * a.out.pitch + (int64_t)(c0 + x) * B;
-#pragma unroll
-        for (int b = 0; b < B; ++b) dst[b] = o[b];
-    }
+    pos += total;
     return true;
 }
 
 template <int B>
 __device__ bool batch_shrink_item(const BatchStage& st, const ShrinkArgs& a, int32_t index, uint64_t* bars,
                                   uint8_t* work, uint32_t stage_bytes, int64_t& pos, volatile int32_t* flag) {
-    const int32_t oy = index / st.n_chunks;
-    int32_t c = index - oy * st.n_chunks;
+    const int32_t band = index / st.n_chunks;
+    int32_t c = index - band * st.n_chunks;
+    const int32_t oy0 = band * st.rows_per_item, oy1 = min(a.out.h, oy0 + st.rows_per_item);
     const int32_t left = st.lo > 0 ? 1 : 0;
     const int32_t n_int = st.hi > st.lo ? (st.hi - st.lo + st.chunk_cols - 1) / st.chunk_cols : 0;
     int32_t c0, c1;
@@ -126,14 +144,15 @@ __device__ bool batch_shrink_item(const BatchStage& st, const ShrinkArgs& a, int
         c1 = min(st.hi, c0 + st.chunk_cols);
         interior = true;
     } else { c0 = st.hi; c1 = a.out.w; }
-    if (c1 <= c0) return true;
+    if (c1 <= c0 || oy1 <= oy0) return true;
     // the bulk copy needs a 16-byte aligned source buffer
     if (interior && (reinterpret_cast<uintptr_t>(a.in.data) & 15) == 0)
-        return batch_shrink_interior<B>(a, oy, c0, c1 - c0, bars, work, stage_bytes, pos, flag);
+        return batch_shrink_interior<B>(a, oy0, oy1, c0, c1 - c0, bars, work, stage_bytes, pos, flag);
     // edge (or unaligned) columns: clamped loads, a few columns at a time
     const int32_t per_col = int32_t(a.fv) * int32_t(a.fh) * B;
     const int32_t step = max(1, int32_t((kRing * stage_bytes - 64) / (per_col + B)));
-    for (int32_t x0 = c0; x0 < c1; x0 += step) shrink_edge_item_u8<B>(a, oy, x0, min(c1, x0 + step), work);
+    for (int32_t oy = oy0; oy < oy1; ++oy)
+        for (int32_t x0 = c0; x0 < c1; x0 += step) shrink_edge_item_u8<B>(a, oy, x0, min(c1, x0 + step), work);
     return true;
 }
 
@@ -219,7 +238,10 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchArgs g) {
             break;
         case kBatchReduce2D: {
             const int nbx = (s.r2.out.w + s.r2.tile_w - 1) / s.r2.tile_w;
-            reduce2d_tile<uint8_t, kReduceFixed, kReduceFixed>(s.r2, it.index % nbx, it.index / nbx, work);
+            const int tbx = it.index % nbx, tby = it.index / nbx;
+            if (s.r2.bands == 3) reduce2d_tile<uint8_t, kReduceFixed, kReduceFixed, 3>(s.r2, tbx, tby, work);
+            else if (s.r2.bands == 4) reduce2d_tile<uint8_t, kReduceFixed, kReduceFixed, 4>(s.r2, tbx, tby, work);
+            else reduce2d_tile<uint8_t, kReduceFixed, kReduceFixed, 0>(s.r2, tbx, tby, work);
             break;
         }
         case kBatchAffine:

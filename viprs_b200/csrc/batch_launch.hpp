@@ -29,8 +29,8 @@ struct BatchStage {
     int32_t n_items = 0;
     int32_t dep = -1;      // stage whose completion this stage waits for
     int32_t dep_items = 0; // that stage's item count
-    // shrink items: chunk layout over the output columns
-    int32_t lo = 0, hi = 0, chunk_cols = 1, n_chunks = 1;
+    // shrink items: chunk layout over the output columns, output rows per item
+    int32_t lo = 0, hi = 0, chunk_cols = 1, n_chunks = 1, rows_per_item = 1;
     // reduce h/v items: samples per item
     int32_t per_item = 256;
     ShrinkArgs sh;

@@ -29,6 +29,8 @@ struct viprs_batch {
     uint32_t ring_target = 8192;  // source bytes per shrink row segment
     int32_t lag_blocks = 2;       // work-list lag between an image's stages, in grids
     int32_t blocks_per_sm = 0;    // 0 = occupancy maximum
+    uint32_t reduce_smem_budget = 48 * 1024;  // shared memory of one fused-reduce tile
+    int64_t item_bytes = 96 * 1024;           // source bytes per shrink work item
     // device work list
     std::vector<BatchStage> stages;
     std::vector<WorkItem> items;
@@ -96,7 +98,11 @@ int plan_stages(viprs_batch* b, int image, std::vector<std::vector<BatchStage>>*
             bs.chunk_cols = int32_t(std::max<int64_t>(1, std::min<int64_t>(256, b->ring_target / std::max<int64_t>(per_col, 1))));
             const int32_t n_int = hi > lo ? (hi - lo + bs.chunk_cols - 1) / bs.chunk_cols : 0;
             bs.n_chunks = (lo > 0 ? 1 : 0) + n_int + (hi < outp.w ? 1 : 0);
-            bs.n_items = outp.h * bs.n_chunks;
+            // output rows per item: about `item_bytes` of source per item, so
+            // that the ring's start-up latency is paid once per many rows
+            const int64_t row_src = int64_t(bs.chunk_cols) * per_col * bs.sh.fv;
+            bs.rows_per_item = int32_t(std::max<int64_t>(1, std::min<int64_t>(outp.h, b->item_bytes / std::max<int64_t>(row_src, 1))));
+            bs.n_items = ((outp.h + bs.rows_per_item - 1) / bs.rows_per_item) * bs.n_chunks;
             const uint32_t need = uint32_t((bs.chunk_cols * per_col + 32 + 15 + 127) / 128 * 128);
             b->ring_stage_bytes = std::max(b->ring_stage_bytes, need);
             // the edge routine stages fv x fh source pixels of one output column in the ring
@@ -117,6 +123,12 @@ int plan_stages(viprs_batch* b, int image, std::vector<std::vector<BatchStage>>*
             bs.r2.phases_v = p->d_tables + st.phases2_off;
             bs.r2.coeffs_h = p->d_tables + st.coeffs_off;
             bs.r2.coeffs_v = p->d_tables + st.coeffs2_off;
+            // many images keep every SM busy: take the largest tile (least halo
+            // work) within the batch's shared-memory budget
+            if (!launch::reduce2d_configure(&bs.r2, reinterpret_cast<const int32_t*>(p->host_tables.data() + st.starts_off),
+                                            reinterpret_cast<const int32_t*>(p->host_tables.data() + st.starts2_off),
+                                            in.x0, in.y0, in.w, in.h, 0, b->reduce_smem_budget))
+                return VIPRS_ERR_UNSUPPORTED_FORMAT;
             const int nbx = (outp.w + bs.r2.tile_w - 1) / bs.r2.tile_w;
             const int nby = (outp.h + bs.r2.tile_h - 1) / bs.r2.tile_h;
             bs.n_items = nbx * nby;

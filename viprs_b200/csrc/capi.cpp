@@ -177,26 +177,13 @@ bool add_reduce2d_stage(viprs_plan* p, const ReduceKernel& first, const ReduceKe
     const double maxv = p->fmt == kU8 ? 255.0 : 65535.0;
     if (a.mode_h == kReduceFixed && double(rh.max_abs_i16_sum()) * maxv >= 2147483647.0) return false;
     if (a.mode_v == kReduceFixed && double(rv.max_abs_i16_sum()) * maxv >= 2147483647.0) return false;
-    // tile shape: 16 output rows x 64 columns, shrunk until the mid tile fits
-    a.tile_h = 16; a.tile_w = 64;
-    for (int attempt = 0; attempt < 8; ++attempt) {
-        const std::vector<int32_t>& st2 = hfirst ? sv : sh;
-        const int64_t n2 = hfirst ? outr.h : outr.w;
-        const int64_t tile = hfirst ? a.tile_h : a.tile_w;
-        const int64_t lo = hfirst ? mid.y : mid.x, hi = lo + (hfirst ? mid.h : mid.w) - 1;
-        const int taps2 = hfirst ? rv.taps : rh.taps;
-        int64_t span = 1;
-        for (int64_t t0 = 0; t0 < n2; t0 += tile) {
-            const int64_t t1 = std::min(n2, t0 + tile) - 1;
-            const int64_t a0 = std::max<int64_t>(st2[size_t(t0)], lo);
-            const int64_t a1 = std::min<int64_t>(int64_t(st2[size_t(t1)]) + taps2 - 1, hi);
-            span = std::max(span, a1 - a0 + 1);
-        }
-        a.span_max = int32_t(span);
-        if (launch::reduce2d_smem_bytes(a) != 0) break;
-        if (hfirst) { if (a.tile_w > 8) a.tile_w /= 2; else a.tile_h = std::max(1, a.tile_h / 2); }
-        else { if (a.tile_h > 2) a.tile_h /= 2; else a.tile_w = std::max(1, a.tile_w / 2); }
-    }
+    // tile shape: the largest whose staged rows, mid tile and output tile fit
+    // 64 KB of shared memory while the launch still has two tiles per SM
+    a.out.w = int32_t(outr.w);
+    a.out.h = int32_t(outr.h);
+    const Region& ir = p->planes[size_t(in_plane)].r;
+    if (!launch::reduce2d_configure(&a, sh.data(), sv.data(), ir.x, ir.y, ir.w, ir.h, 2 * 148, 64 * 1024))
+        return false;
     if (launch::reduce2d_smem_bytes(a) == 0) return false;
     st.starts_off = push_table(p->host_tables, sh.data(), sh.size() * 4);
     st.phases_off = push_table(p->host_tables, ph.data(), ph.size());

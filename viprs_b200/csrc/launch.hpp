@@ -95,7 +95,45 @@ struct Reduce2DArgs {
     int32_t unpremul_out = 0;
     int32_t tile_w = 64, tile_h = 16;
     int32_t span_max = 0;     // largest mid rows (hfirst) or columns (vfirst) one tile reads
+    int32_t in_rows_max = 0;  // largest source rows one tile stages in shared memory
+    int32_t in_cols_max = 0;  // largest source columns one tile stages
 };
+
+#if defined(__CUDACC__)
+#define VIPRS_HD __host__ __device__
+#else
+#define VIPRS_HD
+#endif
+
+// Shared-memory layout of one fused-reduce tile (byte offsets, 16-aligned):
+// both coefficient tables, the tile's start/phase tables, one offset per
+// staged source row, the staged source rows, the mid tile and the output tile.
+struct Reduce2DLayout {
+    int32_t coef_h = 0, coef_v = 0, tab = 0, rowbase = 0, in = 0, mid = 0, out = 0, total = 0;
+    int32_t coef_h_bytes = 0, coef_v_bytes = 0;
+    int32_t pitch = 0;  // bytes per staged source row
+};
+
+VIPRS_HD inline int32_t r2_align16(int64_t v) { return int32_t((v + 15) / 16 * 16); }
+
+VIPRS_HD inline Reduce2DLayout reduce2d_layout(const Reduce2DArgs& a) {
+    Reduce2DLayout L;
+    const int es = a.fmt == kU8 ? 1 : (a.fmt == kU16 ? 2 : 4);
+    L.coef_h_bytes = 65 * a.taps_h * (a.mode_h == kReduceFixed ? 2 : 8);
+    L.coef_v_bytes = 65 * a.taps_v * (a.mode_v == kReduceFixed ? 2 : 8);
+    L.coef_h = 0;
+    L.coef_v = r2_align16(L.coef_h_bytes);
+    L.tab = L.coef_v + r2_align16(L.coef_v_bytes);
+    const int64_t tab_bytes = int64_t(a.tile_w + a.tile_h) * 4 + a.tile_w + a.tile_h;
+    L.rowbase = L.tab + r2_align16(tab_bytes);
+    L.in = L.rowbase + r2_align16(int64_t(a.in_rows_max) * 4);
+    L.pitch = r2_align16(int64_t(a.in_cols_max) * a.bands * es + 16);
+    L.mid = L.in + r2_align16(int64_t(a.in_rows_max) * L.pitch);
+    const int64_t mid_bytes = int64_t(a.span_max) * (a.hfirst ? a.tile_w : a.tile_h) * a.bands * es;
+    L.out = L.mid + r2_align16(mid_bytes);
+    L.total = L.out + r2_align16(int64_t(a.tile_w) * a.tile_h * a.bands * es);
+    return L;
+}
 
 struct PixelArgs {
     PlaneArg in;
@@ -112,6 +150,13 @@ cudaError_t reduce_v(const ReduceArgs& a, cudaStream_t s);
 cudaError_t reduce2d(const Reduce2DArgs& a, cudaStream_t s);
 // Shared memory a reduce2d launch needs for its tile shape; 0 if too large.
 size_t reduce2d_smem_bytes(const Reduce2DArgs& a);
+// Choose the tile shape of a fused reduce and fill span_max / in_rows_max /
+// in_cols_max.  `sh`/`sv`: host copies of the H and V start tables (absolute
+// first tap per output column / row); `in_*`: the source plane's rectangle.
+// Picks the largest tile that fits `smem_budget` bytes and still gives at
+// least `min_tiles` tiles (when any shape does).  False if nothing fits.
+bool reduce2d_configure(Reduce2DArgs* a, const int32_t* sh, const int32_t* sv, int64_t in_x0, int64_t in_y0,
+                        int64_t in_w, int64_t in_h, int64_t min_tiles, size_t smem_budget);
 cudaError_t pixel(const PixelArgs& a, cudaStream_t s);
 // Dynamic shared memory a shrink2d launch needs; 0 if the factor is too large.
 size_t shrink2d_smem_bytes(const ShrinkArgs& a, int32_t* nx);

@@ -207,17 +207,83 @@ cudaError_t reduce_h(const ReduceArgs& a, cudaStream_t s) { return reduce_any<tr
 cudaError_t reduce_v(const ReduceArgs& a, cudaStream_t s) { return reduce_any<false>(a, s); }
 
 size_t reduce2d_smem_bytes(const Reduce2DArgs& a) {
-    const int es = fmt_size(a.fmt);
-    const int mh_b = a.mode_h == kReduceFixed ? 2 : 8, mv_b = a.mode_v == kReduceFixed ? 2 : 8;
-    const size_t ch = (65 * a.taps_h * mh_b + 15) / 16 * 16, cv = (65 * a.taps_v * mv_b + 15) / 16 * 16;
-    const size_t mid = size_t(a.span_max) * (a.hfirst ? a.tile_w : a.tile_h) * a.bands * es;
-    const size_t total = ch + cv + (mid + 15) / 16 * 16 + 256 + 16;
-    return total <= 200 * 1024 ? total : 0;
+    if (a.tile_w <= 0 || a.tile_h <= 0 || a.span_max <= 0 || a.in_rows_max <= 0 || a.in_cols_max <= 0) return 0;
+    const Reduce2DLayout L = reduce2d_layout(a);
+    return L.total <= 200 * 1024 ? size_t(L.total) : 0;
+}
+
+bool reduce2d_configure(Reduce2DArgs* a, const int32_t* sh, const int32_t* sv, int64_t in_x0, int64_t in_y0,
+                        int64_t in_w, int64_t in_h, int64_t min_tiles, size_t smem_budget) {
+    static const int32_t kShapes[][2] = {{128, 32}, {64, 64}, {64, 32}, {32, 64}, {32, 32}, {64, 16}, {32, 16},
+                                         {16, 32}, {16, 16}, {32, 8}, {16, 8}, {8, 8}, {8, 4}, {4, 4},
+                                         {4, 2}, {2, 2}, {2, 1}, {1, 1}};
+    const int64_t ow = a->out.w, oh = a->out.h;
+    // per-axis extents of every tile of a given size: (first, last) tap of the tile
+    auto axis = [&](const int32_t* st, int64_t n, int tile, int taps, auto&& fn) {
+        for (int64_t t0 = 0; t0 < n; t0 += tile) {
+            const int64_t t1 = std::min(n, t0 + tile) - 1;
+            fn(int64_t(st[t0]), int64_t(st[t1]) + taps - 1);
+        }
+    };
+    Reduce2DArgs best = *a;
+    bool found = false;
+    int64_t best_tiles = 0;
+    for (const auto& sz : kShapes) {
+        Reduce2DArgs c = *a;
+        c.tile_w = sz[0];
+        c.tile_h = sz[1];
+        int64_t span = 1, rows = 1, cols = 1;
+        if (c.hfirst) {
+            const int64_t mlo = c.my0, mhi = c.my0 + c.mh - 1;
+            axis(sv, oh, c.tile_h, c.taps_v, [&](int64_t v0, int64_t v1) {
+                span = std::max(span, std::min(v1, mhi) - std::max(v0, mlo) + 1);
+            });
+            rows = span;
+            axis(sh, ow, c.tile_w, c.taps_h, [&](int64_t h0, int64_t h1) {
+                const int64_t c0 = std::min(std::max(h0 - in_x0, int64_t(0)), in_w - 1);
+                const int64_t c1 = std::min(std::max(h1 - in_x0, int64_t(0)), in_w - 1);
+                cols = std::max(cols, c1 - c0 + 1);
+            });
+        } else {
+            const int64_t mlo = c.mx0, mhi = c.mx0 + c.mw - 1;
+            axis(sh, ow, c.tile_w, c.taps_h, [&](int64_t h0, int64_t h1) {
+                const int64_t lo = std::max(h0, mlo), hi = std::min(h1, mhi);
+                span = std::max(span, hi - lo + 1);
+                const int64_t c0 = std::min(std::max(lo - in_x0, int64_t(0)), in_w - 1);
+                const int64_t c1 = std::min(std::max(hi - in_x0, int64_t(0)), in_w - 1);
+                cols = std::max(cols, c1 - c0 + 1);
+            });
+            axis(sv, oh, c.tile_h, c.taps_v, [&](int64_t v0, int64_t v1) {
+                const int64_t r0 = std::min(std::max(v0 - in_y0, int64_t(0)), in_h - 1);
+                const int64_t r1 = std::min(std::max(v1 - in_y0, int64_t(0)), in_h - 1);
+                rows = std::max(rows, r1 - r0 + 1);
+            });
+        }
+        c.span_max = int32_t(span);
+        c.in_rows_max = int32_t(rows);
+        c.in_cols_max = int32_t(cols);
+        const size_t need = reduce2d_smem_bytes(c);
+        if (need == 0 || need > smem_budget) continue;
+        const int64_t tiles = ((ow + c.tile_w - 1) / c.tile_w) * ((oh + c.tile_h - 1) / c.tile_h);
+        if (!found || (best_tiles < min_tiles && tiles > best_tiles)) {
+            best = c;
+            best_tiles = tiles;
+            found = true;
+        }
+        if (tiles >= min_tiles) break;
+    }
+    if (!found) return false;
+    *a = best;
+    return true;
 }
 
 template <typename T, int MH, int MV>
 static cudaError_t r2d(const Reduce2DArgs& a, size_t smem, cudaStream_t s) {
-    auto k = dev::reduce2d_kernel<T, MH, MV>;
+    auto k = a.bands == 1 ? dev::reduce2d_kernel<T, MH, MV, 1>
+           : a.bands == 2 ? dev::reduce2d_kernel<T, MH, MV, 2>
+           : a.bands == 3 ? dev::reduce2d_kernel<T, MH, MV, 3>
+           : a.bands == 4 ? dev::reduce2d_kernel<T, MH, MV, 4>
+                          : dev::reduce2d_kernel<T, MH, MV, 0>;
     if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid((unsigned)((a.out.w + a.tile_w - 1) / a.tile_w), (unsigned)((a.out.h + a.tile_h - 1) / a.tile_h));
     k<<<grid, 256, smem, s>>>(a);

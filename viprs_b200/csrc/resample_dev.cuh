@@ -437,12 +437,13 @@ __global__ void __launch_bounds__(kShrinkThreads, 6) shrink_hv_u8_tma(ShrinkArgs
     int32_t p_oy = p_item / chunks;
     ShrinkChunk pc = shrink_chunk(a, p_item - p_oy * chunks);
     int64_t issued = 0;
+    int p_st = 0;  // ring slot of the next copy (issued mod S, kept incrementally)
     auto issue = [&]() {
         const int64_t s0 = row_of(p_oy, p_k) * a.in.pitch + pc.s_lo * B;
         const int64_t e0 = s0 + (pc.s_hi - pc.s_lo) * B;
         const int64_t as = s0 & ~int64_t(15);
         int64_t ae = (e0 + 15) & ~int64_t(15);
-        uint8_t* dst = bufs + (size_t)(issued % S) * a.stage_bytes;
+        uint8_t* dst = bufs + (size_t)p_st * a.stage_bytes;
         if (ae > a.in.total_bytes) {
             // the 16-byte cover would pass the end of the buffer: copy the aligned
             // part in bulk and the last few bytes with plain loads
@@ -450,10 +451,11 @@ __global__ void __launch_bounds__(kShrinkThreads, 6) shrink_hv_u8_tma(ShrinkArgs
             for (int64_t q = ab > as ? ab : as; q < e0; ++q) dst[q - as] = a.in.data[q];
             ae = ab > as ? ab : as;
         }
-        uint64_t* bar = &bars[issued % S];
+        uint64_t* bar = &bars[p_st];
         mbar_arrive_expect_tx(bar, uint32_t(ae - as));
         if (ae > as) bulk_load(dst, a.in.data + as, uint32_t(ae - as), bar);
         ++issued;
+        if (++p_st == S) p_st = 0;
         if (++p_k == fv) {
             p_k = 0;
             p_item += G;
@@ -481,9 +483,9 @@ __global__ void __launch_bounds__(kShrinkThreads, 6) shrink_hv_u8_tma(ShrinkArgs
     const uint32_t hhalf = uint32_t(fh) / 2;
     const bool hmult = a.hmode == 3;
     int64_t t_fail = -1;
+    int st = 0;           // ring slot of row t (t mod S)
+    uint32_t parity = 0;  // mbarrier phase parity of that slot ((t / S) & 1)
     for (int64_t t = 0; t < total; ++t) {
-        const int st = int(t % S);
-        const uint32_t parity = uint32_t((t / S) & 1);
         if (threadIdx.x == 0 && !mbar_wait(&bars[st], parity)) *flag = 1;
         __syncthreads();
         if (*flag) { t_fail = t; break; }
@@ -510,6 +512,7 @@ __global__ void __launch_bounds__(kShrinkThreads, 6) shrink_hv_u8_tma(ShrinkArgs
             fence_proxy_async_smem();
             issue();
         }
+        if (++st == S) { st = 0; parity ^= 1u; }
         if (++c_k == fv) {
             if (x < cc.ncols) {
                 uint8_t o[B];
@@ -540,7 +543,10 @@ __global__ void __launch_bounds__(kShrinkThreads, 6) shrink_hv_u8_tma(ShrinkArgs
         // this block still has in flight before its shared memory goes away
         if (threadIdx.x == 0) {
             if (a.err) atomicExch(a.err, VIPRS_ERR_TIMEOUT);
-            for (int64_t tt = t_fail + 1; tt < issued; ++tt) mbar_wait(&bars[tt % S], uint32_t((tt / S) & 1));
+            for (int64_t tt = t_fail + 1; tt < issued; ++tt) {
+                if (++st == S) { st = 0; parity ^= 1u; }
+                mbar_wait(&bars[st], parity);
+            }
         }
         __syncthreads();
     }
@@ -682,68 +688,51 @@ __global__ void __launch_bounds__(256) reduce_v_kernel(ReduceArgs a) {
 }
 
 // ---------------------------------------------------------------- fused reduce
+//
+// ReduceH and ReduceV (either order) for one output tile, everything staged in
+// shared memory: the tile's source rows are copied once with coalesced 16-byte
+// loads, the first op's output (the mid tile, rounded to the sample type as
+// viprs stores it) and the output tile never leave the SM.  Edge replication
+// is a clamp of the tap index into the staged range: the staged range is the
+// tile's tap span clamped to the source plane, so the clamp is the source
+// read's clamp (and for the mid tile, clamp_axis of the second op).
 
-template <typename T, int MODE>
-__device__ __forceinline__ T reduce_taps_global(const Plane& in, int64_t lx, int64_t ly, bool horizontal,
-                                                int64_t start_local, int taps, int bands, int b,
-                                                const uint8_t* coef, int ph, bool premul, bool simd_lane) {
+// One sum of `taps` samples p[k * stride], k = clamp(s + t, 0, hi), with
+// coefficient row c, in the accumulation order of `MODE`.
+//   Fixed:      int32 sum of i16 x sample, (acc + 2048) >> 12 clamped
+//   F32Simd, H: 4-lane partial sums of products, then sequential tail fmas
+//               (reduce_h_f32 AVX2, reduce_simd.rs:2621-2694)
+//   F32Simd, V: acc + v * w (mul then add) inside the vector body, fma in the
+//               scalar tail (reduce_v_f32 AVX2, :2830-2888)
+//   F64Fma:     sequential fma (scalar paths, ReduceOp)
+template <typename T, int MODE, bool HORIZ>
+__device__ __forceinline__ T fused_taps(const T* p, int s, int hi, int stride, int taps, const uint8_t* coef, int ph,
+                                        bool simd_lane) {
+    const bool inside = s >= 0 && s + taps - 1 <= hi;
     if (MODE == kReduceFixed) {
         const int16_t* c = reinterpret_cast<const int16_t*>(coef) + ph * taps;
         int32_t acc = 0;
-        for (int t = 0; t < taps; ++t) {
-            const int64_t x = horizontal ? start_local + t : lx, y = horizontal ? ly : start_local + t;
-            acc += (int32_t)c[t] * (int32_t)load_premul<T>(in, x, y, bands, b, premul);
-        }
-        return from_fixed<T>(acc);
-    } else {
-        const double* c = reinterpret_cast<const double*>(coef) + ph * taps;
-        double acc = 0.0;
-        if (MODE == kReduceF32Simd && horizontal) {
-            int t = 0;
-            for (; t + 4 <= taps; t += 4) {
-                double lanes = as_f64(load_sample<T>(in, start_local + t, ly, bands, b)) * c[t];
-                lanes = lanes + as_f64(load_sample<T>(in, start_local + t + 1, ly, bands, b)) * c[t + 1];
-                lanes = lanes + as_f64(load_sample<T>(in, start_local + t + 2, ly, bands, b)) * c[t + 2];
-                lanes = lanes + as_f64(load_sample<T>(in, start_local + t + 3, ly, bands, b)) * c[t + 3];
-                acc = acc + lanes;
-            }
-            for (; t < taps; ++t) acc = fma(as_f64(load_sample<T>(in, start_local + t, ly, bands, b)), c[t], acc);
-        } else if (MODE == kReduceF32Simd && simd_lane) {
-            for (int t = 0; t < taps; ++t) acc = acc + as_f64(load_sample<T>(in, lx, start_local + t, bands, b)) * c[t];
+        if (inside) {
+            const T* q = p + s * stride;
+#pragma unroll 4
+            for (int t = 0; t < taps; ++t) acc += (int32_t)c[t] * (int32_t)q[t * stride];
         } else {
             for (int t = 0; t < taps; ++t) {
-                const int64_t x = horizontal ? start_local + t : lx, y = horizontal ? ly : start_local + t;
-                acc = fma(as_f64(load_sample<T>(in, x, y, bands, b)), c[t], acc);
+                int k = s + t;
+                k = k < 0 ? 0 : (k > hi ? hi : k);
+                acc += (int32_t)c[t] * (int32_t)p[k * stride];
             }
-        }
-        return from_f64<T>(acc);
-    }
-}
-
-// Second pass over the shared-memory mid tile `m` (row stride `mstride` samples).
-template <typename T, int MODE>
-__device__ __forceinline__ T reduce_taps_smem(const T* m, int64_t first, int64_t lo, int64_t hi, int64_t origin,
-                                              int64_t stride, int taps, const uint8_t* coef, int ph, bool horizontal,
-                                              bool simd_lane) {
-    // tap i reads mid index clamp(first + i, lo, hi) - origin along the pass axis
-    if (MODE == kReduceFixed) {
-        const int16_t* c = reinterpret_cast<const int16_t*>(coef) + ph * taps;
-        int32_t acc = 0;
-        for (int t = 0; t < taps; ++t) {
-            int64_t q = first + t;
-            q = q < lo ? lo : (q > hi ? hi : q);
-            acc += (int32_t)c[t] * (int32_t)m[(q - origin) * stride];
         }
         return from_fixed<T>(acc);
     } else {
         const double* c = reinterpret_cast<const double*>(coef) + ph * taps;
-        double acc = 0.0;
-        auto val = [&](int t) {
-            int64_t q = first + t;
-            q = q < lo ? lo : (q > hi ? hi : q);
-            return as_f64(m[(q - origin) * stride]);
+        auto val = [&](int t) -> double {
+            int k = s + t;
+            if (!inside) k = k < 0 ? 0 : (k > hi ? hi : k);
+            return as_f64(p[k * stride]);
         };
-        if (MODE == kReduceF32Simd && horizontal) {
+        double acc = 0.0;
+        if (MODE == kReduceF32Simd && HORIZ) {
             int t = 0;
             for (; t + 4 <= taps; t += 4) {
                 double lanes = val(t) * c[t];
@@ -762,122 +751,221 @@ __device__ __forceinline__ T reduce_taps_smem(const T* m, int64_t first, int64_t
     }
 }
 
-// One block: an output tile of tile_h rows x tile_w columns.
-template <typename T, int MH, int MV>
-__device__ void reduce2d_tile(const Reduce2DArgs& a, int bx, int by, uint8_t* smem_r2) {
-    const int bands = a.bands;
-    const int ch_bytes = 65 * a.taps_h * (MH == kReduceFixed ? 2 : 8);
-    const int cv_bytes = 65 * a.taps_v * (MV == kReduceFixed ? 2 : 8);
-    const int chp = (ch_bytes + 15) / 16 * 16, cvp = (cv_bytes + 15) / 16 * 16;
-    uint8_t* ch = smem_r2;
-    uint8_t* cv = smem_r2 + chp;
-    for (int i = threadIdx.x * 4; i < ch_bytes; i += blockDim.x * 4)
-        *reinterpret_cast<uint32_t*>(ch + i) = *reinterpret_cast<const uint32_t*>((const uint8_t*)a.coeffs_h + i);
-    for (int i = threadIdx.x * 4; i < cv_bytes; i += blockDim.x * 4)
-        *reinterpret_cast<uint32_t*>(cv + i) = *reinterpret_cast<const uint32_t*>((const uint8_t*)a.coeffs_v + i);
-    T* mid = reinterpret_cast<T*>(smem_r2 + chp + cvp);
-    const int tx0 = bx * a.tile_w, ty0 = by * a.tile_h;
-    const int ncols = min(a.tile_w, a.out.w - tx0), nrows = min(a.tile_h, a.out.h - ty0);
-    uint8_t* stage = reinterpret_cast<uint8_t*>(mid) + (size_t)a.span_max * (a.hfirst ? ncols : nrows) * bands * sizeof(T);
-    stage = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(stage) + 15) & ~uintptr_t(15));
-    __syncthreads();
-    const bool premul = a.premul_in != 0;
-    if (a.hfirst) {
-        // rows of the mid plane this tile's vertical taps read
-        int64_t rlo = a.starts_v[ty0], rhi = (int64_t)a.starts_v[ty0 + nrows - 1] + a.taps_v - 1;
-        const int64_t mlo = a.my0, mhi = a.my0 + a.mh - 1;
-        rlo = rlo < mlo ? mlo : rlo;
-        rhi = rhi > mhi ? mhi : rhi;
-        const int R = int(rhi - rlo + 1);
-        const int per_row = ncols * bands;
-        for (int i = threadIdx.x; i < R * per_row; i += blockDim.x) {
-            const int r = i / per_row, rem = i - r * per_row, x = rem / bands, b = rem - x * bands;
-            const int64_t ly = rlo + r - a.in.y0;
-            const int col = tx0 + x;
-            mid[i] = reduce_taps_global<T, MH>(a.in, 0, ly, true, (int64_t)a.starts_h[col] - a.in.x0, a.taps_h, bands,
-                                               b, ch, a.phases_h[col], premul, false);
-        }
-        __syncthreads();
-        const int n_out = nrows * per_row;
-        for (int base = 0; base < n_out; base += blockDim.x) {
-            const int i = base + threadIdx.x;
-            T v = T(0);
-            if (i < n_out) {
-                const int yy = i / per_row, rem = i - yy * per_row, x = rem / bands, b = rem - x * bands;
-                const int y = ty0 + yy;
-                const int64_t vidx = (int64_t)(tx0 + x) * bands + b;
-                v = reduce_taps_smem<T, MV>(mid + x * bands + b, a.starts_v[y], mlo, mhi, rlo, per_row, a.taps_v, cv,
-                                            a.phases_v[y], false, vidx < a.vector_len);
-            }
-            const int yy = i / per_row;
-            uint8_t* orow = a.out.data + (int64_t)(ty0 + (i < n_out ? yy : 0)) * a.out.pitch;
-            const int64_t col_item = (int64_t)tx0 * bands + (i - yy * per_row);
-            if (a.unpremul_out) {
-                stage[threadIdx.x] = (uint8_t)v;
-                __syncthreads();
-                if (i < n_out) {
-                    const int b = int(col_item % bands);
-                    uint32_t o = stage[threadIdx.x];
-                    if (b != bands - 1) o = unpremultiply_u8(o, stage[threadIdx.x + (bands - 1 - b)]);
-                    orow[col_item] = (uint8_t)o;
-                }
-                __syncthreads();
-            } else if (i < n_out) {
-                reinterpret_cast<T*>(orow)[col_item] = v;
-            }
-        }
+// The same vertical sum over staged source rows whose starts differ per row
+// (`rowbase[k]` bytes from `base`).
+template <typename T, int MODE>
+__device__ __forceinline__ T fused_taps_rows(const uint8_t* base, const int32_t* rowbase, int col_bytes, int s, int hi,
+                                             int taps, const uint8_t* coef, int ph, bool simd_lane) {
+    auto at = [&](int t) -> T {
+        int k = s + t;
+        k = k < 0 ? 0 : (k > hi ? hi : k);
+        return *reinterpret_cast<const T*>(base + rowbase[k] + col_bytes);
+    };
+    if (MODE == kReduceFixed) {
+        const int16_t* c = reinterpret_cast<const int16_t*>(coef) + ph * taps;
+        int32_t acc = 0;
+#pragma unroll 4
+        for (int t = 0; t < taps; ++t) acc += (int32_t)c[t] * (int32_t)at(t);
+        return from_fixed<T>(acc);
     } else {
-        // columns of the mid plane this tile's horizontal taps read
-        int64_t clo = a.starts_h[tx0], chi = (int64_t)a.starts_h[tx0 + ncols - 1] + a.taps_h - 1;
-        const int64_t mlo = a.mx0, mhi = a.mx0 + a.mw - 1;
-        clo = clo < mlo ? mlo : clo;
-        chi = chi > mhi ? mhi : chi;
-        const int C = int(chi - clo + 1);
-        const int per_row = C * bands;
-        for (int i = threadIdx.x; i < nrows * per_row; i += blockDim.x) {
-            const int yy = i / per_row, rem = i - yy * per_row, c = rem / bands, b = rem - c * bands;
-            const int y = ty0 + yy;
-            const int64_t mcol = clo + c;
-            const int64_t vidx = (mcol - a.mx0) * bands + b;
-            mid[i] = reduce_taps_global<T, MV>(a.in, mcol - a.in.x0, 0, false, (int64_t)a.starts_v[y] - a.in.y0, a.taps_v,
-                                               bands, b, cv, a.phases_v[y], premul, vidx < a.vector_len);
+        const double* c = reinterpret_cast<const double*>(coef) + ph * taps;
+        double acc = 0.0;
+        if (MODE == kReduceF32Simd && simd_lane) {
+            for (int t = 0; t < taps; ++t) acc = acc + as_f64(at(t)) * c[t];
+        } else {
+            for (int t = 0; t < taps; ++t) acc = fma(as_f64(at(t)), c[t], acc);
         }
-        __syncthreads();
-        const int per_out = ncols * bands;
-        const int n_out = nrows * per_out;
-        for (int base = 0; base < n_out; base += blockDim.x) {
-            const int i = base + threadIdx.x;
-            T v = T(0);
-            if (i < n_out) {
-                const int yy = i / per_out, rem = i - yy * per_out, x = rem / bands, b = rem - x * bands;
-                const int col = tx0 + x;
-                v = reduce_taps_smem<T, MH>(mid + yy * per_row + b, a.starts_h[col], mlo, mhi, clo, bands, a.taps_h, ch,
-                                            a.phases_h[col], true, false);
-            }
-            const int yy = i / per_out;
-            uint8_t* orow = a.out.data + (int64_t)(ty0 + (i < n_out ? yy : 0)) * a.out.pitch;
-            const int64_t col_item = (int64_t)tx0 * bands + (i - yy * per_out);
-            if (a.unpremul_out) {
-                stage[threadIdx.x] = (uint8_t)v;
-                __syncthreads();
-                if (i < n_out) {
-                    const int b = int(col_item % bands);
-                    uint32_t o = stage[threadIdx.x];
-                    if (b != bands - 1) o = unpremultiply_u8(o, stage[threadIdx.x + (bands - 1 - b)]);
-                    orow[col_item] = (uint8_t)o;
-                }
-                __syncthreads();
-            } else if (i < n_out) {
-                reinterpret_cast<T*>(orow)[col_item] = v;
-            }
-        }
+        return from_f64<T>(acc);
     }
 }
 
-template <typename T, int MH, int MV>
+// Copy `bytes` (a multiple of 16, both pointers 16-byte aligned) global -> shared.
+__device__ __forceinline__ void copy_table16(uint8_t* dst, const void* src, int bytes) {
+    const uint4* s = reinterpret_cast<const uint4*>(src);
+    uint4* d = reinterpret_cast<uint4*>(dst);
+    for (int i = threadIdx.x; i < bytes / 16; i += blockDim.x) d[i] = s[i];
+}
+
+// Stage rows [0, nrows) of a source tile: row r is plane row row_of(r), columns
+// [c0, c0 + ncols).  One warp per row: 16-byte loads for the aligned body, byte
+// loads for the unaligned head and tail; the staged copy keeps the source's
+// address modulo 16 so the vector stores stay aligned.
+template <typename T, typename RowOf>
+__device__ __forceinline__ void stage_tile_rows(const Plane& in, RowOf row_of, int nrows, int64_t c0, int ncols,
+                                                int bands, uint8_t* dst_base, int pitch, int32_t* rowbase) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int nbytes = ncols * bands * int(sizeof(T));
+    for (int r = warp; r < nrows; r += nw) {
+        const uint8_t* src = in.data + row_of(r) * in.pitch + c0 * bands * int64_t(sizeof(T));
+        const int off = int(reinterpret_cast<uintptr_t>(src) & 15);
+        uint8_t* dst = dst_base + r * pitch + off;
+        if (lane == 0) rowbase[r] = r * pitch + off;
+        const int head = min((16 - off) & 15, nbytes);
+        const int nvec = (nbytes - head) >> 4;
+        const int tail0 = head + nvec * 16;
+        if (lane < head) dst[lane] = __ldg(src + lane);
+        if (lane < nbytes - tail0) dst[tail0 + lane] = __ldg(src + tail0 + lane);
+        const uint4* vs = reinterpret_cast<const uint4*>(src + head);
+        uint4* vd = reinterpret_cast<uint4*>(dst + head);
+        for (int k = lane; k < nvec; k += 32) vd[k] = __ldg(vs + k);
+    }
+}
+
+// NB: compile-time band count (0 = a.bands at run time), so that the
+// per-sample index splits j -> (pixel, band) compile to multiply-shifts.
+// Premultiply<U8> of the staged source tile (R rows of C pixels, alpha last).
+__device__ __forceinline__ void premultiply_staged(uint8_t* ins, const int32_t* rowbase, int R, int C, int B) {
+    int r = threadIdx.x / C, c = threadIdx.x - r * C;
+    const int dr = blockDim.x / C, dc = blockDim.x - dr * C;
+    for (; r < R;) {
+        uint8_t* px = ins + rowbase[r] + c * B;
+        const uint32_t al = px[B - 1];
+        for (int b = 0; b < B - 1; ++b) px[b] = (uint8_t)premultiply_u8(px[b], al);
+        r += dr; c += dc;
+        if (c >= C) { c -= C; ++r; }
+    }
+}
+
+template <typename T, int MH, int MV, int NB>
+__device__ void reduce2d_tile(const Reduce2DArgs& a, int bx, int by, uint8_t* sm) {
+    const Reduce2DLayout L = reduce2d_layout(a);
+    const int B = NB > 0 ? NB : a.bands;
+    const int tx0 = bx * a.tile_w, ty0 = by * a.tile_h;
+    const int ncols = min(a.tile_w, a.out.w - tx0), nrows = min(a.tile_h, a.out.h - ty0);
+    const uint8_t* ch = sm + L.coef_h;
+    const uint8_t* cv = sm + L.coef_v;
+    int32_t* sx = reinterpret_cast<int32_t*>(sm + L.tab);
+    int32_t* sy = sx + a.tile_w;
+    uint8_t* phx = reinterpret_cast<uint8_t*>(sy + a.tile_h);
+    uint8_t* phy = phx + a.tile_w;
+    int32_t* rowbase = reinterpret_cast<int32_t*>(sm + L.rowbase);
+    uint8_t* ins = sm + L.in;
+    T* mid = reinterpret_cast<T*>(sm + L.mid);
+    T* ost = reinterpret_cast<T*>(sm + L.out);
+
+    copy_table16(sm + L.coef_h, a.coeffs_h, r2_align16(L.coef_h_bytes));
+    copy_table16(sm + L.coef_v, a.coeffs_v, r2_align16(L.coef_v_bytes));
+    for (int i = threadIdx.x; i < ncols; i += blockDim.x) { sx[i] = a.starts_h[tx0 + i]; phx[i] = a.phases_h[tx0 + i]; }
+    for (int i = threadIdx.x; i < nrows; i += blockDim.x) { sy[i] = a.starts_v[ty0 + i]; phy[i] = a.phases_v[ty0 + i]; }
+    // tap spans of the tile (absolute coordinates of each op's input)
+    const int64_t hs0 = a.starts_h[tx0], hs1 = (int64_t)a.starts_h[tx0 + ncols - 1] + a.taps_h - 1;
+    const int64_t vs0 = a.starts_v[ty0], vs1 = (int64_t)a.starts_v[ty0 + nrows - 1] + a.taps_v - 1;
+    const int64_t pw = a.in.w - 1, phh = a.in.h - 1;
+    const bool premul = a.premul_in != 0;
+
+    if (a.hfirst) {
+        // mid rows [rlo, rhi]: the V taps clamped to the mid plane; each is the
+        // H output of source row clamp(r - in.y0)
+        const int64_t mlo = a.my0, mhi = a.my0 + a.mh - 1;
+        const int64_t rlo = vs0 < mlo ? mlo : vs0, rhi = vs1 > mhi ? mhi : vs1;
+        const int R = int(rhi - rlo + 1);
+        const int64_t c0 = clampi64(hs0 - a.in.x0, 0, pw), c1 = clampi64(hs1 - a.in.x0, 0, pw);
+        const int C = int(c1 - c0 + 1);
+        stage_tile_rows<T>(a.in, [&](int r) { return clampi64(rlo + r - a.in.y0, 0, phh); }, R, c0, C, B, ins, L.pitch,
+                           rowbase);
+        __syncthreads();
+        if (premul) {
+            premultiply_staged(ins, rowbase, R, C, B);
+            __syncthreads();
+        }
+        // H: mid[r][x*B + b]
+        const int W1 = ncols * B;
+        {
+            int r = threadIdx.x / W1, j = threadIdx.x - r * W1;
+            const int dr = blockDim.x / W1, dj = blockDim.x - dr * W1;
+            for (; r < R;) {
+                const int x = j / B, b = j - x * B;
+                const T* row = reinterpret_cast<const T*>(ins + rowbase[r]) + b;
+                const int s = int(sx[x] - a.in.x0 - c0);
+                mid[r * W1 + j] = fused_taps<T, MH, true>(row, s, C - 1, B, a.taps_h, ch, phx[x], false);
+                r += dr; j += dj;
+                if (j >= W1) { j -= W1; ++r; }
+            }
+        }
+        __syncthreads();
+        // V: out[y][x*B + b]
+        {
+            int y = threadIdx.x / W1, j = threadIdx.x - y * W1;
+            const int dy = blockDim.x / W1, dj = blockDim.x - dy * W1;
+            for (; y < nrows;) {
+                const int s = int(sy[y] - rlo);
+                const bool lane = (int64_t)tx0 * B + j < a.vector_len;
+                ost[y * W1 + j] = fused_taps<T, MV, false>(mid + j, s, R - 1, W1, a.taps_v, cv, phy[y], lane);
+                y += dy; j += dj;
+                if (j >= W1) { j -= W1; ++y; }
+            }
+        }
+    } else {
+        // mid columns [clo, chi]: the H taps clamped to the mid plane; each is
+        // the V output of source column clamp(c - in.x0)
+        const int64_t mlo = a.mx0, mhi = a.mx0 + a.mw - 1;
+        const int64_t clo = hs0 < mlo ? mlo : hs0, chi = hs1 > mhi ? mhi : hs1;
+        const int Cm = int(chi - clo + 1);
+        const int64_t c0 = clampi64(clo - a.in.x0, 0, pw), c1 = clampi64(chi - a.in.x0, 0, pw);
+        const int C = int(c1 - c0 + 1);
+        const int64_t r0 = clampi64(vs0 - a.in.y0, 0, phh), r1 = clampi64(vs1 - a.in.y0, 0, phh);
+        const int R = int(r1 - r0 + 1);
+        stage_tile_rows<T>(a.in, [&](int r) { return r0 + r; }, R, c0, C, B, ins, L.pitch, rowbase);
+        __syncthreads();
+        if (premul) {
+            premultiply_staged(ins, rowbase, R, C, B);
+            __syncthreads();
+        }
+        // V: mid[y][c*B + b]
+        const int W1 = Cm * B;
+        {
+            int y = threadIdx.x / W1, j = threadIdx.x - y * W1;
+            const int dy = blockDim.x / W1, dj = blockDim.x - dy * W1;
+            for (; y < nrows;) {
+                const int c = j / B, b = j - c * B;
+                const int64_t mcol = clo + c;
+                const int col = int(clampi64(mcol - a.in.x0, 0, pw) - c0);
+                const int s = int(sy[y] - a.in.y0 - r0);
+                const bool lane = (mcol - a.mx0) * B + b < a.vector_len;
+                mid[y * W1 + j] = fused_taps_rows<T, MV>(ins, rowbase, (col * B + b) * int(sizeof(T)), s, R - 1,
+                                                         a.taps_v, cv, phy[y], lane);
+                y += dy; j += dj;
+                if (j >= W1) { j -= W1; ++y; }
+            }
+        }
+        __syncthreads();
+        // H: out[y][x*B + b]
+        const int W2 = ncols * B;
+        {
+            int y = threadIdx.x / W2, j = threadIdx.x - y * W2;
+            const int dy = blockDim.x / W2, dj = blockDim.x - dy * W2;
+            for (; y < nrows;) {
+                const int x = j / B, b = j - x * B;
+                const int s = int(sx[x] - clo);
+                ost[y * W2 + j] = fused_taps<T, MH, true>(mid + y * W1 + b, s, Cm - 1, B, a.taps_h, ch, phx[x], false);
+                y += dy; j += dj;
+                if (j >= W2) { j -= W2; ++y; }
+            }
+        }
+    }
+    __syncthreads();
+    // store the output tile (unpremultiplied when the chain ends with it)
+    const int Wo = ncols * B;
+    const bool unpremul = a.unpremul_out != 0;
+    int y = threadIdx.x / Wo, j = threadIdx.x - y * Wo;
+    const int dy = blockDim.x / Wo, dj = blockDim.x - dy * Wo;
+    for (; y < nrows;) {
+        const int i = y * Wo + j;
+        T v = ost[i];
+        if (unpremul) {
+            const int b = j % B;
+            if (b != B - 1) v = (T)unpremultiply_u8((uint32_t)v, (uint32_t)ost[i + (B - 1 - b)]);
+        }
+        reinterpret_cast<T*>(a.out.data + (int64_t)(ty0 + y) * a.out.pitch)[(int64_t)tx0 * B + j] = v;
+        y += dy; j += dj;
+        if (j >= Wo) { j -= Wo; ++y; }
+    }
+}
+
+template <typename T, int MH, int MV, int NB>
 __global__ void __launch_bounds__(256) reduce2d_kernel(Reduce2DArgs a) {
     extern __shared__ __align__(16) uint8_t smem_r2[];
-    reduce2d_tile<T, MH, MV>(a, blockIdx.x, blockIdx.y, smem_r2);
+    reduce2d_tile<T, MH, MV, NB>(a, blockIdx.x, blockIdx.y, smem_r2);
 }
 
 // ---------------------------------------------------------------- pixel ops
