@@ -224,7 +224,9 @@ void viprs_plan_destroy(viprs_plan *plan);
    point corresponds: viprs runs one pipeline per image
    (ImageApi::thumbnail, image_api/transform.rs:287-301); the per-image path
    below is exactly that, one plan per image, and the persistent path runs
-   the same plans' stages from one launch over a device work list. */
+   the same plans' stages as a few persistent launches over a device work
+   list: one per stage level and kind (the shrinks of every image, then the
+   fused reduces, ...), so that launch order carries every dependency. */
 typedef struct viprs_batch viprs_batch;
 
 /* One PipelineBuilder::thumbnail plan per image (u8 images). */
@@ -235,10 +237,10 @@ int32_t viprs_thumbnail_batch_create(int32_t n_images, const uint32_t *widths,
                                      viprs_batch **out_batch);
 int32_t viprs_batch_output_size(const viprs_batch *batch, int32_t index, uint32_t *width,
                                 uint32_t *height);
-/* Work items, stages and persistent grid size of the current configuration. */
+/* Work items, stages and the largest persistent grid of the current configuration. */
 int32_t viprs_batch_work_items(const viprs_batch *batch, int32_t *items, int32_t *stages,
                                int32_t *grid);
-/* Launches per execution: 1 for the persistent path, the plans' stage count per image. */
+/* Launches per execution: the persistent launches, and the plans' stage count for per-image. */
 int32_t viprs_batch_launch_count(const viprs_batch *batch, int32_t *batched, int32_t *per_image);
 /* Persistent path.  d_srcs / d_dsts are DEVICE arrays of n_images device
    pointers (packed HWC u8 buffers, 16-byte aligned for the bulk-copy path). */
@@ -250,14 +252,17 @@ int32_t viprs_batch_execute_graph(viprs_batch *batch, const uint64_t *d_srcs,
 /* Plain per-image path: h_srcs / h_dsts are HOST arrays of device pointers. */
 int32_t viprs_batch_execute_per_image(viprs_batch *batch, const uint64_t *h_srcs,
                                       const uint64_t *h_dsts, void *stream);
-/* Autotuner: times candidate shrink segment sizes, work-list lags and block
-   counts on the given images and keeps the fastest. */
+/* Autotuner: times candidate shrink row-segment sizes, ring depths and blocks
+   per SM on the given images and keeps the fastest. */
 int32_t viprs_batch_autotune(viprs_batch *batch, const uint64_t *d_srcs, const uint64_t *d_dsts,
                              void *stream, int32_t repeats, float *best_ms);
-int32_t viprs_batch_set_config(viprs_batch *batch, uint32_t ring_bytes, int32_t lag_blocks,
+/* ring_bytes: source bytes per shrink row segment (256..32768); ring_slots:
+   slots of each block's shrink ring (1..16, 0 = from a 56 KB budget);
+   blocks_per_sm: cap of the shrink launches (0 = occupancy maximum). */
+int32_t viprs_batch_set_config(viprs_batch *batch, uint32_t ring_bytes, int32_t ring_slots,
                                int32_t blocks_per_sm);
 int32_t viprs_batch_get_config(const viprs_batch *batch, uint32_t *ring_bytes,
-                               int32_t *lag_blocks, int32_t *blocks_per_sm);
+                               int32_t *ring_slots, int32_t *blocks_per_sm);
 /* Synchronise `stream` and return the first device-side error (VIPRS_ERR_TIMEOUT
    if a bounded wait gave up), 0 if none. */
 int32_t viprs_batch_status(viprs_batch *batch, void *stream);

@@ -471,10 +471,10 @@ class ThumbnailBatch:
         cap = ctypes.c_int32()
         N.check(N.lib().viprs_batch_get_config(self._h, ctypes.byref(r), ctypes.byref(lag), ctypes.byref(cap)),
                 "batch_get_config")
-        return {"ring_bytes": r.value, "lag_blocks": lag.value, "blocks_per_sm": cap.value}
+        return {"ring_bytes": r.value, "ring_slots": lag.value, "blocks_per_sm": cap.value}
 
-    def set_config(self, ring_bytes, lag_blocks, blocks_per_sm):
-        N.check(N.lib().viprs_batch_set_config(self._h, int(ring_bytes), int(lag_blocks), int(blocks_per_sm)),
+    def set_config(self, ring_bytes, ring_slots, blocks_per_sm):
+        N.check(N.lib().viprs_batch_set_config(self._h, int(ring_bytes), int(ring_slots), int(blocks_per_sm)),
                 "batch_set_config")
 
     def close(self):

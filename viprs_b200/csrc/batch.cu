@@ -1,16 +1,29 @@
 // batch.cu -- the persistent batched-thumbnail kernel (sm_100a).
 //
 // One launch processes the thumbnails of many images of uneven size.  Blocks
-// (a few per SM, all resident) claim work items from a device list with an
-// atomic cursor; an item is one piece of one stage of one image's plan:
-//   shrink   (output row, column chunk)  ShrinkH+ShrinkV, TMA ring as in resample.cu
-//   reduce2d (output tile)               fused ReduceH+ReduceV
-//   affine   (output row)                the bicubic correction (rare)
-//   pixel    (output row)                copy / premultiply / unpremultiply
-// A stage waits for the stage it reads: thread 0 polls the producer stage's
-// completion counter with an acquire load, bounded by kMaxPolls; on timeout
-// the block records VIPRS_ERR_TIMEOUT and stops claiming work.  Producers
-// publish with __threadfence() + atomicAdd after the block's stores.
+// (resident on every SM) claim work items from a device list with an atomic
+// cursor; an item is one piece of one stage of one image's plan:
+//   shrink   (band of output rows, column chunk)  ShrinkH+ShrinkV
+//   reduce2d (output tile)                        fused ReduceH+ReduceV
+//   reduce h/v (output row chunk)                 one reduce pass
+//   affine   (output row)                         the bicubic correction (rare)
+//   pixel    (output row)                         copy / premultiply / unpremultiply
+//
+// Each block is warp-specialised.  The producer warp (thread kCThreads) claims
+// items ahead of the consumers into a small queue and, for shrink items, issues
+// the source row segments as TMA bulk copies into the block's ring (the
+// warp-specialised ring of resample_dev.cuh), so the copies of the next items
+// are in flight while the consumers finish the current one.  The eight
+// consumer warps process the items in queue order; block-wide steps among them
+// use barrier 1 (256 threads), which the producer never joins.
+//
+// A stage waits for the stage it reads: one consumer thread polls the producer
+// stage's completion counter with an acquire load, bounded by kMaxPolls and
+// 2 s; producers publish with __threadfence() + atomicAdd after the item's
+// stores.  Items are claimed in list order and each block runs its claimed
+// items in that order, so the earliest unfinished item never waits on a later
+// one.  Every wait is bounded; a timeout is recorded as VIPRS_ERR_TIMEOUT and
+// the block drains its in-flight copies before it exits.
 #include "affine_dev.cuh"
 #include "batch_launch.hpp"
 #include "resample_dev.cuh"
@@ -24,135 +37,105 @@ __device__ __forceinline__ int32_t ld_acquire_i32(const int32_t* p) {
     return v;
 }
 
-constexpr int kRing = 4;
+constexpr int kQueue = 3;  // items the producer may hold ahead of the consumers
 
-// One interior shrink item -- output rows [oy0, oy1) of a column chunk --
-// through the TMA ring.  The item's source rows are consecutive plane rows
-// (oy0 * fv + k), so the ring streams them without a break at output-row
-// boundaries.  `pos` counts ring loads issued so far by this block (identical
-// in every thread).  Returns false on a timed-out copy.
-template <int B>
-__device__ bool batch_shrink_interior(const ShrinkArgs& a, int32_t oy0, int32_t oy1, int32_t c0, int32_t ncols,
-                                      uint64_t* bars, uint8_t* bufs, uint32_t stage_bytes, int64_t& pos,
-                                      volatile int32_t* flag) {
-    const int32_t fh = int32_t(a.fh), fv = int32_t(a.fv);
-    const int64_t sbase = ((a.out.x0 + c0) * (int64_t)fh - a.in.x0) * B;
-    const int64_t row0 = (a.out.y0 + oy0) * (int64_t)fv - a.in.y0;
-    const int32_t nbytes = ncols * fh * B;
-    const int32_t total = (oy1 - oy0) * fv;
-    auto span = [&](int32_t k, int64_t* as, uint32_t* bytes, int32_t* lead) {
-        int64_t ly = row0 + k;
-        ly = ly < 0 ? 0 : (ly >= a.in.h ? a.in.h - 1 : ly);
-        const int64_t s0 = ly * a.in.pitch + sbase;
-        *as = s0 & ~int64_t(15);
-        *bytes = uint32_t(((s0 + nbytes + 15) & ~int64_t(15)) - *as);
-        *lead = int32_t(s0 - *as);
-    };
-    auto issue = [&](int32_t k) {
-        int64_t as; uint32_t bytes; int32_t lead;
-        span(k, &as, &bytes, &lead);
-        const int st = int((pos + k) & (kRing - 1));
-        mbar_arrive_expect_tx(&bars[st], bytes);
-        bulk_load(bufs + (size_t)st * stage_bytes, a.in.data + as, bytes, &bars[st]);
-    };
-    const int32_t first = total < kRing ? total : kRing;
-    if (threadIdx.x == 0)
-        for (int32_t k = 0; k < first; ++k) issue(k);
-    uint32_t vacc[B];
-#pragma unroll
-    for (int b = 0; b < B; ++b) vacc[b] = 0;
-    const int32_t x = threadIdx.x;
-    const uint32_t hhalf = uint32_t(fh) / 2;
-    const bool hmult = a.hmode == 3;
-    bool ok = true;
-    int32_t k = 0, kv = 0, oy = oy0;
-    for (; k < total; ++k) {
-        const int st = int((pos + k) & (kRing - 1));
-        const uint32_t parity = uint32_t(((pos + k) / kRing) & 1);
-        if (threadIdx.x == 0 && !mbar_wait(&bars[st], parity)) *flag = 1;
-        __syncthreads();
-        if (*flag) { ok = false; break; }
-        int64_t as; uint32_t bytes; int32_t lead;
-        span(k, &as, &bytes, &lead);
-        uint8_t* row = bufs + (size_t)st * stage_bytes + lead;
-        if (a.premul_in) {
-            premultiply_pixels<B>(row, ncols * fh);
-            __syncthreads();
-        }
-        if (x < ncols) {
-            uint32_t sums[B];
-            box_sums_u8<B>(row + x * fh * B, fh, sums);
-            if (hmult) {
-#pragma unroll
-                for (int b = 0; b < B; ++b) vacc[b] += round_mult_u8(sums[b], hhalf, a.hmult);
-            } else {
-#pragma unroll
-                for (int b = 0; b < B; ++b) vacc[b] += round_mode_u8(sums[b], a.hmode, uint32_t(fh), a.hmult);
-            }
-        }
-        __syncthreads();
-        if (threadIdx.x == 0 && k + kRing < total) {
-            fence_proxy_async_smem();
-            issue(k + kRing);
-        }
-        if (++kv == fv) {
-            if (x < ncols) {
-                uint8_t o[B];
-#pragma unroll
-                for (int b = 0; b < B; ++b) o[b] = (uint8_t)round_mode_u8(vacc[b], a.vmode, uint32_t(fv), a.vmult);
-                if (a.unpremul_out) {
-#pragma unroll
-                    for (int b = 0; b < B - 1; ++b) o[b] = (uint8_t)unpremultiply_u8(o[b], o[B - 1]);
-                }
-                uint8_t* dst = a.out.data + (int64_t)oy * a.out.pitch + (int64_t)(c0 + x) * B;
-#pragma unroll
-                for (int b = 0; b < B; ++b) dst[b] = o[b];
-            }
-#pragma unroll
-            for (int b = 0; b < B; ++b) vacc[b] = 0;
-            kv = 0;
-            ++oy;
-        }
-    }
-    if (!ok) {
-        // wait (bounded) for the copies of this item still in flight
-        if (threadIdx.x == 0) {
-            const int32_t last = (k + kRing < total) ? k + kRing : total;
-            for (int32_t kk = k + 1; kk < last; ++kk)
-                mbar_wait(&bars[(pos + kk) & (kRing - 1)], uint32_t(((pos + kk) / kRing) & 1));
-        }
-        __syncthreads();
-        return false;
-    }
-    pos += total;
-    return true;
+// Control block at the start of the dynamic shared memory.
+struct BatchCtl {
+    WsRing ring;
+    uint64_t qfull[kQueue];   // producer published the entry (1 arrival)
+    uint64_t qempty[kQueue];  // consumers read the entry (1 arrival)
+    int32_t qidx[kQueue];     // work-list index, or >= n_items: no more work
+    int32_t cur;              // consumers: the item being processed
+    int32_t go;               // consumers: the item's dependency is satisfied
+    int32_t cstop;            // consumers: a bounded wait gave up
+    int32_t pstop;            // producer: a bounded wait gave up
+};
+
+// Band of output rows and column chunk of shrink item `index`.
+__device__ __forceinline__ void shrink_item_geom(const BatchStage& st, const ShrinkArgs& a, int32_t index,
+                                                 int32_t* oy0, int32_t* oy1, ShrinkChunk* c) {
+    const int32_t band = index / st.n_chunks;
+    *oy0 = band * st.rows_per_item;
+    *oy1 = min(a.out.h, *oy0 + st.rows_per_item);
+    *c = shrink_chunk(a, index - band * st.n_chunks);
 }
 
+__device__ __forceinline__ const uint8_t* shrink_source(const BatchArgs& g, const BatchStage& st) {
+    return st.in_src ? reinterpret_cast<const uint8_t*>(g.srcs[st.image]) : st.sh.in.data;
+}
+
+// Producer (one thread): claim items, publish them, stream shrink rows.
 template <int B>
-__device__ bool batch_shrink_item(const BatchStage& st, const ShrinkArgs& a, int32_t index, uint64_t* bars,
-                                  uint8_t* work, uint32_t stage_bytes, int64_t& pos, volatile int32_t* flag) {
-    const int32_t band = index / st.n_chunks;
-    int32_t c = index - band * st.n_chunks;
-    const int32_t oy0 = band * st.rows_per_item, oy1 = min(a.out.h, oy0 + st.rows_per_item);
-    const int32_t left = st.lo > 0 ? 1 : 0;
-    const int32_t n_int = st.hi > st.lo ? (st.hi - st.lo + st.chunk_cols - 1) / st.chunk_cols : 0;
-    int32_t c0, c1;
-    bool interior = false;
-    if (c < left) { c0 = 0; c1 = st.lo; }
-    else if (c - left < n_int) {
-        c0 = st.lo + (c - left) * st.chunk_cols;
-        c1 = min(st.hi, c0 + st.chunk_cols);
-        interior = true;
-    } else { c0 = st.hi; c1 = a.out.w; }
-    if (c1 <= c0 || oy1 <= oy0) return true;
-    // the bulk copy needs a 16-byte aligned source buffer
-    if (interior && (reinterpret_cast<uintptr_t>(a.in.data) & 15) == 0)
-        return batch_shrink_interior<B>(a, oy0, oy1, c0, c1 - c0, bars, work, stage_bytes, pos, flag);
-    // edge (or unaligned) columns: clamped loads, a few columns at a time
+__device__ bool produce_shrink(const BatchArgs& g, const BatchStage& st, int32_t index, BatchCtl* ctl, uint8_t* bufs,
+                               int& slot, uint32_t& ph, int64_t& issued) {
+    const uint8_t* in = shrink_source(g, st);
+    if ((reinterpret_cast<uintptr_t>(in) & 15) != 0) return true;  // consumers take the plain-load path
+    int32_t oy0, oy1;
+    ShrinkChunk c;
+    shrink_item_geom(st, st.sh, index, &oy0, &oy1, &c);
+    return ws_produce<B>(st.sh, in, oy0, oy1, c, &ctl->ring, bufs, g.ring_stage_bytes, g.ring_slots, slot, ph,
+                         issued);
+}
+
+template <bool RING>
+__device__ void batch_producer(const BatchArgs& g, BatchCtl* ctl, uint8_t* bufs) {
+    int q = 0;
+    uint32_t qph = 0;
+    int slot = 0;
+    uint32_t ph = 0;
+    int64_t issued = 0;
+    for (;;) {
+        if (!mbar_wait(&ctl->qempty[q], qph ^ 1u)) {
+            ctl->pstop = 1;
+            break;
+        }
+        const int32_t idx = ctl->pstop ? g.n_items : atomicAdd(g.cursor, 1);
+        ctl->qidx[q] = idx;
+        mbar_arrive(&ctl->qfull[q]);  // releases the qidx store
+        if (++q == kQueue) { q = 0; qph ^= 1u; }
+        if (idx >= g.n_items) break;
+        if constexpr (!RING) continue;
+        const WorkItem it = g.items[idx];
+        const BatchStage& st = g.stages[it.stage];
+        if (st.type != kBatchShrink) continue;
+        bool ok;
+        switch (st.sh.bands) {
+        case 1: ok = produce_shrink<1>(g, st, it.index, ctl, bufs, slot, ph, issued); break;
+        case 2: ok = produce_shrink<2>(g, st, it.index, ctl, bufs, slot, ph, issued); break;
+        case 3: ok = produce_shrink<3>(g, st, it.index, ctl, bufs, slot, ph, issued); break;
+        default: ok = produce_shrink<4>(g, st, it.index, ctl, bufs, slot, ph, issued); break;
+        }
+        if (!ok) {
+            ctl->pstop = 1;
+            atomicExch(g.err, VIPRS_ERR_TIMEOUT);
+            // publish an end marker if a queue slot frees, so consumers stop promptly
+            if (mbar_wait(&ctl->qempty[q], qph ^ 1u)) {
+                ctl->qidx[q] = g.n_items;
+                mbar_arrive(&ctl->qfull[q]);
+            }
+            break;
+        }
+    }
+    ws_drain(&ctl->ring, g.ring_slots, issued);
+}
+
+// Consumers: one shrink item.
+template <int B>
+__device__ bool consume_shrink(const BatchArgs& g, const BatchStage& st, int32_t index, BatchCtl* ctl,
+                               const uint8_t* bufs, uint8_t* work, int& slot, uint32_t& ph) {
+    const ShrinkArgs& a = st.sh;
+    int32_t oy0, oy1;
+    ShrinkChunk c;
+    shrink_item_geom(st, a, index, &oy0, &oy1, &c);
+    if ((reinterpret_cast<uintptr_t>(a.in.data) & 15) == 0)
+        return ws_consume<B, 2>(a, oy0, oy1, c, &ctl->ring, bufs, g.ring_stage_bytes, g.ring_slots, slot, ph,
+                             reinterpret_cast<volatile int32_t*>(&ctl->cstop));
+    // unaligned source: clamped plain loads, a few columns at a time
     const int32_t per_col = int32_t(a.fv) * int32_t(a.fh) * B;
-    const int32_t step = max(1, int32_t((kRing * stage_bytes - 64) / (per_col + B)));
+    const int32_t step = max(1, int32_t((g.work_bytes - 64) / (per_col + B)));
     for (int32_t oy = oy0; oy < oy1; ++oy)
-        for (int32_t x0 = c0; x0 < c1; x0 += step) shrink_edge_item_u8<B>(a, oy, x0, min(c1, x0 + step), work);
+        for (int32_t x0 = c.lx0; x0 < c.lx0 + c.ncols; x0 += step)
+            shrink_edge_item_u8<B>(a, oy, x0, min(c.lx0 + c.ncols, x0 + step), work);
     return true;
 }
 
@@ -160,7 +143,7 @@ __device__ void batch_pixel_row(const PixelArgs& a, int32_t ly) {
     const int bands = a.bands;
     const uint8_t* src = a.in.data + (int64_t)ly * a.in.pitch;
     uint8_t* dst = a.out.data + (int64_t)ly * a.out.pitch;
-    for (int32_t x = threadIdx.x; x < a.out.w; x += blockDim.x) {
+    for (int32_t x = threadIdx.x; x < a.out.w; x += kCThreads) {
         const uint8_t* s = src + (int64_t)x * bands;
         uint8_t* d = dst + (int64_t)x * bands;
         if (a.op == 0 || bands < 2) {
@@ -174,34 +157,38 @@ __device__ void batch_pixel_row(const PixelArgs& a, int32_t ly) {
     }
 }
 
-__global__ void __launch_bounds__(256) batch_kernel(BatchArgs g) {
-    extern __shared__ __align__(128) uint8_t smem_b[];
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem_b);
-    volatile int32_t* flag = reinterpret_cast<volatile int32_t*>(smem_b + 64);
-    volatile int32_t* sidx = reinterpret_cast<volatile int32_t*>(smem_b + 72);
-    BatchStage* sst = reinterpret_cast<BatchStage*>(smem_b + 128);
-    uint8_t* work = smem_b + 128 + ((sizeof(BatchStage) + 127) / 128) * 128;
-    if (threadIdx.x == 0) {
-        for (int i = 0; i < kRing; ++i) mbar_init(&bars[i], 1);
-        *flag = 0;
-        mbar_fence_init();
-    }
-    __syncthreads();
-    int64_t pos = 0;
+template <bool RING>
+__device__ void batch_consumers(const BatchArgs& g, BatchCtl* ctl, BatchStage* sst, const uint8_t* bufs,
+                                uint8_t* work) {
+    int q = 0;
+    uint32_t qph = 0;
+    int slot = 0;
+    uint32_t ph = 0;
     for (;;) {
-        if (threadIdx.x == 0) *sidx = atomicAdd(g.cursor, 1);
-        __syncthreads();
-        const int32_t idx = *sidx;
+        // next queue entry: one thread waits, everyone reads the same answer
+        // (decisions that every consumer takes are read from fields that only
+        // thread 0 writes before the barrier and nobody rewrites until all
+        // consumers have passed the next barrier: `cur` and `go`)
+        if (threadIdx.x == 0) {
+            int32_t idx = g.n_items;
+            if (!ctl->cstop) {
+                if (mbar_wait(&ctl->qfull[q], qph)) idx = ctl->qidx[q];
+                else ctl->cstop = 1;
+            }
+            ctl->cur = idx;
+        }
+        csync();
+        const int32_t idx = ctl->cur;
         if (idx >= g.n_items) break;
         const WorkItem it = g.items[idx];
-        // stage descriptor into shared memory, plane pointers resolved for this launch
         {
             const uint32_t* src = reinterpret_cast<const uint32_t*>(g.stages + it.stage);
             uint32_t* dst = reinterpret_cast<uint32_t*>(sst);
-            for (int i = threadIdx.x; i < int(sizeof(BatchStage) / 4); i += blockDim.x) dst[i] = src[i];
+            for (int i = threadIdx.x; i < int(sizeof(BatchStage) / 4); i += kCThreads) dst[i] = src[i];
         }
-        __syncthreads();
+        csync();
         if (threadIdx.x == 0) {
+            mbar_arrive(&ctl->qempty[q]);
             BatchStage& s = *sst;
             const uint8_t* in = reinterpret_cast<const uint8_t*>(g.srcs[s.image]);
             uint8_t* out = reinterpret_cast<uint8_t*>(g.dsts[s.image]);
@@ -209,6 +196,7 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchArgs g) {
             if (s.out_dst) {
                 s.sh.out.data = out; s.r2.out.data = out; s.px.out.data = out; s.af.out.data = out; s.rd.out.data = out;
             }
+            ctl->go = 1;
             if (s.dep >= 0) {
                 bool done = ld_acquire_i32(g.counters + s.dep) >= s.dep_items;
                 const uint64_t t0 = global_ns();
@@ -218,24 +206,27 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchArgs g) {
                     else if ((i & 63) == 63 && global_ns() - t0 > kWaitLimitNs) break;
                 }
                 if (!done) {
-                    *flag = 1;
+                    ctl->cstop = 1;
+                    ctl->go = 0;
                     atomicExch(g.err, VIPRS_ERR_TIMEOUT);
                 }
             }
         }
-        __syncthreads();
-        if (*flag) break;
+        if (++q == kQueue) { q = 0; qph ^= 1u; }
+        csync();
+        if (!ctl->go) break;
         const BatchStage& s = *sst;
         bool ok = true;
-        switch (s.type) {
-        case kBatchShrink:
+        if constexpr (RING) {
+            // a ring launch runs shrink items only
             switch (s.sh.bands) {
-            case 1: ok = batch_shrink_item<1>(s, s.sh, it.index, bars, work, g.ring_stage_bytes, pos, flag); break;
-            case 2: ok = batch_shrink_item<2>(s, s.sh, it.index, bars, work, g.ring_stage_bytes, pos, flag); break;
-            case 3: ok = batch_shrink_item<3>(s, s.sh, it.index, bars, work, g.ring_stage_bytes, pos, flag); break;
-            default: ok = batch_shrink_item<4>(s, s.sh, it.index, bars, work, g.ring_stage_bytes, pos, flag); break;
+            case 1: ok = consume_shrink<1>(g, s, it.index, ctl, bufs, work, slot, ph); break;
+            case 2: ok = consume_shrink<2>(g, s, it.index, ctl, bufs, work, slot, ph); break;
+            case 3: ok = consume_shrink<3>(g, s, it.index, ctl, bufs, work, slot, ph); break;
+            default: ok = consume_shrink<4>(g, s, it.index, ctl, bufs, work, slot, ph); break;
             }
-            break;
+        } else {
+        switch (s.type) {
         case kBatchReduce2D: {
             const int nbx = (s.r2.out.w + s.r2.tile_w - 1) / s.r2.tile_w;
             const int tbx = it.index % nbx, tby = it.index / nbx;
@@ -245,11 +236,11 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchArgs g) {
             break;
         }
         case kBatchAffine:
-            for (int32_t x = threadIdx.x; x < s.af.out.w; x += blockDim.x) affine_pixel<uint8_t>(s.af, x, it.index);
+            for (int32_t x = threadIdx.x; x < s.af.out.w; x += kCThreads) affine_pixel<uint8_t>(s.af, x, it.index);
             break;
         case kBatchReduceH:
         case kBatchReduceV: {
-            const int32_t chunks = (s.rd.out.w * s.rd.bands + 255) / 256;
+            const int32_t chunks = (s.rd.out.w * s.rd.bands + kCThreads - 1) / kCThreads;
             const int32_t oy = it.index / chunks, ch = it.index - oy * chunks;
             if (s.type == kBatchReduceH) reduce_h_chunk<uint8_t, kReduceFixed>(s.rd, ch, oy, work);
             else reduce_v_chunk<uint8_t, kReduceFixed>(s.rd, ch, oy, work);
@@ -259,33 +250,66 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchArgs g) {
             batch_pixel_row(s.px, it.index);
             break;
         }
-        if (!ok) {
-            if (threadIdx.x == 0) atomicExch(g.err, VIPRS_ERR_TIMEOUT);
-            break;
         }
-        __syncthreads();
-        if (threadIdx.x == 0) {
+        if (!ok && threadIdx.x == 0) atomicExch(g.err, VIPRS_ERR_TIMEOUT);
+        csync();  // the item's stores are done in every consumer
+        // a timed-out item is not published; the loop top then stops this block
+        if (threadIdx.x == 0 && !ctl->cstop) {
             __threadfence();
             atomicAdd(g.counters + it.stage, 1);
         }
     }
 }
 
+// RING: a launch of shrink items (the ring in shared memory); otherwise a
+// launch of the other item kinds (the work region in shared memory).
+template <bool RING>
+__global__ void __launch_bounds__(kWsThreads, 3) batch_kernel(BatchArgs g) {
+    extern __shared__ __align__(128) uint8_t smem_b[];
+    BatchCtl* ctl = reinterpret_cast<BatchCtl*>(smem_b);
+    const size_t ctl_bytes = (sizeof(BatchCtl) + 127) / 128 * 128;
+    BatchStage* sst = reinterpret_cast<BatchStage*>(smem_b + ctl_bytes);
+    uint8_t* bufs = smem_b + ctl_bytes + (sizeof(BatchStage) + 127) / 128 * 128;
+    uint8_t* work = bufs + (size_t)g.ring_slots * g.ring_stage_bytes;
+    if (threadIdx.x == 0) {
+        if (RING) ws_ring_init(&ctl->ring, g.ring_slots);
+        for (int i = 0; i < kQueue; ++i) {
+            mbar_init(&ctl->qfull[i], 1);
+            mbar_init(&ctl->qempty[i], 1);
+        }
+        ctl->cstop = 0;
+        ctl->pstop = 0;
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x >= kCThreads) {
+        if (threadIdx.x == kCThreads) batch_producer<RING>(g, ctl, bufs);
+        return;
+    }
+    batch_consumers<RING>(g, ctl, sst, bufs, work);
+}
+
 }  // namespace dev
 
 namespace launch {
 
-int batch_blocks_per_sm(size_t smem) {
-    cudaFuncSetAttribute(dev::batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+size_t batch_ctl_bytes() {
+    return (sizeof(dev::BatchCtl) + 127) / 128 * 128 + (sizeof(BatchStage) + 127) / 128 * 128;
+}
+
+int batch_blocks_per_sm(size_t smem, bool ring) {
+    void (*k)(BatchArgs) = ring ? dev::batch_kernel<true> : dev::batch_kernel<false>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::batch_kernel, 256, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, dev::kWsThreads, smem);
     return per_sm;
 }
 
-cudaError_t batch(const BatchArgs& a, int grid, cudaStream_t s) {
+cudaError_t batch(const BatchArgs& a, int grid, bool ring, cudaStream_t s) {
     if (a.n_items <= 0) return cudaSuccess;
-    cudaFuncSetAttribute(dev::batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.smem_bytes);
-    dev::batch_kernel<<<grid, 256, a.smem_bytes, s>>>(a);
+    void (*k)(BatchArgs) = ring ? dev::batch_kernel<true> : dev::batch_kernel<false>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.smem_bytes);
+    k<<<grid, dev::kWsThreads, a.smem_bytes, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -1,13 +1,14 @@
 // batch_launch.hpp -- descriptors of the persistent batched-thumbnail kernel.
 //
-// A batch is many thumbnail plans (one per image) executed by ONE persistent
-// launch that walks a device work list.  Every stage of every image plan
-// becomes a BatchStage; its work is split into items (shrink: output row x
-// column chunk; fused reduce: output tile; affine / pixel: output row).  A
-// stage that consumes another stage's output waits (bounded) until that
-// stage's completion counter reaches its item count.  The list is ordered so
-// that every item a stage waits for precedes it: blocks claim items in list
-// order, so every awaited item is already owned by a running block.
+// A batch is many thumbnail plans (one per image) executed by a few
+// persistent launches that walk a device work list.  Every stage of every
+// image plan becomes a BatchStage; its work is split into items (shrink: band
+// of output rows x column chunk; fused reduce: output tile; affine / pixel:
+// output row).  Stages are grouped by level (shrink, then the stage after it,
+// ...) and each level runs as one launch of its shrink items and one of its
+// other items, so a stage's input is complete when its launch starts.  The
+// dependency fields (dep, dep_items, counters) support a bounded in-kernel
+// wait for lists that mix levels; the level launches leave them unused.
 #pragma once
 
 #include <cstdint>
@@ -54,15 +55,20 @@ struct BatchArgs {
     int32_t* err = nullptr;       // first error (timeout) seen by any block
     const uint64_t* srcs = nullptr;  // device array: source pointer of each image
     const uint64_t* dsts = nullptr;  // device array: destination pointer of each image
-    uint32_t ring_stage_bytes = 0;   // shrink ring buffer size
-    uint32_t smem_bytes = 0;
+    uint32_t ring_stage_bytes = 0;   // bytes of one shrink ring slot
+    int32_t ring_slots = 0;          // slots of the shrink ring
+    uint32_t work_bytes = 0;         // shared memory of the other item kinds
+    uint32_t smem_bytes = 0;         // control block + stage copy + ring + work
 };
 
 namespace launch {
-// Launch the persistent kernel on `grid` blocks.
-cudaError_t batch(const BatchArgs& a, int grid, cudaStream_t s);
+// Launch the persistent kernel on `grid` blocks: the shrink-ring variant
+// (`ring`) or the variant for the other item kinds.
+cudaError_t batch(const BatchArgs& a, int grid, bool ring, cudaStream_t s);
 // Largest resident block count per SM for `smem` bytes of shared memory.
-int batch_blocks_per_sm(size_t smem);
+int batch_blocks_per_sm(size_t smem, bool ring);
+// Shared memory ahead of the ring: control block and the item's stage copy.
+size_t batch_ctl_bytes();
 }  // namespace launch
 
 }  // namespace viprs

@@ -21,32 +21,45 @@
 
 using namespace viprs;
 
+// One launch of the persistent kernel: a contiguous range of the work list.
+struct BatchLaunch {
+    bool ring = false;        // shrink items through the TMA ring
+    int64_t offset = 0, count = 0;
+    int32_t ring_slots = 0;
+    uint32_t work_bytes = 0;
+    size_t smem = 0;
+    int grid = 0;
+};
+
 struct viprs_batch {
     int n = 0;
     std::vector<uint32_t> w, h, bands;
     std::vector<viprs_plan*> plans;
     // knobs (autotuned)
     uint32_t ring_target = 8192;  // source bytes per shrink row segment
-    int32_t lag_blocks = 2;       // work-list lag between an image's stages, in grids
-    int32_t blocks_per_sm = 0;    // 0 = occupancy maximum
-    uint32_t reduce_smem_budget = 48 * 1024;  // shared memory of one fused-reduce tile
+    int32_t ring_slots_knob = 0;  // ring slots per block (0: ring_total / slot size)
+    int32_t blocks_per_sm = 0;    // cap of the shrink launches (0 = occupancy maximum)
+    uint32_t reduce_smem_budget = 40 * 1024;  // shared memory of one fused-reduce tile
     int64_t item_bytes = 96 * 1024;           // source bytes per shrink work item
+    uint32_t ring_total = 56 * 1024;          // shrink ring bytes per block (auto slots)
     // device work list
     std::vector<BatchStage> stages;
     std::vector<WorkItem> items;
+    std::vector<BatchLaunch> launches;
     BatchStage* d_stages = nullptr;
     WorkItem* d_items = nullptr;
     int32_t* d_counters = nullptr;
-    int32_t* d_ctrl = nullptr;  // [0] cursor, [1] error
+    int32_t* d_ctrl = nullptr;  // [0] error, [1 + k] cursor of launch k
     size_t counters_cap = 0, stages_cap = 0, items_cap = 0;
     uint32_t ring_stage_bytes = 0;
-    size_t smem = 0;
-    int grid = 0;
+    size_t edge_bytes = 0;
     // captured graph
     cudaGraphExec_t graph = nullptr;
     const uint64_t* graph_srcs = nullptr;
     const uint64_t* graph_dsts = nullptr;
 };
+
+constexpr int kMaxLaunches = 64;
 
 namespace {
 
@@ -94,20 +107,22 @@ int plan_stages(viprs_batch* b, int image, std::vector<std::vector<BatchStage>>*
             int32_t lo, hi;
             launch::shrink_prepare(&bs.sh, &lo, &hi);
             bs.lo = lo; bs.hi = hi;
+            // column chunks partition the output columns (clamped boxes at the
+            // edges, as in the standalone kernel); one consumer thread per column
             const int64_t per_col = int64_t(bs.sh.fh) * p->bands;
-            bs.chunk_cols = int32_t(std::max<int64_t>(1, std::min<int64_t>(256, b->ring_target / std::max<int64_t>(per_col, 1))));
-            const int32_t n_int = hi > lo ? (hi - lo + bs.chunk_cols - 1) / bs.chunk_cols : 0;
-            bs.n_chunks = (lo > 0 ? 1 : 0) + n_int + (hi < outp.w ? 1 : 0);
-            // output rows per item: about `item_bytes` of source per item, so
-            // that the ring's start-up latency is paid once per many rows
+            bs.chunk_cols = int32_t(std::max<int64_t>(1, std::min<int64_t>(512, b->ring_target / std::max<int64_t>(per_col, 1))));
+            bs.sh.nxf = bs.chunk_cols;
+            bs.n_chunks = (outp.w + bs.chunk_cols - 1) / bs.chunk_cols;
+            // output rows per item: about `item_bytes` of source per item
             const int64_t row_src = int64_t(bs.chunk_cols) * per_col * bs.sh.fv;
             bs.rows_per_item = int32_t(std::max<int64_t>(1, std::min<int64_t>(outp.h, b->item_bytes / std::max<int64_t>(row_src, 1))));
             bs.n_items = ((outp.h + bs.rows_per_item - 1) / bs.rows_per_item) * bs.n_chunks;
             const uint32_t need = uint32_t((bs.chunk_cols * per_col + 32 + 15 + 127) / 128 * 128);
             b->ring_stage_bytes = std::max(b->ring_stage_bytes, need);
-            // the edge routine stages fv x fh source pixels of one output column in the ring
+            // the plain-load routine (unaligned sources) stages fv x fh source
+            // pixels of at least one output column in the work region
             const int64_t edge = int64_t(bs.sh.fv) * per_col + p->bands + 64;
-            b->ring_stage_bytes = std::max(b->ring_stage_bytes, uint32_t((edge / 4 + 1 + 127) / 128 * 128));
+            b->edge_bytes = std::max<size_t>(b->edge_bytes, size_t(edge + 64));
             break;
         }
         case StageType::Reduce2D: {
@@ -179,73 +194,86 @@ int plan_stages(viprs_batch* b, int image, std::vector<std::vector<BatchStage>>*
 size_t reduce2d_need(const Reduce2DArgs& a) { return launch::reduce2d_smem_bytes(a); }
 
 // Build the device work list for the current knobs.
+//
+// Stages are grouped into levels: a shrink runs at level 0, the stage after it
+// at level 1, and so on; a chain that does not start with a shrink starts at
+// level 1, so that each level holds one kind of work.  Each level becomes one
+// launch of its shrink items (the ring variant) and one of its other items
+// (the tile variant).  A stage reads only stages of lower levels, so launch
+// order in the stream is the whole dependency structure: no item waits.
 int build_list(viprs_batch* b) {
     b->ring_stage_bytes = 0;
+    b->edge_bytes = 0;
     std::vector<std::vector<BatchStage>> per(size_t(b->n));
     for (int i = 0; i < b->n; ++i) {
         const int st = plan_stages(b, i, &per);
         if (st) return st;
     }
     b->ring_stage_bytes = std::max<uint32_t>(b->ring_stage_bytes, 256);
-    // shared memory: ring buffers, edge scratch, fused-reduce tiles
-    size_t work = size_t(4) * b->ring_stage_bytes;
-    for (auto& v : per)
-        for (auto& s : v)
-            if (s.type == kBatchReduce2D) work = std::max(work, reduce2d_need(s.r2));
-            else if (s.type == kBatchReduceH || s.type == kBatchReduceV)
-                work = std::max(work, size_t(65 * s.rd.taps * 2 + 15) / 16 * 16 + 256);
-    b->smem = 128 + (sizeof(BatchStage) + 127) / 128 * 128 + work + 64;
-    if (b->smem > 200 * 1024) return VIPRS_ERR_INVALID_ARGUMENT;
-    int per_sm = launch::batch_blocks_per_sm(b->smem);
-    if (per_sm <= 0) return VIPRS_ERR_INVALID_ARGUMENT;
-    if (b->blocks_per_sm > 0) per_sm = std::min(per_sm, b->blocks_per_sm);
-    b->grid = per_sm * sm_count();
+    const int32_t ring_slots = b->ring_slots_knob > 0
+        ? std::min(b->ring_slots_knob, 16)
+        : int32_t(std::min<int64_t>(16, std::max<int64_t>(3, int64_t(b->ring_total) / b->ring_stage_bytes)));
 
-    // flatten: global stage index, dependency on the image's previous stage
+    // flatten the stages; levels
     b->stages.clear();
-    std::vector<std::vector<int>> gidx(size_t(b->n));
+    std::vector<std::vector<int>> gidx(size_t(b->n)), level(size_t(b->n));
+    int max_level = 0;
     for (int i = 0; i < b->n; ++i) {
+        const int shift = (!per[size_t(i)].empty() && per[size_t(i)][0].type != kBatchShrink) ? 1 : 0;
         for (size_t j = 0; j < per[size_t(i)].size(); ++j) {
             BatchStage s = per[size_t(i)][j];
-            if (j > 0) {
-                s.dep = gidx[size_t(i)][j - 1];
-                s.dep_items = b->stages[size_t(s.dep)].n_items;
-            }
+            s.dep = -1;  // ordered by the launches
             gidx[size_t(i)].push_back(int(b->stages.size()));
+            level[size_t(i)].push_back(int(j) + shift);
+            max_level = std::max(max_level, int(j) + shift);
             b->stages.push_back(s);
         }
     }
-    // work list: images large first; an image's next stage is emitted once
-    // `lag` further items have been emitted after its previous stage, so that
-    // a block claiming it rarely waits and the producer's output is still in L2
+    // images large first inside every launch (the long items start early)
     std::vector<int> order(size_t(b->n));
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
         return uint64_t(b->w[size_t(x)]) * b->h[size_t(x)] * b->bands[size_t(x)] >
                uint64_t(b->w[size_t(y)]) * b->h[size_t(y)] * b->bands[size_t(y)];
     });
-    const int64_t lag = int64_t(std::max(b->lag_blocks, 0)) * b->grid;
-    struct Pending { int image; size_t j; int64_t ready_at; };
-    std::deque<Pending> pending;
     b->items.clear();
-    auto emit = [&](int image, size_t j) {
-        const int g = gidx[size_t(image)][j];
-        for (int32_t k = 0; k < b->stages[size_t(g)].n_items; ++k) b->items.push_back(WorkItem{g, k});
-        if (j + 1 < gidx[size_t(image)].size())
-            pending.push_back(Pending{image, j + 1, int64_t(b->items.size()) + lag});
-    };
-    auto flush = [&](bool all) {
-        while (!pending.empty() && (all || pending.front().ready_at <= int64_t(b->items.size()))) {
-            Pending q = pending.front();
-            pending.pop_front();
-            emit(q.image, q.j);
+    b->launches.clear();
+    const size_t ctl = launch::batch_ctl_bytes();
+    for (int L = 0; L <= max_level; ++L) {
+        for (int kind = 0; kind < 2; ++kind) {
+            const bool ring = kind == 0;
+            BatchLaunch l;
+            l.ring = ring;
+            l.offset = int64_t(b->items.size());
+            size_t work = 0;
+            for (int image : order) {
+                for (size_t j = 0; j < gidx[size_t(image)].size(); ++j) {
+                    if (level[size_t(image)][j] != L) continue;
+                    const int g = gidx[size_t(image)][j];
+                    const BatchStage& s = b->stages[size_t(g)];
+                    if ((s.type == kBatchShrink) != ring) continue;
+                    for (int32_t k = 0; k < s.n_items; ++k) b->items.push_back(WorkItem{g, k});
+                    if (s.type == kBatchShrink) work = std::max(work, b->edge_bytes);
+                    else if (s.type == kBatchReduce2D) work = std::max(work, reduce2d_need(s.r2));
+                    else if (s.type == kBatchReduceH || s.type == kBatchReduceV)
+                        work = std::max(work, size_t(65 * s.rd.taps * 2 + 15) / 16 * 16 + 256);
+                    else work = std::max<size_t>(work, 1024);
+                }
+            }
+            l.count = int64_t(b->items.size()) - l.offset;
+            if (l.count == 0) continue;
+            if (int(b->launches.size()) >= kMaxLaunches) return VIPRS_ERR_UNSUPPORTED_FORMAT;
+            l.work_bytes = uint32_t((std::max<size_t>(work, 256) + 127) / 128 * 128);
+            l.ring_slots = ring ? ring_slots : 0;
+            l.smem = ctl + size_t(l.ring_slots) * b->ring_stage_bytes + l.work_bytes;
+            if (l.smem > 220 * 1024) return VIPRS_ERR_INVALID_ARGUMENT;
+            int per_sm = launch::batch_blocks_per_sm(l.smem, ring);
+            if (per_sm <= 0) return VIPRS_ERR_INVALID_ARGUMENT;
+            if (ring && b->blocks_per_sm > 0) per_sm = std::min(per_sm, b->blocks_per_sm);
+            l.grid = int(std::min<int64_t>(int64_t(per_sm) * sm_count(), l.count));
+            b->launches.push_back(l);
         }
-    };
-    for (int image : order) {
-        if (!gidx[size_t(image)].empty()) emit(image, 0);
-        flush(false);
     }
-    flush(true);
 
     // upload
     if (b->stages.size() > b->stages_cap || b->items.size() > b->items_cap || b->stages.size() > b->counters_cap) {
@@ -265,20 +293,27 @@ int build_list(viprs_batch* b) {
 
 int launch_batch(viprs_batch* b, const uint64_t* d_srcs, const uint64_t* d_dsts, cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(b->d_counters, 0, b->stages.size() * sizeof(int32_t), s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_ctrl, 0, 2 * sizeof(int32_t), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_ctrl, 0, (1 + b->launches.size()) * sizeof(int32_t), s);
     if (e != cudaSuccess) return cuda_status(e);
-    BatchArgs a;
-    a.stages = b->d_stages;
-    a.items = b->d_items;
-    a.n_items = int32_t(b->items.size());
-    a.counters = b->d_counters;
-    a.cursor = b->d_ctrl;
-    a.err = b->d_ctrl + 1;
-    a.srcs = d_srcs;
-    a.dsts = d_dsts;
-    a.ring_stage_bytes = b->ring_stage_bytes;
-    a.smem_bytes = uint32_t(b->smem);
-    return cuda_status(launch::batch(a, b->grid, s));
+    for (size_t k = 0; k < b->launches.size(); ++k) {
+        const BatchLaunch& l = b->launches[k];
+        BatchArgs a;
+        a.stages = b->d_stages;
+        a.items = b->d_items + l.offset;
+        a.n_items = int32_t(l.count);
+        a.counters = b->d_counters;
+        a.cursor = b->d_ctrl + 1 + k;
+        a.err = b->d_ctrl;
+        a.srcs = d_srcs;
+        a.dsts = d_dsts;
+        a.ring_stage_bytes = b->ring_stage_bytes;
+        a.ring_slots = l.ring_slots;
+        a.work_bytes = l.work_bytes;
+        a.smem_bytes = uint32_t(l.smem);
+        e = launch::batch(a, l.grid, l.ring, s);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    return VIPRS_OK;
 }
 
 }  // namespace
@@ -307,7 +342,7 @@ int32_t viprs_thumbnail_batch_create(int32_t n, const uint32_t* widths, const ui
         if (st == VIPRS_OK) st = create_chain_plan(widths[i], heights[i], bands[i], VIPRS_U8, c, &b->plans[size_t(i)]);
     }
     if (st == VIPRS_OK) {
-        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->d_ctrl), 4 * sizeof(int32_t));
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->d_ctrl), (1 + kMaxLaunches) * sizeof(int32_t));
         st = cuda_status(e);
     }
     if (st == VIPRS_OK) st = build_list(b.get());
@@ -331,7 +366,11 @@ int32_t viprs_batch_work_items(const viprs_batch* b, int32_t* items, int32_t* st
     if (!b) return VIPRS_ERR_NULL_POINTER;
     if (items) *items = int32_t(b->items.size());
     if (stages) *stages = int32_t(b->stages.size());
-    if (grid) *grid = b->grid;
+    if (grid) {
+        int g = 0;
+        for (const auto& l : b->launches) g = std::max(g, l.grid);
+        *grid = g;
+    }
     return VIPRS_OK;
 }
 
@@ -378,7 +417,7 @@ int32_t viprs_batch_execute_per_image(viprs_batch* b, const uint64_t* h_srcs, co
 
 int32_t viprs_batch_launch_count(const viprs_batch* b, int32_t* batched, int32_t* per_image) {
     if (!b) return VIPRS_ERR_NULL_POINTER;
-    if (batched) *batched = 1;
+    if (batched) *batched = int32_t(b->launches.size());
     if (per_image) {
         int32_t n = 0;
         for (auto* p : b->plans) n += int32_t(p->stages.size());
@@ -387,20 +426,21 @@ int32_t viprs_batch_launch_count(const viprs_batch* b, int32_t* batched, int32_t
     return VIPRS_OK;
 }
 
-int32_t viprs_batch_set_config(viprs_batch* b, uint32_t ring_bytes, int32_t lag_blocks, int32_t blocks_per_sm) {
+int32_t viprs_batch_set_config(viprs_batch* b, uint32_t ring_bytes, int32_t ring_slots, int32_t blocks_per_sm) {
     if (!b) return VIPRS_ERR_NULL_POINTER;
-    if (ring_bytes < 256 || ring_bytes > 32768 || lag_blocks < 0 || blocks_per_sm < 0) return VIPRS_ERR_INVALID_ARGUMENT;
+    if (ring_bytes < 256 || ring_bytes > 32768 || ring_slots < 0 || ring_slots > 16 || blocks_per_sm < 0)
+        return VIPRS_ERR_INVALID_ARGUMENT;
     b->ring_target = ring_bytes;
-    b->lag_blocks = lag_blocks;
+    b->ring_slots_knob = ring_slots;
     b->blocks_per_sm = blocks_per_sm;
     drop_graph(b);
     return build_list(b);
 }
 
-int32_t viprs_batch_get_config(const viprs_batch* b, uint32_t* ring_bytes, int32_t* lag_blocks, int32_t* blocks_per_sm) {
+int32_t viprs_batch_get_config(const viprs_batch* b, uint32_t* ring_bytes, int32_t* ring_slots, int32_t* blocks_per_sm) {
     if (!b) return VIPRS_ERR_NULL_POINTER;
     if (ring_bytes) *ring_bytes = b->ring_target;
-    if (lag_blocks) *lag_blocks = b->lag_blocks;
+    if (ring_slots) *ring_slots = b->ring_slots_knob;
     if (blocks_per_sm) *blocks_per_sm = b->blocks_per_sm;
     return VIPRS_OK;
 }
@@ -409,12 +449,12 @@ int32_t viprs_batch_autotune(viprs_batch* b, const uint64_t* d_srcs, const uint6
                              int32_t repeats, float* best_ms) {
     if (!b || !d_srcs || !d_dsts) return VIPRS_ERR_NULL_POINTER;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const uint32_t rings[] = {4096, 8192, 16384};
-    const int32_t lags[] = {1, 2, 4};
-    const int32_t caps[] = {0, 3};
+    const uint32_t rings[] = {8192, 12288, 16384, 24576};
+    const int32_t lags[] = {0, 3, 4, 6};  // ring slots (0: from the ring budget)
+    const int32_t caps[] = {0, 2, 3};
     float best = 1e30f;
     uint32_t br = b->ring_target;
-    int32_t bl = b->lag_blocks, bc = b->blocks_per_sm;
+    int32_t bl = b->ring_slots_knob, bc = b->blocks_per_sm;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -443,10 +483,10 @@ int32_t viprs_batch_status(viprs_batch* b, void* stream) {
     if (!b) return VIPRS_ERR_NULL_POINTER;
     cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return cuda_status(e);
-    int32_t h[2] = {0, 0};
-    e = cudaMemcpy(h, b->d_ctrl, sizeof(h), cudaMemcpyDeviceToHost);
+    int32_t h = 0;
+    e = cudaMemcpy(&h, b->d_ctrl, sizeof(h), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_status(e);
-    return h[1];
+    return h;
 }
 
 void viprs_batch_destroy(viprs_batch* b) {

@@ -13,6 +13,14 @@ namespace viprs {
 namespace dev {
 
 constexpr int kShrinkThreads = 256;
+
+// The routines below that a whole block runs together (the fused reduce
+// tile, the reduce row chunks, the shrink edge items) use kCThreads threads
+// (0..255) and barrier 1 for 256 threads: the standalone kernels launch
+// exactly 256 threads, and the persistent batch kernel adds a producer warp
+// (threads 256..287) that never joins barrier 1.
+constexpr int kCThreads = 256;
+__device__ __forceinline__ void csync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 constexpr int kShrinkMaxItems = 4;  // (column, band) outputs per thread
 constexpr int kShrinkSegCap = 16384;  // target staging bytes per input row
 
@@ -299,7 +307,7 @@ __device__ __forceinline__ void box_sums_u8(const uint8_t* p, int fh, uint32_t (
 // Premultiply<U8> in place over `npx` staged pixels of B bands (alpha last).
 template <int B>
 __device__ __forceinline__ void premultiply_pixels(uint8_t* seg, int npx) {
-    for (int p = threadIdx.x; p < npx; p += blockDim.x) {
+    for (int p = threadIdx.x; p < npx; p += kCThreads) {
         uint8_t* px = seg + p * B;
         const uint32_t a = px[B - 1];
 #pragma unroll
@@ -317,19 +325,19 @@ __device__ void shrink_edge_item_u8(const ShrinkArgs& a, int32_t oy, int32_t c0,
     const int32_t ncols = c1 - c0;
     const int32_t per_row = ncols * fh * B;
     const int64_t Y = a.out.y0 + oy;
-    for (int32_t i = threadIdx.x; i < fv * per_row; i += blockDim.x) {
+    for (int32_t i = threadIdx.x; i < fv * per_row; i += kCThreads) {
         const int32_t k = i / per_row, rem = i - k * per_row;
         const int32_t xb = rem / B, b = rem - xb * B;
         const int64_t sx = (a.out.x0 + c0) * (int64_t)fh + xb - a.in.x0;
         buf[i] = load_sample<uint8_t>(a.in, sx, Y * fv + k - a.in.y0, B, b);
     }
-    __syncthreads();
+    csync();
     if (a.premul_in) {
         premultiply_pixels<B>(buf, fv * ncols * fh);
-        __syncthreads();
+        csync();
     }
     uint8_t* ob = buf + fv * per_row;
-    for (int32_t item = threadIdx.x; item < ncols * B; item += blockDim.x) {
+    for (int32_t item = threadIdx.x; item < ncols * B; item += kCThreads) {
         const int32_t x = item / B, b = item - x * B;
         uint32_t vs = 0;
         for (int32_t k = 0; k < fv; ++k) {
@@ -340,15 +348,15 @@ __device__ void shrink_edge_item_u8(const ShrinkArgs& a, int32_t oy, int32_t c0,
         }
         ob[item] = (uint8_t)round_mode_u8(vs, a.vmode, uint32_t(fv), a.vmult);
     }
-    __syncthreads();
+    csync();
     uint8_t* orow = a.out.data + (int64_t)oy * a.out.pitch + (int64_t)c0 * B;
-    for (int32_t item = threadIdx.x; item < ncols * B; item += blockDim.x) {
+    for (int32_t item = threadIdx.x; item < ncols * B; item += kCThreads) {
         const int32_t x = item / B, b = item - x * B;
         uint32_t v = ob[item];
         if (a.unpremul_out && b != B - 1) v = unpremultiply_u8(v, ob[x * B + B - 1]);
         orow[item] = (uint8_t)v;
     }
-    __syncthreads();
+    csync();
 }
 
 // Box sums of output pixels whose box leaves the plane (the reduce halo):
@@ -393,162 +401,287 @@ __device__ __forceinline__ ShrinkChunk shrink_chunk(const ShrinkArgs& a, int32_t
     return k;
 }
 
-// ShrinkH then ShrinkV over u8.  Items are (output row, column chunk); the
-// chunks partition the output columns, and a block owns every G-th item.  One
-// thread per block fetches each source row segment of its items (the chunk's
-// boxes, clamped into the plane) with a TMA bulk copy into a ring of S
-// shared-memory buffers; the ring runs across item boundaries, so S rows are
-// in flight while the block sums the current one.  Each thread owns one output
-// pixel of the chunk: boxes inside the plane are summed four bytes at a time
-// (box_sums_u8); boxes reaching past an edge (the reduce halo) sum clamped
-// columns.  Every source byte is read from HBM once.  B is the band count.
-// The host picks the chunk count and blocks per SM so that the item count
-// matches the resident grid.
+// ---------------------------------------------------------------- warp-specialised shrink ring
+//
+// ShrinkH then ShrinkV over u8, streaming source row segments through a ring
+// of shared-memory slots.  A producer warp (thread kCThreads, one elected
+// thread) issues one TMA bulk copy (`cp.async.bulk`, no multicast) per source
+// row segment into the next free slot; eight consumer warps (threads 0..255)
+// each own one output pixel of the current column chunk and sum its box as
+// rows land.  Slots hand over through mbarriers only -- `full` (the copy's
+// transaction bytes) and `empty` (one arrival per consumer warp) -- so there
+// is no block-wide barrier per row and the ring runs across item boundaries.
+// Every wait is bounded; a consumer that gives up stops waiting (and raises
+// `stop`), the producer stops issuing, and before it exits the producer waits
+// (bounded) for the copies it still has in flight.
+
+constexpr int kWsThreads = kCThreads + 32;
+constexpr int kConsumerWarps = kCThreads / 32;
+constexpr int kMaxRing = 16;
+
+struct WsRing {
+    uint64_t full[kMaxRing];
+    uint64_t empty[kMaxRing];
+    int32_t lead[kMaxRing];  // offset of the row's first byte within its slot
+};
+
+__device__ __forceinline__ void ws_ring_init(WsRing* r, int S) {
+    for (int i = 0; i < S; ++i) {
+        mbar_init(&r->full[i], 1);
+        mbar_init(&r->empty[i], kConsumerWarps);
+    }
+}
+
+// Producer: plane bytes [s0, s0 + n) -> slot `dst`, completing on `bar`.  The
+// 16-byte aligned cover goes by one bulk copy; bytes whose cover would pass
+// the end of the buffer go by plain loads first.  `lead` gets s0's offset in
+// the slot before the arrival publishes it.
+__device__ __forceinline__ void ws_issue_row(const uint8_t* base, int64_t total_bytes, int64_t s0, int64_t n,
+                                             uint8_t* dst, uint64_t* bar, int32_t* lead) {
+    const int64_t e0 = s0 + n;
+    const int64_t as = s0 & ~int64_t(15);
+    int64_t ae = (e0 + 15) & ~int64_t(15);
+    if (ae > total_bytes) {
+        const int64_t ab = e0 & ~int64_t(15);
+        for (int64_t q = ab > as ? ab : as; q < e0; ++q) dst[q - as] = base[q];
+        ae = ab > as ? ab : as;
+    }
+    *lead = int32_t(s0 - as);
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(bar, uint32_t(ae - as));
+    if (ae > as) bulk_load(dst, base + as, uint32_t(ae - as), bar);
+}
+
+// Producer: wait (bounded) for the copies of the last min(issued, S) issues.
+__device__ __forceinline__ void ws_drain(WsRing* r, int S, int64_t issued) {
+    const int64_t first = issued > S ? issued - S : 0;
+    for (int64_t i = first; i < issued; ++i) mbar_wait(&r->full[int(i % S)], uint32_t((i / S) & 1));
+}
+
+// Box sums of fh premultiplied pixels (Premultiply<U8> applied to each source
+// pixel before the sum, as the separate Premultiply op would): 4 bands, any
+// byte alignment.  Bands 0 and 2 go through one multiply in 16-bit lanes:
+// c * a + 128 <= 65153 and t + (t >> 8) <= 65407 never carry into the next lane.
+__device__ __forceinline__ void box_sums_premul4_u8(const uint8_t* p, int fh, uint32_t (&sums)[4]) {
+    const int o = int(reinterpret_cast<uintptr_t>(p) & 3);
+    const uint32_t* wp = reinterpret_cast<const uint32_t*>(p - o);
+    const uint32_t sh = 8u * uint32_t(o);
+    uint32_t lo = wp[0];
+    uint32_t s0 = 0, s2 = 0, s1 = 0, s3 = 0, s02 = 0;
+    for (int j = 0; j < fh; ++j) {
+        const uint32_t hi = wp[j + 1];
+        const uint32_t w = __funnelshift_r(lo, hi, sh);
+        lo = hi;
+        const uint32_t al = w >> 24;
+        const uint32_t t02 = (w & 0x00FF00FFu) * al + 0x00800080u;
+        s02 += ((t02 + ((t02 >> 8) & 0x00FF00FFu)) >> 8) & 0x00FF00FFu;
+        const uint32_t t1 = ((w >> 8) & 0xFFu) * al + 128u;
+        s1 += (t1 + (t1 >> 8)) >> 8;
+        s3 += al;
+        if ((j & 255) == 255) {  // each 16-bit lane holds at most 256 x 255
+            s0 += s02 & 0xFFFFu;
+            s2 += s02 >> 16;
+            s02 = 0;
+        }
+    }
+    sums[0] = s0 + (s02 & 0xFFFFu);
+    sums[1] = s1;
+    sums[2] = s2 + (s02 >> 16);
+    sums[3] = s3;
+}
+
+// Box sums with columns clamped to the plane (boxes of the reduce halo), and
+// for 2/4 bands optionally premultiplied.
 template <int B>
-__global__ void __launch_bounds__(kShrinkThreads, 6) shrink_hv_u8_tma(ShrinkArgs a) {
-    extern __shared__ __align__(128) uint8_t smem_tma[];
-    uint8_t* smem = smem_tma;
-    const int S = a.stages;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
-    volatile int32_t* flag = reinterpret_cast<volatile int32_t*>(smem + 64);
-    uint8_t* bufs = smem + 128;
-    const int32_t fh = int32_t(a.fh), fv = int32_t(a.fv);
-    const int32_t chunks = a.chunks;
-    const int32_t G = gridDim.x;
-    const int32_t n_items = a.out.h * chunks;
-    if ((int32_t)blockIdx.x >= n_items) return;
-    const int32_t n_my = (n_items - 1 - (int32_t)blockIdx.x) / G + 1;
-    const int64_t total = (int64_t)n_my * fv;
-    if (threadIdx.x == 0) {
-        for (int i = 0; i < S; ++i) mbar_init(&bars[i], 1);
-        *flag = 0;
-        mbar_fence_init();
-    }
-    __syncthreads();
-
-    // source rows of item `item`, row k: plane row and the staged span's bytes
-    auto row_of = [&](int32_t oy, int32_t k) {
-        int64_t ly = (a.out.y0 + oy) * (int64_t)fv + k - a.in.y0;
-        return ly < 0 ? int64_t(0) : (ly >= a.in.h ? int64_t(a.in.h - 1) : ly);
-    };
-
-    // producer state (thread 0)
-    int32_t p_item = blockIdx.x, p_k = 0;
-    int32_t p_oy = p_item / chunks;
-    ShrinkChunk pc = shrink_chunk(a, p_item - p_oy * chunks);
-    int64_t issued = 0;
-    int p_st = 0;  // ring slot of the next copy (issued mod S, kept incrementally)
-    auto issue = [&]() {
-        const int64_t s0 = row_of(p_oy, p_k) * a.in.pitch + pc.s_lo * B;
-        const int64_t e0 = s0 + (pc.s_hi - pc.s_lo) * B;
-        const int64_t as = s0 & ~int64_t(15);
-        int64_t ae = (e0 + 15) & ~int64_t(15);
-        uint8_t* dst = bufs + (size_t)p_st * a.stage_bytes;
-        if (ae > a.in.total_bytes) {
-            // the 16-byte cover would pass the end of the buffer: copy the aligned
-            // part in bulk and the last few bytes with plain loads
-            const int64_t ab = e0 & ~int64_t(15);
-            for (int64_t q = ab > as ? ab : as; q < e0; ++q) dst[q - as] = a.in.data[q];
-            ae = ab > as ? ab : as;
-        }
-        uint64_t* bar = &bars[p_st];
-        mbar_arrive_expect_tx(bar, uint32_t(ae - as));
-        if (ae > as) bulk_load(dst, a.in.data + as, uint32_t(ae - as), bar);
-        ++issued;
-        if (++p_st == S) p_st = 0;
-        if (++p_k == fv) {
-            p_k = 0;
-            p_item += G;
-            if (p_item < n_items) {
-                p_oy = p_item / chunks;
-                pc = shrink_chunk(a, p_item - p_oy * chunks);
-            }
-        }
-    };
-    if (threadIdx.x == 0) {
-        const int64_t first = total < S ? total : (int64_t)S;
-        for (int64_t t = 0; t < first; ++t) issue();
-    }
-
-    int32_t c_item = blockIdx.x, c_k = 0;
-    int32_t c_oy = c_item / chunks;
-    ShrinkChunk cc = shrink_chunk(a, c_item - c_oy * chunks);
-    const int32_t x = threadIdx.x;  // this thread's output pixel within the chunk (nxf <= blockDim)
-    // this pixel's first source column, and whether its whole box is inside the plane
-    int64_t fcol = (a.out.x0 + cc.lx0 + x) * (int64_t)fh - a.in.x0;
-    bool inside = fcol >= 0 && fcol + fh <= a.in.w;
-    uint32_t vacc[B];
+__device__ __forceinline__ void box_sums_clamped_pm_u8(const uint8_t* span, int64_t first_col, int fh, int64_t c_lo,
+                                                       int64_t w, bool premul, uint32_t (&sums)[B]) {
 #pragma unroll
-    for (int b = 0; b < B; ++b) vacc[b] = 0;
+    for (int b = 0; b < B; ++b) sums[b] = 0;
+    for (int j = 0; j < fh; ++j) {
+        int64_t c = first_col + j;
+        c = c < 0 ? 0 : (c >= w ? w - 1 : c);
+        const uint8_t* px = span + (c - c_lo) * B;
+        const uint32_t al = px[B - 1];
+#pragma unroll
+        for (int b = 0; b < B; ++b)
+            sums[b] += (premul && b != B - 1) ? premultiply_u8(px[b], al) : (uint32_t)px[b];
+    }
+}
+
+// Premultiplied box sums of fh pixels, 2 bands (grey, alpha).
+__device__ __forceinline__ void box_sums_premul2_u8(const uint8_t* p, int fh, uint32_t (&sums)[2]) {
+    uint32_t s0 = 0, s1 = 0;
+    for (int j = 0; j < fh; ++j) {
+        const uint32_t al = p[2 * j + 1];
+        s0 += premultiply_u8(p[2 * j], al);
+        s1 += al;
+    }
+    sums[0] = s0;
+    sums[1] = s1;
+}
+
+// Box sums of one output pixel from the staged span (inside or clamped box,
+// premultiplied or not).
+template <int B>
+__device__ __forceinline__ void ws_box(const ShrinkArgs& a, const uint8_t* span, int64_t s_lo, int64_t fcol,
+                                       bool inside, bool premul, uint32_t (&sums)[B]) {
+    const int fh = int(a.fh);
+    const uint8_t* box = span + (fcol - s_lo) * B;
+    if (!inside) {
+        box_sums_clamped_pm_u8<B>(span, fcol, fh, s_lo, a.in.w, premul, sums);
+    } else if (premul) {
+        if constexpr (B == 4) box_sums_premul4_u8(box, fh, sums);
+        else if constexpr (B == 2) box_sums_premul2_u8(box, fh, sums);
+        else box_sums_u8<B>(box, fh, sums);
+    } else {
+        box_sums_u8<B>(box, fh, sums);
+    }
+}
+
+// Consumers: output rows [oy0, oy1) of column chunk `c`, whose (oy1 - oy0) * fv
+// source row segments arrive in ring order starting at (slot, ph).  Thread x
+// owns output pixels c.lx0 + x + kCThreads * j, j < P (P pixels per thread
+// share the per-row wait, release and addressing).  Returns false once `stop`
+// is raised.
+template <int B, int P>
+__device__ bool ws_consume(const ShrinkArgs& a, int32_t oy0, int32_t oy1, const ShrinkChunk& c, WsRing* ring,
+                           const uint8_t* bufs, uint32_t stage_bytes, int S, int& slot, uint32_t& ph,
+                           volatile int32_t* stop) {
+    const int32_t fh = int32_t(a.fh), fv = int32_t(a.fv);
+    const int x = threadIdx.x, lane = x & 31;
+    bool mine[P], inside[P];
+    int64_t fcol[P];
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+        const int px = x + kCThreads * j;
+        mine[j] = px < c.ncols;
+        fcol[j] = (a.out.x0 + c.lx0 + px) * (int64_t)fh - a.in.x0;
+        inside[j] = fcol[j] >= 0 && fcol[j] + fh <= a.in.w;
+    }
+    const bool any = mine[0];
+    const bool premul = a.premul_in != 0;
     const uint32_t hhalf = uint32_t(fh) / 2;
     const bool hmult = a.hmode == 3;
-    int64_t t_fail = -1;
-    int st = 0;           // ring slot of row t (t mod S)
-    uint32_t parity = 0;  // mbarrier phase parity of that slot ((t / S) & 1)
-    for (int64_t t = 0; t < total; ++t) {
-        if (threadIdx.x == 0 && !mbar_wait(&bars[st], parity)) *flag = 1;
-        __syncthreads();
-        if (*flag) { t_fail = t; break; }
-        const int32_t lead = int32_t((row_of(c_oy, c_k) * a.in.pitch + cc.s_lo * B) & 15);
-        uint8_t* span = bufs + (size_t)st * a.stage_bytes + lead;
-        if (a.premul_in) {
-            premultiply_pixels<B>(span, int32_t(cc.s_hi - cc.s_lo));
-            __syncthreads();
-        }
-        if (x < cc.ncols) {
-            uint32_t sums[B];
-            if (inside) box_sums_u8<B>(span + (fcol - cc.s_lo) * B, fh, sums);
-            else box_sums_clamped_u8<B>(span, fcol, fh, cc.s_lo, a.in.w, sums);
-            if (hmult) {
+    for (int32_t oy = oy0; oy < oy1; ++oy) {
+        uint32_t vacc[P][B];
 #pragma unroll
-                for (int b = 0; b < B; ++b) vacc[b] += round_mult_u8(sums[b], hhalf, a.hmult);
-            } else {
+        for (int j = 0; j < P; ++j)
 #pragma unroll
-                for (int b = 0; b < B; ++b) vacc[b] += round_mode_u8(sums[b], a.hmode, uint32_t(fh), a.hmult);
+            for (int b = 0; b < B; ++b) vacc[j][b] = 0;
+        for (int32_t k = 0; k < fv; ++k) {
+            bool live = *stop == 0;
+            if (live && !mbar_wait(&ring->full[slot], ph)) {
+                *stop = 1;
+                live = false;
             }
+            if (live && any) {
+                const uint8_t* span = bufs + (size_t)slot * stage_bytes + ring->lead[slot];
+#pragma unroll
+                for (int j = 0; j < P; ++j) {
+                    if (!mine[j]) continue;
+                    uint32_t sums[B];
+                    ws_box<B>(a, span, c.s_lo, fcol[j], inside[j], premul, sums);
+                    if (hmult) {
+#pragma unroll
+                        for (int b = 0; b < B; ++b) vacc[j][b] += round_mult_u8(sums[b], hhalf, a.hmult);
+                    } else {
+#pragma unroll
+                        for (int b = 0; b < B; ++b) vacc[j][b] += round_mode_u8(sums[b], a.hmode, uint32_t(fh), a.hmult);
+                    }
+                }
+            }
+            __syncwarp();
+            if (live && lane == 0) mbar_arrive(&ring->empty[slot]);
+            if (++slot == S) { slot = 0; ph ^= 1u; }
         }
-        __syncthreads();  // all reads of this buffer are done
-        if (threadIdx.x == 0 && issued < total) {
-            fence_proxy_async_smem();
-            issue();
-        }
-        if (++st == S) { st = 0; parity ^= 1u; }
-        if (++c_k == fv) {
-            if (x < cc.ncols) {
+        if (*stop == 0) {
+#pragma unroll
+            for (int j = 0; j < P; ++j) {
+                if (!mine[j]) continue;
                 uint8_t o[B];
 #pragma unroll
-                for (int b = 0; b < B; ++b) o[b] = (uint8_t)round_mode_u8(vacc[b], a.vmode, uint32_t(fv), a.vmult);
+                for (int b = 0; b < B; ++b) o[b] = (uint8_t)round_mode_u8(vacc[j][b], a.vmode, uint32_t(fv), a.vmult);
                 if (a.unpremul_out) {
 #pragma unroll
                     for (int b = 0; b < B - 1; ++b) o[b] = (uint8_t)unpremultiply_u8(o[b], o[B - 1]);
                 }
-                uint8_t* dst = a.out.data + (int64_t)c_oy * a.out.pitch + (int64_t)(cc.lx0 + x) * B;
+                uint8_t* dst = a.out.data + (int64_t)oy * a.out.pitch + (int64_t)(c.lx0 + x + kCThreads * j) * B;
 #pragma unroll
                 for (int b = 0; b < B; ++b) dst[b] = o[b];
             }
-#pragma unroll
-            for (int b = 0; b < B; ++b) vacc[b] = 0;
-            c_k = 0;
-            c_item += G;
-            if (c_item < n_items) {
-                c_oy = c_item / chunks;
-                cc = shrink_chunk(a, c_item - c_oy * chunks);
-                fcol = (a.out.x0 + cc.lx0 + x) * (int64_t)fh - a.in.x0;
-                inside = fcol >= 0 && fcol + fh <= a.in.w;
-            }
         }
     }
-    if (t_fail >= 0) {
-        // a copy never completed: record it, then wait (bounded) for the copies
-        // this block still has in flight before its shared memory goes away
-        if (threadIdx.x == 0) {
-            if (a.err) atomicExch(a.err, VIPRS_ERR_TIMEOUT);
-            for (int64_t tt = t_fail + 1; tt < issued; ++tt) {
-                if (++st == S) { st = 0; parity ^= 1u; }
-                mbar_wait(&bars[st], parity);
-            }
+    return *stop == 0;
+}
+
+// Producer: issue the source rows of output rows [oy0, oy1) of chunk `c`.
+// Returns false if a slot never came free.
+template <int B>
+__device__ bool ws_produce(const ShrinkArgs& a, const uint8_t* in_data, int32_t oy0, int32_t oy1,
+                           const ShrinkChunk& c, WsRing* ring, uint8_t* bufs, uint32_t stage_bytes, int S,
+                           int& slot, uint32_t& ph, int64_t& issued) {
+    const int32_t fv = int32_t(a.fv);
+    const int64_t n = (c.s_hi - c.s_lo) * B;
+    for (int32_t oy = oy0; oy < oy1; ++oy) {
+        for (int32_t k = 0; k < fv; ++k) {
+            if (!mbar_wait(&ring->empty[slot], ph ^ 1u)) return false;
+            int64_t ly = (a.out.y0 + oy) * (int64_t)fv + k - a.in.y0;
+            ly = ly < 0 ? 0 : (ly >= a.in.h ? a.in.h - 1 : ly);
+            ws_issue_row(in_data, a.in.total_bytes, ly * a.in.pitch + c.s_lo * B, n, bufs + (size_t)slot * stage_bytes,
+                         &ring->full[slot], &ring->lead[slot]);
+            ++issued;
+            if (++slot == S) { slot = 0; ph ^= 1u; }
         }
-        __syncthreads();
+    }
+    return true;
+}
+
+// Standalone ShrinkH+ShrinkV (u8, B bands, source 16-byte aligned).  Items are
+// (output row, column chunk); the chunks partition the output columns and
+// block b owns items b, b + G, ...  The host picks the chunk count, ring depth
+// and blocks per SM (makespan model over the resident grid).
+template <int B, int P>
+__global__ void __launch_bounds__(kWsThreads) shrink_hv_u8_ws(ShrinkArgs a) {
+    extern __shared__ __align__(128) uint8_t smem_ws[];
+    WsRing* ring = reinterpret_cast<WsRing*>(smem_ws);
+    volatile int32_t* stop = reinterpret_cast<volatile int32_t*>(smem_ws + sizeof(WsRing));
+    uint8_t* bufs = smem_ws + (sizeof(WsRing) + 4 + 127) / 128 * 128;
+    const int S = a.stages;
+    const int32_t chunks = a.chunks, G = gridDim.x;
+    const int32_t n_items = a.out.h * chunks;
+    if (threadIdx.x == 0) {
+        ws_ring_init(ring, S);
+        *stop = 0;
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x >= kCThreads) {
+        if (threadIdx.x == kCThreads) {
+            int slot = 0;
+            uint32_t ph = 0;
+            int64_t issued = 0;
+            for (int32_t item = blockIdx.x; item < n_items && *stop == 0; item += G) {
+                const int32_t oy = item / chunks;
+                const ShrinkChunk c = shrink_chunk(a, item - oy * chunks);
+                if (!ws_produce<B>(a, a.in.data, oy, oy + 1, c, ring, bufs, a.stage_bytes, S, slot, ph, issued)) {
+                    *stop = 1;
+                    if (a.err) atomicExch(a.err, VIPRS_ERR_TIMEOUT);
+                    break;
+                }
+            }
+            ws_drain(ring, S, issued);
+        }
+        return;
+    }
+    int slot = 0;
+    uint32_t ph = 0;
+    for (int32_t item = blockIdx.x; item < n_items; item += G) {
+        const int32_t oy = item / chunks;
+        const ShrinkChunk c = shrink_chunk(a, item - oy * chunks);
+        if (!ws_consume<B, P>(a, oy, oy + 1, c, ring, bufs, a.stage_bytes, S, slot, ph, stop)) {
+            if (threadIdx.x == 0 && a.err) atomicExch(a.err, VIPRS_ERR_TIMEOUT);
+            break;
+        }
     }
 }
 
@@ -573,7 +706,7 @@ __device__ __forceinline__ void store_or_unpremul(uint8_t* orow, int64_t item, i
     }
     const int local = threadIdx.x;
     if (item < nitems) stage[local] = (uint8_t)v;
-    __syncthreads();
+    csync();
     if (item < nitems) {
         const int b = int(item % bands);
         uint32_t o = stage[local];
@@ -582,7 +715,7 @@ __device__ __forceinline__ void store_or_unpremul(uint8_t* orow, int64_t item, i
     }
 }
 
-// One chunk of blockDim.x output samples (`chunk`) of output row `oy`.
+// One chunk of kCThreads output samples (`chunk`) of output row `oy`.
 template <typename T, int MODE>
 __device__ void reduce_h_chunk(const ReduceArgs& a, int64_t chunk, int64_t oy, uint8_t* smem) {
     const int taps = a.taps, bands = a.bands;
@@ -590,14 +723,14 @@ __device__ void reduce_h_chunk(const ReduceArgs& a, int64_t chunk, int64_t oy, u
     const bool coef_in_smem = coef_bytes <= 48 * 1024;
     const uint8_t* coef = reinterpret_cast<const uint8_t*>(a.coeffs);
     if (coef_in_smem) {
-        for (int i = threadIdx.x * 4; i < coef_bytes; i += blockDim.x * 4)
+        for (int i = threadIdx.x * 4; i < coef_bytes; i += kCThreads * 4)
             *reinterpret_cast<uint32_t*>(smem + i) = *reinterpret_cast<const uint32_t*>(coef + i);
-        __syncthreads();
+        csync();
         coef = smem;
     }
     uint8_t* stage = smem + ((coef_in_smem ? coef_bytes : 0) + 15) / 16 * 16;
     const int nitems = a.out.w * bands;
-    const int64_t item = chunk * blockDim.x + threadIdx.x;
+    const int64_t item = chunk * kCThreads + threadIdx.x;
     const int64_t ly = a.out.y0 + oy - a.in.y0;
     T outv = T(0);
     if (item < nitems) {
@@ -647,14 +780,14 @@ __device__ void reduce_v_chunk(const ReduceArgs& a, int64_t chunk, int64_t oy, u
     const bool coef_in_smem = coef_bytes <= 48 * 1024;
     const uint8_t* coef = reinterpret_cast<const uint8_t*>(a.coeffs);
     if (coef_in_smem) {
-        for (int i = threadIdx.x * 4; i < coef_bytes; i += blockDim.x * 4)
+        for (int i = threadIdx.x * 4; i < coef_bytes; i += kCThreads * 4)
             *reinterpret_cast<uint32_t*>(smem + i) = *reinterpret_cast<const uint32_t*>(coef + i);
-        __syncthreads();
+        csync();
         coef = smem;
     }
     uint8_t* stage = smem + ((coef_in_smem ? coef_bytes : 0) + 15) / 16 * 16;
     const int nitems = a.out.w * bands;
-    const int64_t item = chunk * blockDim.x + threadIdx.x;
+    const int64_t item = chunk * kCThreads + threadIdx.x;
     const int64_t base = (int64_t)a.starts[oy] - a.in.y0;
     const int ph = a.phases[oy];
     T outv = T(0);
@@ -783,7 +916,7 @@ __device__ __forceinline__ T fused_taps_rows(const uint8_t* base, const int32_t*
 __device__ __forceinline__ void copy_table16(uint8_t* dst, const void* src, int bytes) {
     const uint4* s = reinterpret_cast<const uint4*>(src);
     uint4* d = reinterpret_cast<uint4*>(dst);
-    for (int i = threadIdx.x; i < bytes / 16; i += blockDim.x) d[i] = s[i];
+    for (int i = threadIdx.x; i < bytes / 16; i += kCThreads) d[i] = s[i];
 }
 
 // Stage rows [0, nrows) of a source tile: row r is plane row row_of(r), columns
@@ -793,7 +926,7 @@ __device__ __forceinline__ void copy_table16(uint8_t* dst, const void* src, int 
 template <typename T, typename RowOf>
 __device__ __forceinline__ void stage_tile_rows(const Plane& in, RowOf row_of, int nrows, int64_t c0, int ncols,
                                                 int bands, uint8_t* dst_base, int pitch, int32_t* rowbase) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = kCThreads >> 5;
     const int nbytes = ncols * bands * int(sizeof(T));
     for (int r = warp; r < nrows; r += nw) {
         const uint8_t* src = in.data + row_of(r) * in.pitch + c0 * bands * int64_t(sizeof(T));
@@ -816,7 +949,7 @@ __device__ __forceinline__ void stage_tile_rows(const Plane& in, RowOf row_of, i
 // Premultiply<U8> of the staged source tile (R rows of C pixels, alpha last).
 __device__ __forceinline__ void premultiply_staged(uint8_t* ins, const int32_t* rowbase, int R, int C, int B) {
     int r = threadIdx.x / C, c = threadIdx.x - r * C;
-    const int dr = blockDim.x / C, dc = blockDim.x - dr * C;
+    const int dr = kCThreads / C, dc = kCThreads - dr * C;
     for (; r < R;) {
         uint8_t* px = ins + rowbase[r] + c * B;
         const uint32_t al = px[B - 1];
@@ -845,8 +978,8 @@ __device__ void reduce2d_tile(const Reduce2DArgs& a, int bx, int by, uint8_t* sm
 
     copy_table16(sm + L.coef_h, a.coeffs_h, r2_align16(L.coef_h_bytes));
     copy_table16(sm + L.coef_v, a.coeffs_v, r2_align16(L.coef_v_bytes));
-    for (int i = threadIdx.x; i < ncols; i += blockDim.x) { sx[i] = a.starts_h[tx0 + i]; phx[i] = a.phases_h[tx0 + i]; }
-    for (int i = threadIdx.x; i < nrows; i += blockDim.x) { sy[i] = a.starts_v[ty0 + i]; phy[i] = a.phases_v[ty0 + i]; }
+    for (int i = threadIdx.x; i < ncols; i += kCThreads) { sx[i] = a.starts_h[tx0 + i]; phx[i] = a.phases_h[tx0 + i]; }
+    for (int i = threadIdx.x; i < nrows; i += kCThreads) { sy[i] = a.starts_v[ty0 + i]; phy[i] = a.phases_v[ty0 + i]; }
     // tap spans of the tile (absolute coordinates of each op's input)
     const int64_t hs0 = a.starts_h[tx0], hs1 = (int64_t)a.starts_h[tx0 + ncols - 1] + a.taps_h - 1;
     const int64_t vs0 = a.starts_v[ty0], vs1 = (int64_t)a.starts_v[ty0 + nrows - 1] + a.taps_v - 1;
@@ -863,16 +996,16 @@ __device__ void reduce2d_tile(const Reduce2DArgs& a, int bx, int by, uint8_t* sm
         const int C = int(c1 - c0 + 1);
         stage_tile_rows<T>(a.in, [&](int r) { return clampi64(rlo + r - a.in.y0, 0, phh); }, R, c0, C, B, ins, L.pitch,
                            rowbase);
-        __syncthreads();
+        csync();
         if (premul) {
             premultiply_staged(ins, rowbase, R, C, B);
-            __syncthreads();
+            csync();
         }
         // H: mid[r][x*B + b]
         const int W1 = ncols * B;
         {
             int r = threadIdx.x / W1, j = threadIdx.x - r * W1;
-            const int dr = blockDim.x / W1, dj = blockDim.x - dr * W1;
+            const int dr = kCThreads / W1, dj = kCThreads - dr * W1;
             for (; r < R;) {
                 const int x = j / B, b = j - x * B;
                 const T* row = reinterpret_cast<const T*>(ins + rowbase[r]) + b;
@@ -882,11 +1015,11 @@ __device__ void reduce2d_tile(const Reduce2DArgs& a, int bx, int by, uint8_t* sm
                 if (j >= W1) { j -= W1; ++r; }
             }
         }
-        __syncthreads();
+        csync();
         // V: out[y][x*B + b]
         {
             int y = threadIdx.x / W1, j = threadIdx.x - y * W1;
-            const int dy = blockDim.x / W1, dj = blockDim.x - dy * W1;
+            const int dy = kCThreads / W1, dj = kCThreads - dy * W1;
             for (; y < nrows;) {
                 const int s = int(sy[y] - rlo);
                 const bool lane = (int64_t)tx0 * B + j < a.vector_len;
@@ -906,16 +1039,16 @@ __device__ void reduce2d_tile(const Reduce2DArgs& a, int bx, int by, uint8_t* sm
         const int64_t r0 = clampi64(vs0 - a.in.y0, 0, phh), r1 = clampi64(vs1 - a.in.y0, 0, phh);
         const int R = int(r1 - r0 + 1);
         stage_tile_rows<T>(a.in, [&](int r) { return r0 + r; }, R, c0, C, B, ins, L.pitch, rowbase);
-        __syncthreads();
+        csync();
         if (premul) {
             premultiply_staged(ins, rowbase, R, C, B);
-            __syncthreads();
+            csync();
         }
         // V: mid[y][c*B + b]
         const int W1 = Cm * B;
         {
             int y = threadIdx.x / W1, j = threadIdx.x - y * W1;
-            const int dy = blockDim.x / W1, dj = blockDim.x - dy * W1;
+            const int dy = kCThreads / W1, dj = kCThreads - dy * W1;
             for (; y < nrows;) {
                 const int c = j / B, b = j - c * B;
                 const int64_t mcol = clo + c;
@@ -928,12 +1061,12 @@ __device__ void reduce2d_tile(const Reduce2DArgs& a, int bx, int by, uint8_t* sm
                 if (j >= W1) { j -= W1; ++y; }
             }
         }
-        __syncthreads();
+        csync();
         // H: out[y][x*B + b]
         const int W2 = ncols * B;
         {
             int y = threadIdx.x / W2, j = threadIdx.x - y * W2;
-            const int dy = blockDim.x / W2, dj = blockDim.x - dy * W2;
+            const int dy = kCThreads / W2, dj = kCThreads - dy * W2;
             for (; y < nrows;) {
                 const int x = j / B, b = j - x * B;
                 const int s = int(sx[x] - clo);
@@ -943,12 +1076,12 @@ __device__ void reduce2d_tile(const Reduce2DArgs& a, int bx, int by, uint8_t* sm
             }
         }
     }
-    __syncthreads();
+    csync();
     // store the output tile (unpremultiplied when the chain ends with it)
     const int Wo = ncols * B;
     const bool unpremul = a.unpremul_out != 0;
     int y = threadIdx.x / Wo, j = threadIdx.x - y * Wo;
-    const int dy = blockDim.x / Wo, dj = blockDim.x - dy * Wo;
+    const int dy = kCThreads / Wo, dj = kCThreads - dy * Wo;
     for (; y < nrows;) {
         const int i = y * Wo + j;
         T v = ost[i];
