@@ -40,7 +40,7 @@ struct viprs_batch {
     int32_t ring_slots_knob = 0;  // ring slots per block (0: ring_total / slot size)
     int32_t blocks_per_sm = 0;    // cap of the shrink launches (0 = occupancy maximum)
     uint32_t reduce_smem_budget = 40 * 1024;  // shared memory of one fused-reduce tile
-    int64_t item_bytes = 96 * 1024;           // source bytes per shrink work item
+    int64_t item_bytes = 256 * 1024;          // source bytes per shrink work item
     uint32_t ring_total = 56 * 1024;          // shrink ring bytes per block (auto slots)
     // device work list
     std::vector<BatchStage> stages;
@@ -110,15 +110,18 @@ int plan_stages(viprs_batch* b, int image, std::vector<std::vector<BatchStage>>*
             // column chunks partition the output columns (clamped boxes at the
             // edges, as in the standalone kernel); one consumer thread per column
             const int64_t per_col = int64_t(bs.sh.fh) * p->bands;
-            bs.chunk_cols = int32_t(std::max<int64_t>(1, std::min<int64_t>(512, b->ring_target / std::max<int64_t>(per_col, 1))));
+            // at most one column per consumer thread and `ring_target` source
+            // bytes per row segment; balanced chunk widths
+            const int64_t cap = std::max<int64_t>(1, std::min<int64_t>(256, b->ring_target / std::max<int64_t>(per_col, 1)));
+            const int64_t nch = (outp.w + cap - 1) / cap;
+            bs.chunk_cols = int32_t(std::max<int64_t>(1, (outp.w + nch - 1) / nch));
             bs.sh.nxf = bs.chunk_cols;
             bs.n_chunks = (outp.w + bs.chunk_cols - 1) / bs.chunk_cols;
             // output rows per item: about `item_bytes` of source per item
             const int64_t row_src = int64_t(bs.chunk_cols) * per_col * bs.sh.fv;
             bs.rows_per_item = int32_t(std::max<int64_t>(1, std::min<int64_t>(outp.h, b->item_bytes / std::max<int64_t>(row_src, 1))));
             bs.n_items = ((outp.h + bs.rows_per_item - 1) / bs.rows_per_item) * bs.n_chunks;
-            const uint32_t need = uint32_t((bs.chunk_cols * per_col + 32 + 15 + 127) / 128 * 128);
-            b->ring_stage_bytes = std::max(b->ring_stage_bytes, need);
+            b->ring_stage_bytes = std::max(b->ring_stage_bytes, ws_slot_bytes(int64_t(bs.chunk_cols) * per_col));
             // the plain-load routine (unaligned sources) stages fv x fh source
             // pixels of at least one output column in the work region
             const int64_t edge = int64_t(bs.sh.fv) * per_col + p->bands + 64;
@@ -292,8 +295,7 @@ int build_list(viprs_batch* b) {
 }
 
 int launch_batch(viprs_batch* b, const uint64_t* d_srcs, const uint64_t* d_dsts, cudaStream_t s) {
-    cudaError_t e = cudaMemsetAsync(b->d_counters, 0, b->stages.size() * sizeof(int32_t), s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_ctrl, 0, (1 + b->launches.size()) * sizeof(int32_t), s);
+    cudaError_t e = cudaMemsetAsync(b->d_ctrl, 0, (1 + b->launches.size()) * sizeof(int32_t), s);
     if (e != cudaSuccess) return cuda_status(e);
     for (size_t k = 0; k < b->launches.size(); ++k) {
         const BatchLaunch& l = b->launches[k];

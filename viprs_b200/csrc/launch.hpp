@@ -43,8 +43,9 @@ struct ShrinkArgs {
     // rounding constants of ShrinkH / ShrinkV for u8 (host-computed)
     int32_t hmode = 0, vmode = 0;       // 0 copy, 1 factor 2, 2 exact /5, 3 multiplier
     uint64_t hmult = 0, vmult = 0;
-    // bulk-copy pipeline of the interior columns (u8, ShrinkH then ShrinkV)
-    int32_t chunks = 0, nxf = 0, stages = 0;
+    // bulk-copy pipeline (u8, ShrinkH then ShrinkV): column chunks of nxf
+    // outputs, output rows per item, ring slots of stage_bytes
+    int32_t chunks = 0, nxf = 0, stages = 0, rows_per_item = 1;
     uint32_t stage_bytes = 0;
     int32_t* err = nullptr;    // device error word (timeout), may be null
 };
@@ -104,6 +105,12 @@ struct Reduce2DArgs {
 #else
 #define VIPRS_HD
 #endif
+
+// Shrink ring slot (u8 box shrink) for a source row segment of n bytes: the
+// segment sits at its plane offset mod 16 within the slot (the 16-byte aligned
+// cover is copied), with 32 bytes of slack after it for the box sums'
+// over-read.
+VIPRS_HD inline uint32_t ws_slot_bytes(int64_t n) { return uint32_t((n + 15 + 32 + 127) / 128 * 128); }
 
 // Shared-memory layout of one fused-reduce tile (byte offsets, 16-aligned):
 // both coefficient tables, the tile's start/phase tables, one offset per

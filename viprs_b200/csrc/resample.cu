@@ -115,54 +115,35 @@ cudaError_t shrink2d(ShrinkArgs a, cudaStream_t s) {
     round_consts(a.fv, a.bands, false, &a.vmode, &a.vmult);
     if (a.fmt == kU8 && a.hv_order && (reinterpret_cast<uintptr_t>(a.in.data) & 15) == 0 && a.bands <= 4 &&
         int64_t(a.fh) * a.bands <= 16384) {
-        // chunk count and ring depth: model the makespan as waves x per-item bytes
-        // and prefer the configuration whose items fill the resident grid evenly
+        // One consumer thread per output column of a chunk: the fewest chunks
+        // (widest row segments, least per-row overhead), three ring slots of
+        // one row segment, and as many blocks per SM as fit -- the consumers
+        // are latency-bound, so resident warps set the rate.
         const int64_t per_col = int64_t(a.fh) * a.bands;
-        int best_chunks = 0, best_stages = 0, best_bps = 0;
-        uint32_t best_stage_bytes = 0;
-        double best_cost = 1e300;
-        // two output pixels per consumer thread (chunks up to 512 columns)
-        constexpr int P = 2;
-        const int64_t c_min = std::max<int64_t>(1, (a.out.w + P * dev::kCThreads - 1) / (P * dev::kCThreads));
-        void (*kern)(ShrinkArgs) = a.bands == 1 ? dev::shrink_hv_u8_ws<1, P>
-                                  : a.bands == 2 ? dev::shrink_hv_u8_ws<2, P>
-                                  : a.bands == 3 ? dev::shrink_hv_u8_ws<3, P> : dev::shrink_hv_u8_ws<4, P>;
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        const int64_t chunks = std::max<int64_t>(1, (a.out.w + dev::kCThreads - 1) / dev::kCThreads);
+        const int64_t nxf = (a.out.w + chunks - 1) / chunks;
+        const int stages = 3;
+        const uint32_t stage_bytes = ws_slot_bytes(nxf * per_col);
+        void (*kern)(ShrinkArgs) = a.bands == 1 ? dev::shrink_hv_u8_ws<1, 1>
+                                  : a.bands == 2 ? dev::shrink_hv_u8_ws<2, 1>
+                                  : a.bands == 3 ? dev::shrink_hv_u8_ws<3, 1> : dev::shrink_hv_u8_ws<4, 1>;
         const size_t ctl = (sizeof(dev::WsRing) + 4 + 127) / 128 * 128;
-        for (int stages : {3, 4, 6, 8}) {
-            for (int64_t c = c_min; c <= c_min + 7; ++c) {
-                const int64_t nxf = (a.out.w + c - 1) / c;
-                const uint32_t stage_bytes = uint32_t((nxf * per_col + 32 + 15 + 127) / 128 * 128);
-                const size_t smem = ctl + size_t(stages) * stage_bytes;
-                if (smem > 200 * 1024) continue;
-                int bps = 0;
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, dev::kWsThreads, smem);
-                bps = std::max(1, bps);
-                const int64_t grid = int64_t(bps) * sm_count();
-                const int64_t items = int64_t(a.out.h) * c;
-                const int64_t waves = (items + grid - 1) / grid;
-                // makespan ~ waves x bytes per item; among equals prefer deeper rings
-                // (more bytes in flight per SM) and fewer items
-                const double inflight = double(bps) * double(stages) * double(stage_bytes);
-                const double cost = double(waves) * double(nxf * per_col) * double(std::min(items, grid)) *
-                                        (1.0 + 32768.0 / inflight) +
-                                    1e-3 * double(items);
-                if (cost < best_cost) {
-                    best_cost = cost; best_chunks = int(c); best_stages = stages; best_bps = bps;
-                    best_stage_bytes = stage_bytes;
-                }
-            }
-        }
-        if (best_chunks > 0 && int64_t(a.out.h) * best_chunks < (int64_t(1) << 30)) {
+        const size_t smem = ctl + size_t(stages) * stage_bytes;
+        if (smem <= 200 * 1024 && int64_t(a.out.h) * chunks < (int64_t(1) << 30)) {
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            int bps = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, dev::kWsThreads, smem);
+            bps = std::max(1, bps);
             ShrinkArgs f = a;
-            f.chunks = best_chunks;
-            f.nxf = (a.out.w + best_chunks - 1) / best_chunks;
-            f.stages = best_stages;
-            f.stage_bytes = best_stage_bytes;
-            const size_t smem = ctl + size_t(best_stages) * best_stage_bytes;
-            const int per_sm = std::max(1, best_bps);
-            const int64_t items = int64_t(a.out.h) * best_chunks;
-            const int64_t grid = std::min<int64_t>(items, int64_t(per_sm) * sm_count());
+            f.chunks = int32_t(chunks);
+            f.nxf = int32_t(nxf);
+            f.stages = stages;
+            f.stage_bytes = stage_bytes;
+            const int64_t resident = int64_t(bps) * sm_count();
+            const int64_t rpi = 1;
+            f.rows_per_item = 1;
+            const int64_t items = ((a.out.h + rpi - 1) / rpi) * chunks;
+            const int64_t grid = std::min<int64_t>(items, resident);
             kern<<<(unsigned)grid, dev::kWsThreads, smem, s>>>(f);
             return cudaGetLastError();
         }

@@ -249,18 +249,23 @@ __global__ void __launch_bounds__(kShrinkThreads) shrink2d_kernel(ShrinkArgs a) 
 
 // Box sums of one output pixel's fh source pixels (B bands, u8) from shared
 // memory at any byte alignment: words are realigned with a funnel shift and
-// the bands are summed four bytes at a time with dp4a masks.  The word after
-// the box is read (the stage buffers carry 32 bytes of slack) but masked out.
+// the bands are summed four bytes at a time with dp4a masks.  Words go in
+// groups of G (3 for 3 bands: the band pattern repeats every 12 bytes, else 1);
+// the last group is masked to the box and may read up to 12 bytes past it (the
+// stage buffers carry 32 bytes of slack).  Alternate groups feed two sets of
+// accumulators, so the dp4a chains are half as long.
 template <int B>
 __device__ __forceinline__ void box_sums_u8(const uint8_t* p, int fh, uint32_t (&sums)[B]) {
+    constexpr int G = B == 3 ? 3 : 1;
     const int o = int(reinterpret_cast<uintptr_t>(p) & 3);
     const uint32_t* wp = reinterpret_cast<const uint32_t*>(p - o);
     const int nbytes = fh * B;
-    const int K = (nbytes + 3) >> 2;  // realigned words, the last one partial
+    const int K = (nbytes + 3) >> 2;             // realigned words, the last one partial
+    const int Kp = (K + G - 1) / G * G;          // whole groups
     const uint32_t sh = 8u * uint32_t(o);
-    const uint32_t tail_mask = (nbytes & 3) ? ((1u << (8 * (nbytes & 3))) - 1u) : 0xFFFFFFFFu;
+    uint32_t sa[B], sb[B];
 #pragma unroll
-    for (int b = 0; b < B; ++b) sums[b] = 0;
+    for (int b = 0; b < B; ++b) { sa[b] = 0; sb[b] = 0; }
     uint32_t lo = wp[0];
     auto next = [&](int k) {
         const uint32_t hi = wp[k + 1];
@@ -268,40 +273,46 @@ __device__ __forceinline__ void box_sums_u8(const uint8_t* p, int fh, uint32_t (
         lo = hi;
         return w;
     };
-    // masks: bands of the four bytes of realigned word k (period 3 words for B == 3)
-    auto acc = [&](uint32_t w, int phase) {
+    // word of phase `ph` within a group -> band sums
+    auto acc = [&](uint32_t (&s)[B], uint32_t w, int ph) {
         if (B == 1) {
-            sums[0] = __dp4a(w, 0x01010101u, sums[0]);
+            s[0] = __dp4a(w, 0x01010101u, s[0]);
         } else if (B == 2) {
-            sums[0] = __dp4a(w, 0x00010001u, sums[0]);
-            sums[1 % B] = __dp4a(w, 0x01000100u, sums[1 % B]);
+            s[0] = __dp4a(w, 0x00010001u, s[0]);
+            s[1 % B] = __dp4a(w, 0x01000100u, s[1 % B]);
         } else if (B == 3) {
-            const uint32_t m0 = phase == 0 ? 0x01000001u : (phase == 1 ? 0x00010000u : 0x00000100u);
-            const uint32_t m1 = phase == 0 ? 0x00000100u : (phase == 1 ? 0x01000001u : 0x00010000u);
-            const uint32_t m2 = phase == 0 ? 0x00010000u : (phase == 1 ? 0x00000100u : 0x01000001u);
-            sums[0] = __dp4a(w, m0, sums[0]);
-            sums[1 % B] = __dp4a(w, m1, sums[1 % B]);
-            sums[2 % B] = __dp4a(w, m2, sums[2 % B]);
+            const uint32_t m0 = ph == 0 ? 0x01000001u : (ph == 1 ? 0x00010000u : 0x00000100u);
+            const uint32_t m1 = ph == 0 ? 0x00000100u : (ph == 1 ? 0x01000001u : 0x00010000u);
+            const uint32_t m2 = ph == 0 ? 0x00010000u : (ph == 1 ? 0x00000100u : 0x01000001u);
+            s[0] = __dp4a(w, m0, s[0]);
+            s[1 % B] = __dp4a(w, m1, s[1 % B]);
+            s[2 % B] = __dp4a(w, m2, s[2 % B]);
         } else {
 #pragma unroll
-            for (int b = 0; b < B; ++b) sums[b] = __dp4a(w, 1u << (8 * b), sums[b]);
+            for (int b = 0; b < B; ++b) s[b] = __dp4a(w, 1u << (8 * b), s[b]);
         }
     };
     int k = 0;
-    if (B == 3) {
-        for (; k + 3 < K; k += 3) {
-            acc(next(k), 0);
-            acc(next(k + 1), 1);
-            acc(next(k + 2), 2);
-        }
-    } else {
-        for (; k + 2 < K; k += 2) {
-            acc(next(k), 0);
-            acc(next(k + 1), 0);
-        }
+    const int kfull = Kp - G;  // words before the (masked) last group
+    for (; k + 2 * G <= kfull; k += 2 * G) {
+#pragma unroll
+        for (int j = 0; j < G; ++j) acc(sa, next(k + j), j);
+#pragma unroll
+        for (int j = 0; j < G; ++j) acc(sb, next(k + G + j), j);
     }
-    for (; k < K - 1; ++k) acc(next(k), B == 3 ? k % 3 : 0);
-    acc(next(K - 1) & tail_mask, B == 3 ? (K - 1) % 3 : 0);
+    if (k < kfull) {
+#pragma unroll
+        for (int j = 0; j < G; ++j) acc(sa, next(k + j), j);
+        k += G;
+    }
+#pragma unroll
+    for (int j = 0; j < G; ++j) {
+        const int valid = nbytes - 4 * (k + j);
+        const uint32_t m = valid >= 4 ? 0xFFFFFFFFu : (valid <= 0 ? 0u : ((1u << (8 * valid)) - 1u));
+        acc(sb, next(k + j) & m, j);
+    }
+#pragma unroll
+    for (int b = 0; b < B; ++b) sums[b] = sa[b] + sb[b];
 }
 
 // Premultiply<U8> in place over `npx` staged pixels of B bands (alpha last).
@@ -467,26 +478,43 @@ __device__ __forceinline__ void box_sums_premul4_u8(const uint8_t* p, int fh, ui
     const uint32_t* wp = reinterpret_cast<const uint32_t*>(p - o);
     const uint32_t sh = 8u * uint32_t(o);
     uint32_t lo = wp[0];
-    uint32_t s0 = 0, s2 = 0, s1 = 0, s3 = 0, s02 = 0;
-    for (int j = 0; j < fh; ++j) {
-        const uint32_t hi = wp[j + 1];
-        const uint32_t w = __funnelshift_r(lo, hi, sh);
-        lo = hi;
+    uint32_t s0 = 0, s2 = 0, s1 = 0, s3 = 0;
+    // one premultiplied pixel into the packed (bands 0, 2) sum and the band-1 sum
+    auto pix = [&](uint32_t w, uint32_t& s02, uint32_t& s1x) {
         const uint32_t al = w >> 24;
         const uint32_t t02 = (w & 0x00FF00FFu) * al + 0x00800080u;
         s02 += ((t02 + ((t02 >> 8) & 0x00FF00FFu)) >> 8) & 0x00FF00FFu;
         const uint32_t t1 = ((w >> 8) & 0xFFu) * al + 128u;
-        s1 += (t1 + (t1 >> 8)) >> 8;
+        s1x += (t1 + (t1 >> 8)) >> 8;
         s3 += al;
-        if ((j & 255) == 255) {  // each 16-bit lane holds at most 256 x 255
-            s0 += s02 & 0xFFFFu;
-            s2 += s02 >> 16;
-            s02 = 0;
+    };
+    for (int j0 = 0; j0 < fh; j0 += 256) {  // each 16-bit lane holds at most 256 x 255
+        const int j1 = min(fh, j0 + 256);
+        uint32_t a02 = 0, b02 = 0, a1 = 0, b1 = 0;
+        int j = j0;
+        for (; j + 2 <= j1; j += 2) {
+            uint32_t hi = wp[j + 1];
+            const uint32_t w0 = __funnelshift_r(lo, hi, sh);
+            lo = hi;
+            hi = wp[j + 2];
+            const uint32_t w1 = __funnelshift_r(lo, hi, sh);
+            lo = hi;
+            pix(w0, a02, a1);
+            pix(w1, b02, b1);
         }
+        if (j < j1) {
+            const uint32_t hi = wp[j + 1];
+            const uint32_t w0 = __funnelshift_r(lo, hi, sh);
+            lo = hi;
+            pix(w0, a02, a1);
+        }
+        s0 += (a02 & 0xFFFFu) + (b02 & 0xFFFFu);
+        s2 += (a02 >> 16) + (b02 >> 16);
+        s1 += a1 + b1;
     }
-    sums[0] = s0 + (s02 & 0xFFFFu);
+    sums[0] = s0;
     sums[1] = s1;
-    sums[2] = s2 + (s02 >> 16);
+    sums[2] = s2;
     sums[3] = s3;
 }
 
@@ -641,14 +669,14 @@ __device__ bool ws_produce(const ShrinkArgs& a, const uint8_t* in_data, int32_t 
 // block b owns items b, b + G, ...  The host picks the chunk count, ring depth
 // and blocks per SM (makespan model over the resident grid).
 template <int B, int P>
-__global__ void __launch_bounds__(kWsThreads) shrink_hv_u8_ws(ShrinkArgs a) {
+__global__ void __launch_bounds__(kWsThreads, 5) shrink_hv_u8_ws(ShrinkArgs a) {
     extern __shared__ __align__(128) uint8_t smem_ws[];
     WsRing* ring = reinterpret_cast<WsRing*>(smem_ws);
     volatile int32_t* stop = reinterpret_cast<volatile int32_t*>(smem_ws + sizeof(WsRing));
-    uint8_t* bufs = smem_ws + (sizeof(WsRing) + 4 + 127) / 128 * 128;
+    uint8_t* bufs = smem_ws + (sizeof(WsRing) + 4 + 127) / 128 * 128;  // stop flag after the ring
     const int S = a.stages;
-    const int32_t chunks = a.chunks, G = gridDim.x;
-    const int32_t n_items = a.out.h * chunks;
+    const int32_t chunks = a.chunks, G = gridDim.x, rpi = a.rows_per_item;
+    const int32_t n_items = ((a.out.h + rpi - 1) / rpi) * chunks;
     if (threadIdx.x == 0) {
         ws_ring_init(ring, S);
         *stop = 0;
@@ -661,9 +689,10 @@ __global__ void __launch_bounds__(kWsThreads) shrink_hv_u8_ws(ShrinkArgs a) {
             uint32_t ph = 0;
             int64_t issued = 0;
             for (int32_t item = blockIdx.x; item < n_items && *stop == 0; item += G) {
-                const int32_t oy = item / chunks;
-                const ShrinkChunk c = shrink_chunk(a, item - oy * chunks);
-                if (!ws_produce<B>(a, a.in.data, oy, oy + 1, c, ring, bufs, a.stage_bytes, S, slot, ph, issued)) {
+                const int32_t band = item / chunks;
+                const ShrinkChunk c = shrink_chunk(a, item - band * chunks);
+                const int32_t oy0 = band * rpi, oy1 = min(a.out.h, oy0 + rpi);
+                if (!ws_produce<B>(a, a.in.data, oy0, oy1, c, ring, bufs, a.stage_bytes, S, slot, ph, issued)) {
                     *stop = 1;
                     if (a.err) atomicExch(a.err, VIPRS_ERR_TIMEOUT);
                     break;
@@ -676,9 +705,10 @@ __global__ void __launch_bounds__(kWsThreads) shrink_hv_u8_ws(ShrinkArgs a) {
     int slot = 0;
     uint32_t ph = 0;
     for (int32_t item = blockIdx.x; item < n_items; item += G) {
-        const int32_t oy = item / chunks;
-        const ShrinkChunk c = shrink_chunk(a, item - oy * chunks);
-        if (!ws_consume<B, P>(a, oy, oy + 1, c, ring, bufs, a.stage_bytes, S, slot, ph, stop)) {
+        const int32_t band = item / chunks;
+        const ShrinkChunk c = shrink_chunk(a, item - band * chunks);
+        const int32_t oy0 = band * rpi, oy1 = min(a.out.h, oy0 + rpi);
+        if (!ws_consume<B, P>(a, oy0, oy1, c, ring, bufs, a.stage_bytes, S, slot, ph, stop)) {
             if (threadIdx.x == 0 && a.err) atomicExch(a.err, VIPRS_ERR_TIMEOUT);
             break;
         }
