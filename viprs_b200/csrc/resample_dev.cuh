@@ -942,6 +942,136 @@ __device__ __forceinline__ T fused_taps_rows(const uint8_t* base, const int32_t*
     }
 }
 
+// All NB bands of one output pixel at once: the coefficient of each tap is
+// loaded once for the NB products.  p[k * stride + b] is band b of tap
+// position k, k = clamp(s + t, 0, hi); each band keeps fused_taps' order.
+// `lanes`: bit b set when band b lies in the V f32 vector body.
+template <typename T, int MODE, bool HORIZ, int NB>
+__device__ __forceinline__ void fused_taps_px(const T* p, int s, int hi, int stride, int taps, const uint8_t* coef,
+                                              int ph, uint32_t lanes, T* out) {
+    const bool inside = s >= 0 && s + taps - 1 <= hi;
+    if (MODE == kReduceFixed) {
+        const int16_t* c = reinterpret_cast<const int16_t*>(coef) + ph * taps;
+        int32_t acc[NB];
+#pragma unroll
+        for (int b = 0; b < NB; ++b) acc[b] = 0;
+        if (inside) {
+            const T* q = p + s * stride;
+#pragma unroll 4
+            for (int t = 0; t < taps; ++t) {
+                const int32_t ct = c[t];
+#pragma unroll
+                for (int b = 0; b < NB; ++b) acc[b] += ct * (int32_t)q[t * stride + b];
+            }
+        } else {
+            for (int t = 0; t < taps; ++t) {
+                int k = s + t;
+                k = k < 0 ? 0 : (k > hi ? hi : k);
+                const int32_t ct = c[t];
+#pragma unroll
+                for (int b = 0; b < NB; ++b) acc[b] += ct * (int32_t)p[k * stride + b];
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < NB; ++b) out[b] = from_fixed<T>(acc[b]);
+    } else {
+        const double* c = reinterpret_cast<const double*>(coef) + ph * taps;
+        auto pos = [&](int t) {
+            int k = s + t;
+            if (!inside) k = k < 0 ? 0 : (k > hi ? hi : k);
+            return k * stride;
+        };
+        double acc[NB];
+#pragma unroll
+        for (int b = 0; b < NB; ++b) acc[b] = 0.0;
+        if (MODE == kReduceF32Simd && HORIZ) {
+            int t = 0;
+            for (; t + 4 <= taps; t += 4) {
+                const int k0 = pos(t), k1 = pos(t + 1), k2 = pos(t + 2), k3 = pos(t + 3);
+#pragma unroll
+                for (int b = 0; b < NB; ++b) {
+                    double lanes4 = as_f64(p[k0 + b]) * c[t];
+                    lanes4 = lanes4 + as_f64(p[k1 + b]) * c[t + 1];
+                    lanes4 = lanes4 + as_f64(p[k2 + b]) * c[t + 2];
+                    lanes4 = lanes4 + as_f64(p[k3 + b]) * c[t + 3];
+                    acc[b] = acc[b] + lanes4;
+                }
+            }
+            for (; t < taps; ++t) {
+                const int k = pos(t);
+#pragma unroll
+                for (int b = 0; b < NB; ++b) acc[b] = fma(as_f64(p[k + b]), c[t], acc[b]);
+            }
+        } else {
+            for (int t = 0; t < taps; ++t) {
+                const int k = pos(t);
+                const double ct = c[t];
+#pragma unroll
+                for (int b = 0; b < NB; ++b) {
+                    if (MODE == kReduceF32Simd && ((lanes >> b) & 1u)) acc[b] = acc[b] + as_f64(p[k + b]) * ct;
+                    else acc[b] = fma(as_f64(p[k + b]), ct, acc[b]);
+                }
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < NB; ++b) out[b] = from_f64<T>(acc[b]);
+    }
+}
+
+// The same vertical sum over staged source rows whose starts differ per row.
+template <typename T, int MODE, int NB>
+__device__ __forceinline__ void fused_taps_rows_px(const uint8_t* base, const int32_t* rowbase, int col_bytes, int s,
+                                                   int hi, int taps, const uint8_t* coef, int ph, uint32_t lanes,
+                                                   T* out) {
+    if (MODE == kReduceFixed) {
+        const int16_t* c = reinterpret_cast<const int16_t*>(coef) + ph * taps;
+        int32_t acc[NB];
+#pragma unroll
+        for (int b = 0; b < NB; ++b) acc[b] = 0;
+#pragma unroll 4
+        for (int t = 0; t < taps; ++t) {
+            int k = s + t;
+            k = k < 0 ? 0 : (k > hi ? hi : k);
+            const T* q = reinterpret_cast<const T*>(base + rowbase[k] + col_bytes);
+            const int32_t ct = c[t];
+#pragma unroll
+            for (int b = 0; b < NB; ++b) acc[b] += ct * (int32_t)q[b];
+        }
+#pragma unroll
+        for (int b = 0; b < NB; ++b) out[b] = from_fixed<T>(acc[b]);
+    } else {
+        const double* c = reinterpret_cast<const double*>(coef) + ph * taps;
+        double acc[NB];
+#pragma unroll
+        for (int b = 0; b < NB; ++b) acc[b] = 0.0;
+        for (int t = 0; t < taps; ++t) {
+            int k = s + t;
+            k = k < 0 ? 0 : (k > hi ? hi : k);
+            const T* q = reinterpret_cast<const T*>(base + rowbase[k] + col_bytes);
+            const double ct = c[t];
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                if (MODE == kReduceF32Simd && ((lanes >> b) & 1u)) acc[b] = acc[b] + as_f64(q[b]) * ct;
+                else acc[b] = fma(as_f64(q[b]), ct, acc[b]);
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < NB; ++b) out[b] = from_f64<T>(acc[b]);
+    }
+}
+
+// Walk the (row, column) pairs of a rows x cols grid, thread-strided.
+template <typename F>
+__device__ __forceinline__ void grid_walk(int rows, int cols, F&& f) {
+    int r = threadIdx.x / cols, c = threadIdx.x - r * cols;
+    const int dr = kCThreads / cols, dc = kCThreads - dr * cols;
+    for (; r < rows;) {
+        f(r, c);
+        r += dr; c += dc;
+        if (c >= cols) { c -= cols; ++r; }
+    }
+}
+
 // Copy `bytes` (a multiple of 16, both pointers 16-byte aligned) global -> shared.
 __device__ __forceinline__ void copy_table16(uint8_t* dst, const void* src, int bytes) {
     const uint4* s = reinterpret_cast<const uint4*>(src);
@@ -1033,7 +1163,14 @@ __device__ void reduce2d_tile(const Reduce2DArgs& a, int bx, int by, uint8_t* sm
         }
         // H: mid[r][x*B + b]
         const int W1 = ncols * B;
-        {
+        if constexpr (NB > 0) {
+            // one thread per (mid row, pixel), all bands
+            grid_walk(R, ncols, [&](int r, int x) {
+                const T* row = reinterpret_cast<const T*>(ins + rowbase[r]);
+                const int s = int(sx[x] - a.in.x0 - c0);
+                fused_taps_px<T, MH, true, NB>(row, s, C - 1, NB, a.taps_h, ch, phx[x], 0u, mid + r * W1 + x * NB);
+            });
+        } else {
             int r = threadIdx.x / W1, j = threadIdx.x - r * W1;
             const int dr = kCThreads / W1, dj = kCThreads - dr * W1;
             for (; r < R;) {
@@ -1047,7 +1184,17 @@ __device__ void reduce2d_tile(const Reduce2DArgs& a, int bx, int by, uint8_t* sm
         }
         csync();
         // V: out[y][x*B + b]
-        {
+        if constexpr (NB > 0) {
+            grid_walk(nrows, ncols, [&](int y, int x) {
+                const int s = int(sy[y] - rlo);
+                uint32_t lanes = 0;
+#pragma unroll
+                for (int b = 0; b < NB; ++b)
+                    if ((int64_t)(tx0 + x) * NB + b < a.vector_len) lanes |= 1u << b;
+                fused_taps_px<T, MV, false, NB>(mid + x * NB, s, R - 1, W1, a.taps_v, cv, phy[y], lanes,
+                                                ost + y * W1 + x * NB);
+            });
+        } else {
             int y = threadIdx.x / W1, j = threadIdx.x - y * W1;
             const int dy = kCThreads / W1, dj = kCThreads - dy * W1;
             for (; y < nrows;) {
@@ -1076,7 +1223,19 @@ __device__ void reduce2d_tile(const Reduce2DArgs& a, int bx, int by, uint8_t* sm
         }
         // V: mid[y][c*B + b]
         const int W1 = Cm * B;
-        {
+        if constexpr (NB > 0) {
+            grid_walk(nrows, Cm, [&](int y, int cc) {
+                const int64_t mcol = clo + cc;
+                const int col = int(clampi64(mcol - a.in.x0, 0, pw) - c0);
+                const int s = int(sy[y] - a.in.y0 - r0);
+                uint32_t lanes = 0;
+#pragma unroll
+                for (int b = 0; b < NB; ++b)
+                    if ((mcol - a.mx0) * NB + b < a.vector_len) lanes |= 1u << b;
+                fused_taps_rows_px<T, MV, NB>(ins, rowbase, col * NB * int(sizeof(T)), s, R - 1, a.taps_v, cv, phy[y],
+                                              lanes, mid + y * W1 + cc * NB);
+            });
+        } else {
             int y = threadIdx.x / W1, j = threadIdx.x - y * W1;
             const int dy = kCThreads / W1, dj = kCThreads - dy * W1;
             for (; y < nrows;) {
@@ -1094,7 +1253,13 @@ __device__ void reduce2d_tile(const Reduce2DArgs& a, int bx, int by, uint8_t* sm
         csync();
         // H: out[y][x*B + b]
         const int W2 = ncols * B;
-        {
+        if constexpr (NB > 0) {
+            grid_walk(nrows, ncols, [&](int y, int x) {
+                const int s = int(sx[x] - clo);
+                fused_taps_px<T, MH, true, NB>(mid + y * W1, s, Cm - 1, NB, a.taps_h, ch, phx[x], 0u,
+                                               ost + y * W2 + x * NB);
+            });
+        } else {
             int y = threadIdx.x / W2, j = threadIdx.x - y * W2;
             const int dy = kCThreads / W2, dj = kCThreads - dy * W2;
             for (; y < nrows;) {
