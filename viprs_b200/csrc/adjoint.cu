@@ -17,49 +17,49 @@
 //   mapim_grad_kernel ...... d/d(image) scatter; d/d(coordinates) by the
 //                            quotient rule over the renormalised separable
 //                            weights (affine/core.rs:648-696)
+#include <algorithm>
+
 #include "adjoint_launch.hpp"
 #include "affine_dev.cuh"
 
 namespace viprs {
 namespace dev {
 
+// One block row per input row (grid-stride over rows), threads over the row's
+// samples; 32-bit indexing (every plane holds fewer than 2^31 samples).
 __global__ void __launch_bounds__(256) reduce_adjoint_kernel(ReduceAdjArgs a) {
-    const int64_t n = (int64_t)a.in_w * a.in_h * a.bands;
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= n) return;
-    const int b = int(idx % a.bands);
-    const int64_t px = idx / a.bands;
-    const int32_t ix = int32_t(px % a.in_w), iy = int32_t(px / a.in_w);
-    // the axis this pass folds, and the index along it
-    const int32_t i = a.horizontal ? ix : iy;
-    const int32_t n_axis = a.horizontal ? a.in_w : a.in_h;
-    double acc = 0.0;
-    // rows of g_out this input row gathers from (H pass: one row, or the
-    // virtual rows that the source read clamps onto an edge row)
-    int32_t r0 = iy, r1 = iy;
-    if (a.horizontal && a.fold_rows) {
-        const int32_t mrows = a.out_h;
-        r0 = iy - a.mid_y0;
-        r1 = r0;
-        if (iy == 0) r0 = 0;
-        if (iy == a.in_h - 1) r1 = mrows - 1;
-        r0 = r0 < 0 ? 0 : r0;
-        r1 = r1 >= mrows ? mrows - 1 : r1;
-    }
-    const int32_t olo = a.lo[i], ohi = a.hi[i];
-    for (int32_t r = r0; r <= r1; ++r) {
-        for (int32_t o = olo; o <= ohi; ++o) {
-            double w;
-            if (n_axis == 1) w = a.fold_lo[o] + 0.0;
-            else if (i == 0) w = a.fold_lo[o];
-            else if (i == n_axis - 1) w = a.fold_hi[o];
-            else w = a.coeffs[a.phases[o] * a.taps + (i - a.starts[o])];
-            const int64_t g = a.horizontal ? ((int64_t)r * a.out_w + o) * a.bands + b
-                                           : ((int64_t)o * a.out_w + ix) * a.bands + b;
-            acc = fma((double)a.g_out[g], w, acc);
+    const int32_t rowlen = a.in_w * a.bands;
+    const int32_t t = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (t >= rowlen) return;
+    const int32_t ix = t / a.bands, b = t - ix * a.bands;
+    const int32_t gstride = a.out_w * a.bands;  // g_out row length
+    for (int32_t iy = (int32_t)blockIdx.y; iy < a.in_h; iy += (int32_t)gridDim.y) {
+        const int32_t i = a.horizontal ? ix : iy;  // index along the folded axis
+        // rows of g_out this input row gathers (H pass: one row, or the
+        // virtual rows that the source read clamps onto an edge row)
+        int32_t r0 = iy, r1 = iy;
+        if (a.horizontal && a.fold_rows) {
+            r0 = iy - a.mid_y0;
+            r1 = r0;
+            if (iy == 0) r0 = 0;
+            if (iy == a.in_h - 1) r1 = a.out_h - 1;
+            r0 = r0 < 0 ? 0 : r0;
+            r1 = r1 >= a.out_h ? a.out_h - 1 : r1;
         }
+        const int32_t olo = a.lo[i], n = a.hi[i] - olo + 1;
+        const double* w = a.wt + (size_t)i * a.wstride;
+        double acc = 0.0;
+        if (a.horizontal) {
+            for (int32_t r = r0; r <= r1; ++r) {
+                const float* g = a.g_out + (size_t)r * gstride + (size_t)olo * a.bands + b;
+                for (int32_t j = 0; j < n; ++j) acc = fma((double)g[j * a.bands], w[j], acc);
+            }
+        } else {
+            const float* g = a.g_out + (size_t)olo * gstride + t;
+            for (int32_t j = 0; j < n; ++j) acc = fma((double)g[(size_t)j * gstride], w[j], acc);
+        }
+        a.g_in[(size_t)iy * rowlen + t] = (float)acc;
     }
-    a.g_in[idx] = (float)acc;
 }
 
 // Image-gradient scatter; both targets null = the image gradient was not requested.
@@ -67,6 +67,9 @@ __device__ __forceinline__ void scatter(float* g, unsigned long long* fx, double
     if (fx) atomicAdd(fx + idx, (unsigned long long)(long long)llrint(v * scale));
     else if (g) atomicAdd(g + idx, (float)v);
 }
+
+// Output pixels per thread of the affine gradient kernel.
+constexpr int kGradGroup = 8;
 
 // Bilinear forward of one band with derivative, from four samples.
 struct Bil {
@@ -81,104 +84,123 @@ __device__ __forceinline__ Bil bil(double p00, double p01, double p10, double p1
     return r;
 }
 
+// Gradient contributions of one output pixel at position (x_in, y_in); NB
+// bands (NB == 0: a.bands, up to 8, read at run time).
+template <int NB>
+__device__ __forceinline__ void affine_grad_px(const AffineGradArgs& g, const AffineCtx<float>& c, double x_in,
+                                               double y_in, int64_t X, int64_t Y, const float* gy, double* part) {
+    const AffineArgs& a = g.fwd;
+    constexpr int NBmax = NB > 0 ? NB : 8;
+    const int bands = NB > 0 ? NB : a.bands;
+    if (!isfinite(x_in) || !isfinite(y_in)) return;
+    const int64_t x0 = trunc_i64(x_in), y0 = trunc_i64(y_in);
+    const double fx = x_in - (double)x0, fy = y_in - (double)y0;
+    const double w[4] = {(1.0 - fx) * (1.0 - fy), fx * (1.0 - fy), (1.0 - fx) * fy, fx * fy};
+    // element offset of each tap's first band in the input plane (-1: the constant fill)
+    const float* src = reinterpret_cast<const float*>(a.in.data);
+    const int64_t pitch_f = a.in.pitch / 4;
+    int64_t e[4];
+    double sv[4][NBmax];
+    const double fill = c.fill();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        int64_t rx, ry;
+        const bool ok = c.resolve(x0 + (k & 1), a.src_w, &rx) && c.resolve(y0 + (k >> 1), a.src_h, &ry) &&
+                        rx >= c.rx0 && rx <= c.rx1 && ry >= c.ry0 && ry <= c.ry1;
+        e[k] = ok ? (ry - a.in.y0) * pitch_f + (rx - a.in.x0) * bands : -1;
+#pragma unroll
+        for (int b = 0; b < NBmax; ++b)
+            if (b < bands) sv[k][b] = ok ? (double)src[e[k] + b] : fill;
+    }
+    double dx = 0.0, dy = 0.0;
+    if (bands == 4 && !a.premultiplied) {
+        // alpha-premultiplied sampler (affine/core.rs:988-1019), alpha_max = 1
+        double al[4], pm[3][4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) al[k] = sv[k][3];
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) pm[b][k] = sv[k][b] * al[k];
+        const Bil A = bil(al[0], al[1], al[2], al[3], fx, fy);
+        Bil P[3];
+#pragma unroll
+        for (int b = 0; b < 3; ++b) P[b] = bil(pm[b][0], pm[b][1], pm[b][2], pm[b][3], fx, fy);
+        double dP[3] = {0, 0, 0}, dA = 0.0;
+        if (A.out > 0.0 && A.out < 1.0) {
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                dP[b] = (double)gy[b] / A.out;
+                dA -= (double)gy[b] * P[b].out / (A.out * A.out);
+            }
+            dA += (double)gy[3];
+        } else if (A.out >= 1.0) {
+#pragma unroll
+            for (int b = 0; b < 3; ++b) dP[b] = (double)gy[b];
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (e[k] < 0) continue;
+            double da = dA * w[k];
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                scatter(g.g_in, g.g_fixed, g.fixed_scale, e[k] + b, dP[b] * w[k] * al[k]);
+                da += dP[b] * w[k] * sv[k][b];
+            }
+            scatter(g.g_in, g.g_fixed, g.fixed_scale, e[k] + 3, da);
+        }
+#pragma unroll
+        for (int b = 0; b < 3; ++b) { dx += dP[b] * P[b].dfx; dy += dP[b] * P[b].dfy; }
+        dx += dA * A.dfx;
+        dy += dA * A.dfy;
+    } else {
+#pragma unroll
+        for (int b = 0; b < NBmax; ++b) {
+            if (b >= bands) break;
+            const double gb = (double)gy[b];
+            const Bil v = bil(sv[0][b], sv[1][b], sv[2][b], sv[3][b], fx, fy);
+            dx += gb * v.dfx;
+            dy += gb * v.dfy;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (e[k] >= 0) scatter(g.g_in, g.g_fixed, g.fixed_scale, e[k] + b, gb * w[k]);
+        }
+    }
+    // x_in = m0 X + m1 Y + tx, y_in = m2 X + m3 Y + ty
+    part[0] += dx * (double)X; part[1] += dx * (double)Y;
+    part[2] += dy * (double)X; part[3] += dy * (double)Y;
+    part[4] += dx; part[5] += dy;
+}
+
+// kGradGroup consecutive output pixels of one row per thread, positions by
+// the same walk as the forward kernel (AffineWalk), fixed per-thread order of
+// the matrix-gradient partial sums.
+template <int NB>
 __global__ void __launch_bounds__(256) affine_grad_kernel(AffineGradArgs g) {
     const AffineArgs& a = g.fwd;
-    const int64_t npx = (int64_t)a.out.w * a.out.h;
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t gw = (a.out.w + kGradGroup - 1) / kGradGroup;
+    const int64_t gi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     double part[6] = {0, 0, 0, 0, 0, 0};
-    if (p < npx) {
-        const int64_t ly = p / a.out.w, lx = p - ly * a.out.w;
-        const int64_t X = a.out.x0 + lx, Y = a.out.y0 + ly;
-        AffineCtx<float> c(a);
-        c.set_tile(X, Y);
+    if (gi < gw * a.out.h) {
+        const int64_t ly = gi / gw, lx0 = (gi - ly * gw) * kGradGroup;
+        const int64_t lx1 = min((int64_t)a.out.w, lx0 + kGradGroup);
+        const int64_t Y = a.out.y0 + ly;
         const double* m = a.m;
-        double x_in, y_in;
-        if (a.fast == 2 && X >= 0 && X < (int64_t)a.total_w && Y >= 0 && Y < (int64_t)a.total_h) {
-            x_in = fma(m[0], (double)X, a.tx);
-            y_in = fma(m[3], (double)Y, a.ty);
-        } else if (a.separable && a.xs != nullptr) {
-            x_in = a.xs[X];
-            y_in = a.ys[Y];
-        } else {
-            const int64_t X0 = tile_origin(X, a.tile_off_x, a.tile_w), Y0 = tile_origin(Y, a.tile_off_y, a.tile_h);
-            double rx = fma(m[1], (double)Y0, m[0] * (double)X0) + a.tx;
-            double ry = fma(m[3], (double)Y0, m[2] * (double)X0) + a.ty;
-            for (int64_t r = Y0; r < Y; ++r) { rx += m[1]; ry += m[3]; }
-            x_in = rx; y_in = ry;
-            for (int64_t q = X0; q < X; ++q) { x_in += m[0]; y_in += m[2]; }
-        }
-        const int bands = a.bands;
-        const float* gy = g.g_out + p * bands;
-        if (isfinite(x_in) && isfinite(y_in)) {
-            const int64_t x0 = trunc_i64(x_in), y0 = trunc_i64(y_in);
-            const double fx = x_in - (double)x0, fy = y_in - (double)y0;
-            const double w[4] = {(1.0 - fx) * (1.0 - fy), fx * (1.0 - fy), (1.0 - fx) * fy, fx * fy};
-            const int64_t tx_[4] = {x0, x0 + 1, x0, x0 + 1}, ty_[4] = {y0, y0, y0 + 1, y0 + 1};
-            // resolved in-plane sample index of each tap (-1: the constant fill)
-            int64_t lin[4];
-            for (int k = 0; k < 4; ++k) {
-                int64_t rx, ry;
-                const bool ok = c.resolve(tx_[k], a.src_w, &rx) && c.resolve(ty_[k], a.src_h, &ry) && rx >= c.rx0 &&
-                                rx <= c.rx1 && ry >= c.ry0 && ry <= c.ry1;
-                lin[k] = ok ? ((ry - a.in.y0) * (int64_t)a.in.w + (rx - a.in.x0)) : -1;
+        AffineCtx<float> c(a);
+        AffineWalk walk;
+        for (int64_t lx = lx0; lx < lx1; ++lx) {
+            const int64_t X = a.out.x0 + lx;
+            walk.step<float>(a, c, X, Y);
+            double x_in = walk.x, y_in = walk.y;
+            if (a.fast == 2 && X >= 0 && X < (int64_t)a.total_w && Y >= 0 && Y < (int64_t)a.total_h) {
+                x_in = fma(m[0], (double)X, a.tx);
+                y_in = fma(m[3], (double)Y, a.ty);
+            } else if (a.separable && a.xs != nullptr) {
+                x_in = a.xs[X];
+                y_in = a.ys[Y];
             }
-            const float* src = reinterpret_cast<const float*>(a.in.data);
-            const int64_t pitch_f = a.in.pitch / 4;
-            auto sample = [&](int k, int band) -> double {
-                if (lin[k] < 0) return c.fill();
-                const int64_t ry = lin[k] / a.in.w, rx = lin[k] - ry * a.in.w;
-                return (double)src[ry * pitch_f + rx * bands + band];
-            };
-            auto gidx = [&](int k, int band) -> int64_t {
-                const int64_t ry = lin[k] / a.in.w, rx = lin[k] - ry * a.in.w;
-                return ry * pitch_f + rx * bands + band;
-            };
-            double dx = 0.0, dy = 0.0;
-            if (bands == 4 && !a.premultiplied) {
-                // alpha-premultiplied sampler (affine/core.rs:988-1019), alpha_max = 1
-                double al[4], pm[3][4];
-                for (int k = 0; k < 4; ++k) al[k] = sample(k, 3);
-                for (int b = 0; b < 3; ++b)
-                    for (int k = 0; k < 4; ++k) pm[b][k] = sample(k, b) * al[k];
-                const Bil A = bil(al[0], al[1], al[2], al[3], fx, fy);
-                Bil P[3];
-                for (int b = 0; b < 3; ++b) P[b] = bil(pm[b][0], pm[b][1], pm[b][2], pm[b][3], fx, fy);
-                double dP[3] = {0, 0, 0}, dA = 0.0;
-                if (A.out > 0.0 && A.out < 1.0) {
-                    for (int b = 0; b < 3; ++b) {
-                        dP[b] = (double)gy[b] / A.out;
-                        dA -= (double)gy[b] * P[b].out / (A.out * A.out);
-                    }
-                    dA += (double)gy[3];
-                } else if (A.out >= 1.0) {
-                    for (int b = 0; b < 3; ++b) dP[b] = (double)gy[b];
-                }
-                for (int k = 0; k < 4; ++k) {
-                    if (lin[k] < 0) continue;
-                    double da = dA * w[k];
-                    for (int b = 0; b < 3; ++b) {
-                        scatter(g.g_in, g.g_fixed, g.fixed_scale, gidx(k, b), dP[b] * w[k] * al[k]);
-                        da += dP[b] * w[k] * sample(k, b);
-                    }
-                    scatter(g.g_in, g.g_fixed, g.fixed_scale, gidx(k, 3), da);
-                }
-                for (int b = 0; b < 3; ++b) { dx += dP[b] * P[b].dfx; dy += dP[b] * P[b].dfy; }
-                dx += dA * A.dfx;
-                dy += dA * A.dfy;
-            } else {
-                for (int b = 0; b < bands; ++b) {
-                    const double gb = (double)gy[b];
-                    const Bil v = bil(sample(0, b), sample(1, b), sample(2, b), sample(3, b), fx, fy);
-                    dx += gb * v.dfx;
-                    dy += gb * v.dfy;
-                    for (int k = 0; k < 4; ++k)
-                        if (lin[k] >= 0) scatter(g.g_in, g.g_fixed, g.fixed_scale, gidx(k, b), gb * w[k]);
-                }
-            }
-            // x_in = m0 X + m1 Y + tx, y_in = m2 X + m3 Y + ty
-            part[0] = dx * (double)X; part[1] = dx * (double)Y;
-            part[2] = dy * (double)X; part[3] = dy * (double)Y;
-            part[4] = dx; part[5] = dy;
+            const float* gy = g.g_out + (ly * a.out.w + lx) * a.bands;
+            affine_grad_px<NB>(g, c, x_in, y_in, X, Y, gy, part);
         }
     }
     if (g.partial) {
@@ -222,106 +244,235 @@ __device__ __forceinline__ double kernel_dw(int k, double i_minus_x) {
     return dk * s;
 }
 
-__global__ void __launch_bounds__(256) mapim_grad_kernel(MapimGradArgs g) {
+// Image-gradient sink of one block of mapim_grad: while the block's scatter
+// footprint (the bounding box of every tap it writes) fits in shared memory,
+// contributions add there (shared atomics) and the block flushes the box to
+// the global gradient once; otherwise they go to global atomics directly.
+// Fixed-point sums stay integer all the way, so the deterministic mode keeps
+// its order independence.
+constexpr int kMapimTile = 16;           // 16 x 16 output pixels per block
+constexpr int kMapimSmemElems = 4096;    // footprint capacity (elements x bands)
+
+struct MapimSink {
+    float* sf = nullptr;
+    unsigned long long* su = nullptr;
+    int32_t bx0 = 0, by0 = 0, bw = 0;
+    bool local = false;
+    const MapimGradArgs* g = nullptr;
+    int64_t pitch_f = 0;
+    int bands = 1;
+    // element (rx, ry, b): local index li when the block accumulates
+    // locally, global index gi otherwise
+    __device__ __forceinline__ void add_at(int32_t li, int64_t gi, double v) const {
+        if (local) {
+            if (g->g_fixed) atomicAdd(su + li, (unsigned long long)(long long)llrint(v * g->fixed_scale));
+            else atomicAdd(sf + li, (float)v);
+        } else {
+            scatter(g->g_src, g->g_fixed, g->fixed_scale, gi, v);
+        }
+    }
+    __device__ __forceinline__ void add(int64_t rx, int64_t ry, int b, double v) const {
+        add_at(((int32_t)(ry - by0) * bw + (int32_t)(rx - bx0)) * bands + b, ry * pitch_f + rx * bands + b, v);
+    }
+};
+
+// NT: taps per axis of the separable samplers (4: support 2, 6: Lanczos3);
+// 0 for the nearest / bilinear kernels.
+template <int NT>
+__global__ void __launch_bounds__(256, 4) mapim_grad_kernel(MapimGradArgs g) {
+    extern __shared__ __align__(16) unsigned char mg_smem[];
+    __shared__ int32_t box[4];  // min x, max x, min y, max y of the block's taps
     const MapimArgs& a = g.fwd;
-    const int64_t npx = (int64_t)a.out.w * a.out.h;
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= npx) return;
-    const int64_t ly = p / a.out.w, lx = p - ly * a.out.w;
-    const float2 idx = *reinterpret_cast<const float2*>(a.index.data + ly * a.index.pitch + lx * 8);
-    const double x = (double)idx.x, y = (double)idx.y;
+    const int64_t lx = (int64_t)blockIdx.x * kMapimTile + (threadIdx.x % kMapimTile);
+    const int64_t ly = (int64_t)blockIdx.y * kMapimTile + (threadIdx.x / kMapimTile);
+    const bool live = lx < a.out.w && ly < a.out.h;
     const int bands = a.bands;
+    const int64_t p = ly * a.out.w + lx;
+    double x = NAN, y = NAN;
+    if (live) {
+        const float2 idx = *reinterpret_cast<const float2*>(a.index.data + ly * a.index.pitch + lx * 8);
+        x = (double)idx.x;
+        y = (double)idx.y;
+    }
+    const bool valid = live && isfinite(x) && isfinite(y);
+    const int k = a.kernel;
+    const bool want_img = g.g_src != nullptr || g.g_fixed != nullptr;
+    // tap bounding box of this pixel, clipped / clamped as the scatter resolves it
+    int64_t tx0 = 0, tx1 = -1, ty0 = 0, ty1 = -1;
+    const int64_t W = a.src_w, H = a.src_h;
+    if (valid && want_img) {
+        if (k == 0 || k == 1) {
+            const int64_t x0 = trunc_i64(floor(x)), y0 = trunc_i64(floor(y)), d = k;
+            tx0 = x0; tx1 = x0 + d; ty0 = y0; ty1 = y0 + d;
+            if (a.extend_copy) {
+                tx0 = clampi64(tx0, 0, W - 1); tx1 = clampi64(tx1, 0, W - 1);
+                ty0 = clampi64(ty0, 0, H - 1); ty1 = clampi64(ty1, 0, H - 1);
+            } else {
+                tx0 = max(tx0, (int64_t)0); tx1 = min(tx1, W - 1);
+                ty0 = max(ty0, (int64_t)0); ty1 = min(ty1, H - 1);
+            }
+        } else {
+            constexpr int64_t support = NT / 2;
+            const int64_t cx = trunc_i64(floor(x)), cy = trunc_i64(floor(y));
+            tx0 = max(cx - (support - 1), (int64_t)0); tx1 = min(cx + support, W - 1);
+            ty0 = max(cy - (support - 1), (int64_t)0); ty1 = min(cy + support, H - 1);
+        }
+    }
+    if (threadIdx.x == 0) { box[0] = INT32_MAX; box[1] = INT32_MIN; box[2] = INT32_MAX; box[3] = INT32_MIN; }
+    __syncthreads();
+    if (tx0 <= tx1 && ty0 <= ty1) {
+        atomicMin(&box[0], (int32_t)tx0); atomicMax(&box[1], (int32_t)tx1);
+        atomicMin(&box[2], (int32_t)ty0); atomicMax(&box[3], (int32_t)ty1);
+    }
+    __syncthreads();
+    MapimSink sink;
+    sink.g = &g;
+    sink.bands = bands;
+    sink.pitch_f = a.src.pitch / 4;
+    const int64_t bw = (int64_t)box[1] - box[0] + 1, bh = (int64_t)box[3] - box[2] + 1;
+    const int64_t n_local = (box[1] >= box[0] && box[3] >= box[2]) ? bw * bh * bands : 0;
+    sink.local = n_local > 0 && n_local <= kMapimSmemElems;  // uniform across the block
+    if (sink.local) {
+        sink.bx0 = box[0]; sink.by0 = box[2]; sink.bw = (int32_t)bw;
+        if (g.g_fixed) {
+            sink.su = reinterpret_cast<unsigned long long*>(mg_smem);
+            for (int i = threadIdx.x; i < (int)n_local; i += blockDim.x) sink.su[i] = 0ull;
+        } else {
+            sink.sf = reinterpret_cast<float*>(mg_smem);
+            for (int i = threadIdx.x; i < (int)n_local; i += blockDim.x) sink.sf[i] = 0.0f;
+        }
+        __syncthreads();
+    }
     const float* gy = g.g_out + p * bands;
     const float* src = reinterpret_cast<const float*>(a.src.data);
     const int64_t pitch_f = a.src.pitch / 4;
     double gx = 0.0, gyy = 0.0;
-    if (isfinite(x) && isfinite(y)) {
-        const int k = a.kernel;
-        auto inb = [&](int64_t ix, int64_t iy) {
-            return ix >= 0 && ix < (int64_t)a.src_w && iy >= 0 && iy < (int64_t)a.src_h;
-        };
+    if (valid) {
+        auto inb = [&](int64_t ix, int64_t iy) { return ix >= 0 && ix < W && iy >= 0 && iy < H; };
         if (k == 0) {
             const int64_t ix = trunc_i64(floor(x)), iy = trunc_i64(floor(y));
             int64_t rx = ix, ry = iy;
             bool ok = inb(ix, iy);
             if (!ok && a.extend_copy) {
-                ok = !(ix < -1 || ix > (int64_t)a.src_w || iy < -1 || iy > (int64_t)a.src_h);
-                rx = clampi64(ix, 0, (int64_t)a.src_w - 1);
-                ry = clampi64(iy, 0, (int64_t)a.src_h - 1);
+                ok = !(ix < -1 || ix > W || iy < -1 || iy > H);
+                rx = clampi64(ix, 0, W - 1);
+                ry = clampi64(iy, 0, H - 1);
             }
-            if (ok)
-                for (int b = 0; b < bands; ++b) scatter(g.g_src, g.g_fixed, g.fixed_scale, ry * pitch_f + rx * bands + b, gy[b]);
+            if (ok && want_img)
+                for (int b = 0; b < bands; ++b) sink.add(rx, ry, b, gy[b]);
         } else if (k == 1) {
             const int64_t x0 = trunc_i64(floor(x)), y0 = trunc_i64(floor(y));
             const double fx = x - (double)x0, fy = y - (double)y0;
             const double w[4] = {(1.0 - fx) * (1.0 - fy), fx * (1.0 - fy), (1.0 - fx) * fy, fx * fy};
-            const int64_t tx_[4] = {x0, x0 + 1, x0, x0 + 1}, ty_[4] = {y0, y0, y0 + 1, y0 + 1};
-            for (int b = 0; b < bands; ++b) {
-                double s[4];
-                for (int q = 0; q < 4; ++q) {
-                    int64_t rx = tx_[q], ry = ty_[q];
-                    bool ok = inb(rx, ry);
-                    if (!ok && a.extend_copy) {
-                        ok = !(rx < -1 || rx > (int64_t)a.src_w + 1 || ry < -1 || ry > (int64_t)a.src_h + 1);
-                        rx = clampi64(rx, 0, (int64_t)a.src_w - 1);
-                        ry = clampi64(ry, 0, (int64_t)a.src_h - 1);
-                    }
-                    s[q] = ok ? (double)src[ry * pitch_f + rx * bands + b] : a.background;
-                    if (ok) scatter(g.g_src, g.g_fixed, g.fixed_scale, ry * pitch_f + rx * bands + b, (double)gy[b] * w[q]);
+            int64_t rxq[4], ryq[4];
+            bool okq[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                int64_t rx = x0 + (q & 1), ry = y0 + (q >> 1);
+                bool ok = inb(rx, ry);
+                if (!ok && a.extend_copy) {
+                    ok = !(rx < -1 || rx > W + 1 || ry < -1 || ry > H + 1);
+                    rx = clampi64(rx, 0, W - 1);
+                    ry = clampi64(ry, 0, H - 1);
                 }
-                const Bil v = bil(s[0], s[1], s[2], s[3], fx, fy);
+                rxq[q] = rx; ryq[q] = ry; okq[q] = ok;
+            }
+            for (int b = 0; b < bands; ++b) {
+                double sq[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    // every tap loads (a clamped, readable address); the background replaces it after
+                    const double raw = (double)src[clampi64(ryq[q], 0, H - 1) * pitch_f + clampi64(rxq[q], 0, W - 1) * bands + b];
+                    sq[q] = okq[q] ? raw : a.background;
+                    if (okq[q] && want_img) sink.add(rxq[q], ryq[q], b, (double)gy[b] * w[q]);
+                }
+                const Bil v = bil(sq[0], sq[1], sq[2], sq[3], fx, fy);
                 gx += (double)gy[b] * v.dfx;
                 gyy += (double)gy[b] * v.dfy;
             }
-        } else {
-            const int64_t support = k == 9 ? 3 : 2;
+        } else if (NT > 0) {
+            // separable sampler y = N / W with N = sum_ij wx_i wy_j s_ij and
+            // W = (sum_i wx_i)(sum_j wy_j); taps whose weight and derivative
+            // are both zero are skipped, as the forward skips zero weights
+            constexpr int64_t support = NT / 2;
+            constexpr int nt = NT > 0 ? NT : 1;
             const int64_t cx = trunc_i64(floor(x)), cy = trunc_i64(floor(y));
-            const int nt = int(2 * support);
-            double wx[6], wy[6], dwx[6], dwy[6];
+            const int64_t tx0 = cx - (support - 1), ty0 = cy - (support - 1);
+            double wx[nt], dwx[nt], wy[nt], dwy[nt];
+            bool okx[nt];
+            int32_t col[nt], lcol[nt];
+            double Sx = 0.0, Sdx = 0.0, Sy = 0.0, Sdy = 0.0;
+#pragma unroll
             for (int t = 0; t < nt; ++t) {
-                const int64_t ix = cx - (support - 1) + t, iy = cy - (support - 1) + t;
+                const int64_t ix = tx0 + t, iy = ty0 + t;
                 wx[t] = kernel_w(k, fabs((double)ix - x));
-                wy[t] = kernel_w(k, fabs((double)iy - y));
                 dwx[t] = kernel_dw(k, (double)ix - x);
+                wy[t] = kernel_w(k, fabs((double)iy - y));
                 dwy[t] = kernel_dw(k, (double)iy - y);
+                Sx += wx[t]; Sdx += dwx[t]; Sy += wy[t]; Sdy += dwy[t];
+                okx[t] = ix >= 0 && ix < W;
+                col[t] = (int32_t)clampi64(ix, 0, W - 1) * bands;
+                lcol[t] = (int32_t)(ix - sink.bx0) * bands;
             }
-            double W = 0.0, Wx = 0.0, Wy = 0.0;
-            for (int ty = 0; ty < nt; ++ty) {
-                if (wy[ty] == 0.0) continue;
-                for (int tx = 0; tx < nt; ++tx) {
-                    if (wx[tx] == 0.0) continue;
-                    W += wx[tx] * wy[ty];
-                    Wx += dwx[tx] * wy[ty];
-                    Wy += wx[tx] * dwy[ty];
-                }
-            }
-            if (W > 0.0) {
+            const double Wt = Sx * Sy, Wx = Sdx * Sy, Wy = Sx * Sdy;
+            if (Wt > 0.0) {
+                const double inv = 1.0 / Wt;
                 for (int b = 0; b < bands; ++b) {
                     double Nv = 0.0, Nx = 0.0, Ny = 0.0;
                     const double gb = (double)gy[b];
+#pragma unroll 1
                     for (int ty = 0; ty < nt; ++ty) {
-                        if (wy[ty] == 0.0) continue;
-                        const int64_t iy = cy - (support - 1) + ty;
+                        if (wy[ty] == 0.0 && dwy[ty] == 0.0) continue;
+                        const int64_t iy = ty0 + ty;
+                        const bool oky = iy >= 0 && iy < H;
+                        const int64_t grow = clampi64(iy, 0, H - 1) * pitch_f + b;
+                        // the row's taps load unconditionally (clamped addresses)
+                        double sv[nt];
+#pragma unroll
+                        for (int tx = 0; tx < nt; ++tx) sv[tx] = (double)src[grow + col[tx]];
+                        double rv = 0.0, rd = 0.0;
+#pragma unroll
                         for (int tx = 0; tx < nt; ++tx) {
-                            if (wx[tx] == 0.0) continue;
-                            const int64_t ix = cx - (support - 1) + tx;
-                            const bool ok = inb(ix, iy);
-                            const double s = ok ? (double)src[iy * pitch_f + ix * bands + b] : a.background;
-                            Nv += wx[tx] * wy[ty] * s;
-                            Nx += dwx[tx] * wy[ty] * s;
-                            Ny += wx[tx] * dwy[ty] * s;
-                            if (ok) scatter(g.g_src, g.g_fixed, g.fixed_scale, iy * pitch_f + ix * bands + b, gb * wx[tx] * wy[ty] / W);
+                            if (wx[tx] == 0.0 && dwx[tx] == 0.0) continue;
+                            const double s = okx[tx] && oky ? sv[tx] : a.background;
+                            rv += wx[tx] * s;
+                            rd += dwx[tx] * s;
+                        }
+                        Nv += wy[ty] * rv;
+                        Nx += wy[ty] * rd;
+                        Ny += dwy[ty] * rv;
+                        if (want_img && oky && wy[ty] != 0.0) {
+                            const double c = gb * inv * wy[ty];
+                            const int32_t lrow = (int32_t)(iy - sink.by0) * sink.bw * bands + b;
+#pragma unroll
+                            for (int tx = 0; tx < nt; ++tx)
+                                if (okx[tx] && wx[tx] != 0.0) sink.add_at(lrow + lcol[tx], grow + col[tx], c * wx[tx]);
                         }
                     }
-                    gx += gb * (Nx * W - Nv * Wx) / (W * W);
-                    gyy += gb * (Ny * W - Nv * Wy) / (W * W);
+                    gx += gb * (Nx * Wt - Nv * Wx) / (Wt * Wt);
+                    gyy += gb * (Ny * Wt - Nv * Wy) / (Wt * Wt);
                 }
             }
         }
     }
-    if (g.g_index) {
+    if (g.g_index && live) {
         g.g_index[p * 2] = (float)gx;
         g.g_index[p * 2 + 1] = (float)gyy;
+    }
+    if (sink.local) {
+        __syncthreads();
+        const int32_t rowe = sink.bw * bands;
+        for (int i = threadIdx.x; i < (int)n_local; i += blockDim.x) {
+            const int r = i / rowe, c = i - r * rowe;
+            const int64_t gi = (int64_t)(sink.by0 + r) * pitch_f + (int64_t)sink.bx0 * bands + c;
+            if (g.g_fixed) {
+                const unsigned long long v = sink.su[i];
+                if (v) atomicAdd(g.g_fixed + gi, v);
+            } else {
+                const float v = sink.sf[i];
+                if (v != 0.0f) atomicAdd(g.g_src + gi, v);
+            }
+        }
     }
 }
 
@@ -330,13 +481,15 @@ __global__ void fixed_to_f32_kernel(const unsigned long long* acc, float* out, i
         out[i] = (float)((double)(long long)acc[i] * inv);
 }
 
-__global__ void sum_partials_kernel(const double* partial, int blocks, double* out) {
-    // one thread per component, fixed order: deterministic
-    if (threadIdx.x < 6) {
-        double s = 0.0;
-        for (int b = 0; b < blocks; ++b) s += partial[(int64_t)b * 6 + threadIdx.x];
-        out[threadIdx.x] = s;
-    }
+__global__ void __launch_bounds__(192) sum_partials_kernel(const double* partial, int blocks, double* out) {
+    // warp w sums component w: lane l takes blocks l, l + 32, ... and the lanes
+    // combine in a fixed butterfly, so the result is the same on every run
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    double s = 0.0;
+    for (int b = l; b < blocks; b += 32) s += partial[(int64_t)b * 6 + w];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (l == 0) out[w] = s;
 }
 
 }  // namespace dev
@@ -344,22 +497,45 @@ __global__ void sum_partials_kernel(const double* partial, int blocks, double* o
 namespace launch {
 
 cudaError_t reduce_adjoint(const ReduceAdjArgs& a, cudaStream_t s) {
-    const int64_t n = (int64_t)a.in_w * a.in_h * a.bands;
-    if (n <= 0) return cudaSuccess;
-    dev::reduce_adjoint_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a);
+    const int64_t rowlen = (int64_t)a.in_w * a.bands;
+    if (rowlen <= 0 || a.in_h <= 0) return cudaSuccess;
+    if (rowlen * a.in_h >= ((int64_t)1 << 31) || (int64_t)a.out_w * a.bands * a.out_h >= ((int64_t)1 << 31))
+        return cudaErrorInvalidValue;
+    const dim3 grid((unsigned)((rowlen + 255) / 256), (unsigned)std::min<int64_t>(a.in_h, 65535));
+    dev::reduce_adjoint_kernel<<<grid, 256, 0, s>>>(a);
     return cudaGetLastError();
+}
+
+int affine_grad_blocks(int32_t out_w, int32_t out_h) {
+    const int64_t groups = ((int64_t)out_w + dev::kGradGroup - 1) / dev::kGradGroup * out_h;
+    return (int)((groups + 255) / 256);
 }
 
 cudaError_t affine_grad(const AffineGradArgs& a, int blocks, cudaStream_t s) {
     if (blocks <= 0) return cudaSuccess;
-    dev::affine_grad_kernel<<<blocks, 256, 0, s>>>(a);
+    if (a.fwd.bands > 8) return cudaErrorInvalidValue;
+    switch (a.fwd.bands) {
+    case 1: dev::affine_grad_kernel<1><<<blocks, 256, 0, s>>>(a); break;
+    case 3: dev::affine_grad_kernel<3><<<blocks, 256, 0, s>>>(a); break;
+    case 4: dev::affine_grad_kernel<4><<<blocks, 256, 0, s>>>(a); break;
+    default: dev::affine_grad_kernel<0><<<blocks, 256, 0, s>>>(a); break;
+    }
     return cudaGetLastError();
 }
 
 cudaError_t mapim_grad(const MapimGradArgs& a, cudaStream_t s) {
     const int64_t npx = (int64_t)a.fwd.out.w * a.fwd.out.h;
     if (npx <= 0) return cudaSuccess;
-    dev::mapim_grad_kernel<<<(unsigned)((npx + 255) / 256), 256, 0, s>>>(a);
+    const int64_t gx = ((int64_t)a.fwd.out.w + dev::kMapimTile - 1) / dev::kMapimTile;
+    const int64_t gy = ((int64_t)a.fwd.out.h + dev::kMapimTile - 1) / dev::kMapimTile;
+    if (gy > 65535 || (int64_t)a.fwd.src_w * a.fwd.bands >= ((int64_t)1 << 31) || a.fwd.src_h >= (1u << 31))
+        return cudaErrorInvalidValue;
+    const size_t smem = (size_t)dev::kMapimSmemElems * (a.g_fixed ? 8 : 4);
+    const dim3 grid((unsigned)gx, (unsigned)gy);
+    const int k = a.fwd.kernel;
+    if (k == 0 || k == 1) dev::mapim_grad_kernel<0><<<grid, dev::kMapimTile * dev::kMapimTile, smem, s>>>(a);
+    else if (k == 9) dev::mapim_grad_kernel<6><<<grid, dev::kMapimTile * dev::kMapimTile, smem, s>>>(a);
+    else dev::mapim_grad_kernel<4><<<grid, dev::kMapimTile * dev::kMapimTile, smem, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -371,7 +547,7 @@ cudaError_t fixed_to_f32(const unsigned long long* acc, float* out, int64_t n, d
 }
 
 cudaError_t sum_partials(const double* partial, int blocks, double* out, cudaStream_t s) {
-    dev::sum_partials_kernel<<<1, 32, 0, s>>>(partial, blocks, out);
+    dev::sum_partials_kernel<<<1, 192, 0, s>>>(partial, blocks, out);
     return cudaGetLastError();
 }
 

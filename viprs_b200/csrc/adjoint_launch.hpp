@@ -15,10 +15,9 @@ namespace viprs {
 
 // Transpose of one separable reduce pass over f32, as a gather: every input
 // sample sums the output samples whose taps read it.  For input index i the
-// outputs are [lo[i], hi[i]] (lo > hi: none); the weight of output o is
-// coeffs[phase[o]][i - start[o]], and at the two clamped edges the sum of the
-// folded taps (fold_lo / fold_hi give, per output, the summed weight that
-// clamp_axis folds onto the first / last index).
+// outputs are [lo[i], hi[i]] (lo > hi: none) and the weight of output o is
+// wt[i * wstride + (o - lo[i])]: the forward coefficient of that tap, or at a
+// clamped edge the sum of the taps that clamp_axis folds onto it.
 struct ReduceAdjArgs {
     const float* g_out = nullptr;  // gradient wrt the pass output
     float* g_in = nullptr;         // gradient wrt the pass input (overwritten)
@@ -26,18 +25,15 @@ struct ReduceAdjArgs {
     int32_t out_w = 0, out_h = 0;  // pass output size
     int32_t in_w = 0, in_h = 0;    // pass input size (the folded axis)
     int32_t bands = 1;
-    int32_t taps = 1;
-    const int32_t* starts = nullptr;   // per output index, relative to the input origin
-    const uint8_t* phases = nullptr;
-    const double* coeffs = nullptr;    // 65 x taps
-    const int32_t* lo = nullptr;       // per input index
+    const int32_t* lo = nullptr;   // per input index
     const int32_t* hi = nullptr;
-    const double* fold_lo = nullptr;   // per output index
-    const double* fold_hi = nullptr;
-    // input row / column r of this pass corresponds to row / column clamp(r, 0, n-1)
-    // of the gradient buffer (the source read's edge replication), `n` = g_in extent
-    int32_t fold_rows = 0;             // V pass of an H-then-V chain folds virtual mid rows
-    int32_t mid_y0 = 0;                // origin of the pass input rows (may be negative)
+    const double* wt = nullptr;    // per input index, wstride weights
+    int32_t wstride = 1;
+    // H pass of an H-then-V chain: input row r gathers mid row r - mid_y0, and
+    // the edge rows also gather the virtual mid rows that the source read
+    // clamps onto them
+    int32_t fold_rows = 0;
+    int32_t mid_y0 = 0;            // origin of the mid rows (may be negative)
 };
 
 // Gradient of the bilinear affine (forward: Affine::process_region with
@@ -62,6 +58,8 @@ struct MapimGradArgs {
 
 namespace launch {
 cudaError_t reduce_adjoint(const ReduceAdjArgs& a, cudaStream_t s);
+// blocks of affine_grad for an out_w x out_h output (one partial row each)
+int affine_grad_blocks(int32_t out_w, int32_t out_h);
 cudaError_t affine_grad(const AffineGradArgs& a, int blocks, cudaStream_t s);
 cudaError_t mapim_grad(const MapimGradArgs& a, cudaStream_t s);
 // fixed-point accumulator -> f32 (deterministic scatter), n values

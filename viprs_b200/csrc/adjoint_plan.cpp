@@ -13,6 +13,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "adjoint_launch.hpp"
@@ -57,40 +60,40 @@ int check_f32(const viprs_image* im) {
 
 // Tables of one transposed reduce pass.  `out_origin`/`out_len`: the pass's
 // output positions; the pass input has `in_len` samples starting at `in_origin`
-// (clamp folding at both ends when `fold`).
+// (clamp folding at both ends when `fold`).  Input index i gathers outputs
+// [lo[i], hi[i]] with weights wt[i * wstride + (o - lo[i])].
 struct PassTables {
-    std::vector<int32_t> starts, lo, hi;
-    std::vector<uint8_t> phases;
-    std::vector<double> fold_lo, fold_hi;
+    std::vector<int32_t> lo, hi;
+    std::vector<double> wt;
+    int32_t wstride = 1;
 };
 
 PassTables pass_tables(const ReduceKernel& rk, int64_t out_origin, int64_t out_len, int64_t in_origin,
                        int64_t in_len, bool fold) {
-    PassTables t;
-    t.starts.resize(size_t(out_len));
-    t.phases.resize(size_t(out_len));
-    t.fold_lo.assign(size_t(out_len), 0.0);
-    t.fold_hi.assign(size_t(out_len), 0.0);
+    std::vector<int64_t> starts(size_t(out_len), 0);
+    std::vector<int32_t> phases(size_t(out_len), 0);
+    std::vector<double> fold_lo(size_t(out_len), 0.0), fold_hi(size_t(out_len), 0.0);
     for (int64_t o = 0; o < out_len; ++o) {
         int64_t s; int32_t ph;
         rk.plan(rk.source_position(double(out_origin + o)), &s, &ph);
-        t.starts[size_t(o)] = int32_t(s - in_origin);
-        t.phases[size_t(o)] = uint8_t(ph);
+        starts[size_t(o)] = s - in_origin;
+        phases[size_t(o)] = ph;
         const double* c = &rk.coeffs_f64[size_t(ph) * rk.taps];
         const int64_t rel = s - in_origin;
         if (fold) {
             for (int32_t k = 0; k < rk.taps; ++k) {
                 // a one-sample axis: every tap clamps onto it
-                if (rel + k <= 0 || in_len == 1) t.fold_lo[size_t(o)] += c[k];
-                else if (rel + k >= in_len - 1) t.fold_hi[size_t(o)] += c[k];
+                if (rel + k <= 0 || in_len == 1) fold_lo[size_t(o)] += c[k];
+                else if (rel + k >= in_len - 1) fold_hi[size_t(o)] += c[k];
             }
         }
     }
+    PassTables t;
     t.lo.assign(size_t(in_len), 0);
     t.hi.assign(size_t(in_len), -1);
     // outputs whose taps reach input index i (after the clamp when folding)
     for (int64_t o = 0; o < out_len; ++o) {
-        int64_t a = t.starts[size_t(o)], b = a + rk.taps - 1;
+        int64_t a = starts[size_t(o)], b = a + rk.taps - 1;
         if (fold) { a = std::max<int64_t>(a, 0); b = std::min<int64_t>(b, in_len - 1); a = std::min(a, in_len - 1); b = std::max<int64_t>(b, 0); }
         else { a = std::max<int64_t>(a, 0); b = std::min<int64_t>(b, in_len - 1); }
         for (int64_t i = a; i <= b; ++i) {
@@ -98,20 +101,101 @@ PassTables pass_tables(const ReduceKernel& rk, int64_t out_origin, int64_t out_l
             else { t.lo[size_t(i)] = std::min(t.lo[size_t(i)], int32_t(o)); t.hi[size_t(i)] = std::max(t.hi[size_t(i)], int32_t(o)); }
         }
     }
+    int32_t ws = 1;
+    for (int64_t i = 0; i < in_len; ++i) ws = std::max(ws, t.hi[size_t(i)] - t.lo[size_t(i)] + 1);
+    t.wstride = ws;
+    t.wt.assign(size_t(in_len) * size_t(ws), 0.0);
+    for (int64_t i = 0; i < in_len; ++i) {
+        for (int32_t o = t.lo[size_t(i)]; o <= t.hi[size_t(i)]; ++o) {
+            double w;
+            const int64_t k = i - starts[size_t(o)];
+            if (fold && (in_len == 1 || i == 0)) w = fold_lo[size_t(o)];
+            else if (fold && i == in_len - 1) w = fold_hi[size_t(o)];
+            else w = (k >= 0 && k < rk.taps) ? rk.coeffs_f64[size_t(phases[size_t(o)]) * rk.taps + size_t(k)] : 0.0;
+            t.wt[size_t(i) * size_t(ws) + size_t(o - t.lo[size_t(i)])] = w;
+        }
+    }
     return t;
 }
 
-int launch_pass(Scratch& sc, const ReduceKernel& rk, const PassTables& t, ReduceAdjArgs a, cudaStream_t s) {
-    cudaError_t e = cudaSuccess;
-    a.starts = sc.upload(t.starts, &e);
-    if (e == cudaSuccess) a.phases = sc.upload(t.phases, &e);
-    if (e == cudaSuccess) a.coeffs = sc.upload(rk.coeffs_f64, &e);
-    if (e == cudaSuccess) a.lo = sc.upload(t.lo, &e);
-    if (e == cudaSuccess) a.hi = sc.upload(t.hi, &e);
-    if (e == cudaSuccess) a.fold_lo = sc.upload(t.fold_lo, &e);
-    if (e == cudaSuccess) a.fold_hi = sc.upload(t.fold_hi, &e);
-    a.taps = rk.taps;
+// The tables of a pass packed in one buffer: lo, hi (int32, in_len each), then
+// the weights (f64, 8-byte aligned).
+std::vector<uint8_t> pack_tables(const PassTables& t, size_t* wt_off) {
+    const size_t n = t.lo.size();
+    *wt_off = (n * 8 + 7) / 8 * 8;
+    std::vector<uint8_t> buf(*wt_off + t.wt.size() * 8);
+    std::memcpy(buf.data(), t.lo.data(), n * 4);
+    std::memcpy(buf.data() + n * 4, t.hi.data(), n * 4);
+    std::memcpy(buf.data() + *wt_off, t.wt.data(), t.wt.size() * 8);
+    return buf;
+}
+
+// Device copies of pass tables, kept per device and geometry: a backward pass
+// over the same shapes (every training step) reuses them instead of uploading
+// again.  Entries are immutable and live until the process exits; past
+// kMaxCached entries a pass uploads its tables stream-ordered per call.
+struct TableKey {
+    int device;
+    int32_t kernel, fold;
+    uint64_t factor_bits;
+    int64_t bound, out_origin, out_len, in_origin, in_len;
+    bool operator<(const TableKey& o) const {
+        return std::tie(device, kernel, fold, factor_bits, bound, out_origin, out_len, in_origin, in_len) <
+               std::tie(o.device, o.kernel, o.fold, o.factor_bits, o.bound, o.out_origin, o.out_len, o.in_origin,
+                        o.in_len);
+    }
+};
+struct DevTables {
+    const uint8_t* data = nullptr;
+    size_t wt_off = 0;
+    int32_t wstride = 1;
+};
+constexpr size_t kMaxCached = 256;
+std::mutex g_table_mu;
+std::map<TableKey, DevTables> g_tables;
+
+int launch_pass(Scratch& sc, const ReduceKernel& rk, int32_t kernel, double factor, int64_t bound,
+                int64_t out_origin, int64_t out_len, int64_t in_origin, int64_t in_len, bool fold, ReduceAdjArgs a,
+                cudaStream_t s) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_status(e);
+    uint64_t fb;
+    std::memcpy(&fb, &factor, 8);
+    const TableKey key{dev, kernel, fold ? 1 : 0, fb, bound, out_origin, out_len, in_origin, in_len};
+    DevTables d;
+    {
+        std::lock_guard<std::mutex> lk(g_table_mu);
+        auto it = g_tables.find(key);
+        if (it != g_tables.end()) d = it->second;
+    }
+    if (!d.data) {
+        const PassTables t = pass_tables(rk, out_origin, out_len, in_origin, in_len, fold);
+        const std::vector<uint8_t> buf = pack_tables(t, &d.wt_off);
+        d.wstride = t.wstride;
+        std::lock_guard<std::mutex> lk(g_table_mu);
+        auto it = g_tables.find(key);
+        if (it != g_tables.end()) {
+            d = it->second;
+        } else if (g_tables.size() < kMaxCached) {
+            void* p = nullptr;
+            e = cudaMalloc(&p, buf.size());
+            if (e == cudaSuccess) e = cudaMemcpy(p, buf.data(), buf.size(), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) {
+                if (p) cudaFree(p);
+                return cuda_status(e);
+            }
+            d.data = static_cast<const uint8_t*>(p);
+            g_tables.emplace(key, d);
+        } else {
+            d.data = sc.upload(buf, &e);
+            if (e != cudaSuccess) return cuda_status(e);
+        }
+    }
+    a.lo = reinterpret_cast<const int32_t*>(d.data);
+    a.hi = reinterpret_cast<const int32_t*>(d.data + size_t(in_len) * 4);
+    a.wt = reinterpret_cast<const double*>(d.data + d.wt_off);
+    a.wstride = d.wstride;
     return cuda_status(launch::reduce_adjoint(a, s));
 }
 
@@ -138,7 +222,6 @@ int32_t viprs_reduce_adjoint(const viprs_image* grad_out, const viprs_image* gra
         return VIPRS_ERR_SIZE_MISMATCH;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     Scratch sc(s);
-    const PassTables t = pass_tables(rk, 0, n_out, 0, n_in, true);
     ReduceAdjArgs a;
     a.g_out = static_cast<const float*>(grad_out->data);
     a.g_in = static_cast<float*>(grad_in->data);
@@ -146,7 +229,7 @@ int32_t viprs_reduce_adjoint(const viprs_image* grad_out, const viprs_image* gra
     a.out_w = int32_t(grad_out->width); a.out_h = int32_t(grad_out->height);
     a.in_w = int32_t(grad_in->width); a.in_h = int32_t(grad_in->height);
     a.bands = int32_t(grad_in->bands);
-    return launch_pass(sc, rk, t, a, s);
+    return launch_pass(sc, rk, kernel, factor, n_in, 0, n_out, 0, n_in, true, a, s);
 }
 
 int32_t viprs_reduce_hv_adjoint(const viprs_image* grad_out, const viprs_image* grad_in, double hfactor,
@@ -178,7 +261,6 @@ int32_t viprs_reduce_hv_adjoint(const viprs_image* grad_out, const viprs_image* 
     float* g_mid = sc.alloc<float>(size_t(mh) * OW * B, &e);
     if (e != cudaSuccess) return cuda_status(e);
     // V^T: no clamp inside the mid plane (it covers every tap)
-    const PassTables tv = pass_tables(rv, 0, OH, my0, mh, false);
     ReduceAdjArgs av;
     av.g_out = static_cast<const float*>(grad_out->data);
     av.g_in = g_mid;
@@ -186,10 +268,9 @@ int32_t viprs_reduce_hv_adjoint(const viprs_image* grad_out, const viprs_image* 
     av.out_w = int32_t(OW); av.out_h = int32_t(OH);
     av.in_w = int32_t(OW); av.in_h = int32_t(mh);
     av.bands = int32_t(B);
-    st = launch_pass(sc, rv, tv, av, s);
+    st = launch_pass(sc, rv, kernel, vfactor, H, 0, OH, my0, mh, false, av, s);
     if (st) return st;
     // H^T with the source clamp: edge columns fold, virtual mid rows fold onto edge rows
-    const PassTables th = pass_tables(rh, 0, OW, 0, W, true);
     ReduceAdjArgs ah;
     ah.g_out = g_mid;
     ah.g_in = static_cast<float*>(grad_in->data);
@@ -199,7 +280,7 @@ int32_t viprs_reduce_hv_adjoint(const viprs_image* grad_out, const viprs_image* 
     ah.bands = int32_t(B);
     ah.fold_rows = 1;
     ah.mid_y0 = int32_t(my0);
-    return launch_pass(sc, rh, th, ah, s);
+    return launch_pass(sc, rh, kernel, hfactor, W, 0, OW, 0, W, true, ah, s);
 }
 
 int32_t viprs_affine_grad(const viprs_image* in, const viprs_image* grad_out, const viprs_image* grad_in,
@@ -247,8 +328,7 @@ int32_t viprs_affine_grad(const viprs_image* in, const viprs_image* grad_out, co
     g.fwd.out.w = int32_t(grad_out->width); g.fwd.out.h = int32_t(grad_out->height);
     g.fwd.out.pitch = int64_t(grad_out->width) * grad_out->bands * 4;
     g.g_out = static_cast<const float*>(grad_out->data);
-    const int64_t npx = int64_t(grad_out->width) * grad_out->height;
-    const int blocks = int((npx + 255) / 256);
+    const int blocks = launch::affine_grad_blocks(int32_t(grad_out->width), int32_t(grad_out->height));
     const int64_t n_in = int64_t(in->width) * in->height * in->bands;
     if (grad_in) {
         if (deterministic) {

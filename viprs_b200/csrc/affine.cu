@@ -26,7 +26,9 @@ cudaError_t affine(const AffineArgs& a, cudaStream_t s) {
     const int64_t npx = (int64_t)a.out.w * a.out.h;
     if (npx <= 0) return cudaSuccess;
     if (a.bands > 8) return cudaErrorInvalidValue;
-    const unsigned grid = (unsigned)((npx + 255) / 256);
+    const bool walk = a.fast == 0 && !(a.separable && a.xs != nullptr);
+    const int64_t threads = walk ? ((int64_t)(a.out.w + dev::kAffineGroup - 1) / dev::kAffineGroup) * a.out.h : npx;
+    const unsigned grid = (unsigned)((threads + 255) / 256);
     switch (a.fmt) {
     case kU8: dev::affine_kernel<uint8_t><<<grid, 256, 0, s>>>(a); break;
     case kU16: dev::affine_kernel<uint16_t><<<grid, 256, 0, s>>>(a); break;
@@ -38,11 +40,21 @@ cudaError_t affine(const AffineArgs& a, cudaStream_t s) {
 cudaError_t mapim(const MapimArgs& a, cudaStream_t s) {
     const int64_t npx = (int64_t)a.out.w * a.out.h;
     if (npx <= 0) return cudaSuccess;
-    const unsigned grid = (unsigned)((npx + 255) / 256);
-    switch (a.fmt) {
-    case kU8: dev::mapim_kernel<uint8_t><<<grid, 256, 0, s>>>(a); break;
-    case kU16: dev::mapim_kernel<uint16_t><<<grid, 256, 0, s>>>(a); break;
-    default: dev::mapim_kernel<float><<<grid, 256, 0, s>>>(a); break;
+    const dim3 grid((unsigned)((a.out.w + 255) / 256), (unsigned)std::min<int64_t>(a.out.h, 65535));
+    // the kernels index a source row with 32-bit element offsets
+    if ((int64_t)a.src_w * a.bands >= ((int64_t)1 << 31)) return cudaErrorInvalidValue;
+    const int nt = (a.kernel == 0 || a.kernel == 1) ? 0 : (a.kernel == 9 ? 6 : 4);
+    switch (a.fmt * 8 + nt) {
+    case kU8 * 8 + 0: dev::mapim_kernel<uint8_t, 0><<<grid, 256, 0, s>>>(a); break;
+    case kU8 * 8 + 4: dev::mapim_kernel<uint8_t, 4><<<grid, 256, 0, s>>>(a); break;
+    case kU8 * 8 + 6: dev::mapim_kernel<uint8_t, 6><<<grid, 256, 0, s>>>(a); break;
+    case kU16 * 8 + 0: dev::mapim_kernel<uint16_t, 0><<<grid, 256, 0, s>>>(a); break;
+    case kU16 * 8 + 4: dev::mapim_kernel<uint16_t, 4><<<grid, 256, 0, s>>>(a); break;
+    case kU16 * 8 + 6: dev::mapim_kernel<uint16_t, 6><<<grid, 256, 0, s>>>(a); break;
+    case kF32 * 8 + 0: dev::mapim_kernel<float, 0><<<grid, 256, 0, s>>>(a); break;
+    case kF32 * 8 + 4: dev::mapim_kernel<float, 4><<<grid, 256, 0, s>>>(a); break;
+    case kF32 * 8 + 6: dev::mapim_kernel<float, 6><<<grid, 256, 0, s>>>(a); break;
+    default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }

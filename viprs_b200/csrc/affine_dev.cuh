@@ -112,12 +112,21 @@ struct AffineCtx {
         default: return false;
         }
     }
+    // Tap (ix, iy) resolved against the source bounds (extend) and the tile's
+    // input region: its in-plane address (always readable) and whether it
+    // reads the image (false: the fill value).
+    __device__ __forceinline__ const T* tap(int64_t ix, int64_t iy, bool* ok) const {
+        int64_t rx = 0, ry = 0;
+        const bool okx = resolve(ix, a.src_w, &rx);
+        const bool oky = resolve(iy, a.src_h, &ry);
+        *ok = okx && oky && rx >= rx0 && rx <= rx1 && ry >= ry0 && ry <= ry1;
+        return sample_ptr<T>(a.in, rx - a.in.x0, ry - a.in.y0, a.bands);
+    }
     // Affine::sample_band: extend against the source bounds, read the plane
     __device__ double sb(int64_t ix, int64_t iy, int band) const {
-        int64_t rx, ry;
-        if (!resolve(ix, a.src_w, &rx) || !resolve(iy, a.src_h, &ry)) return fill();
-        if (rx < rx0 || rx > rx1 || ry < ry0 || ry > ry1) return fill();
-        return (double)load_sample<T>(a.in, rx - a.in.x0, ry - a.in.y0, a.bands, band);
+        bool ok;
+        const double v = (double)tap(ix, iy, &ok)[band];
+        return ok ? v : fill();
     }
     __device__ double sbp(int64_t ix, int64_t iy, int band, int ab, double amax) const {
         const double v = sb(ix, iy, band);
@@ -146,29 +155,103 @@ struct AffineCtx {
             const double bottom = fma(p11, fx, p10 * (1.0 - fx));
             return top * (1.0 - fy) + bottom * fy;
         }
-        const int64_t support = k == 9 ? 3 : 2;
+        // taps cx - (support - 1) .. cx + support per axis, each axis's
+        // weights evaluated once, taps with a zero weight skipped
+        const int support = k == 9 ? 3 : 2;
+        const int nt = 2 * support;
         const int64_t cx = trunc_i64(floor(x)), cy = trunc_i64(floor(y));
+        const int64_t tx0 = cx - (support - 1), ty0 = cy - (support - 1);
+        double wxs[6], wys[6];
+#pragma unroll
+        for (int t = 0; t < 6; ++t) {
+            wxs[t] = t < nt ? kernel_w(k, fabs((double)(tx0 + t) - x)) : 0.0;
+            wys[t] = t < nt ? kernel_w(k, fabs((double)(ty0 + t) - y)) : 0.0;
+        }
         double acc = 0.0, wsum = 0.0;
-        for (int64_t ky = -(support - 1); ky <= support; ++ky) {
-            const int64_t iy = cy + ky;
-            const double wy = kernel_w(k, fabs((double)iy - y));
-            if (wy != 0.0) {
-                for (int64_t kx = -(support - 1); kx <= support; ++kx) {
-                    const int64_t ix = cx + kx;
-                    const double wx = kernel_w(k, fabs((double)ix - x));
-                    if (wx != 0.0) {
-                        const double w = wx * wy;
-                        wsum += w;
-                        acc = fma(pm ? sbp(ix, iy, band, ab, amax) : sb(ix, iy, band), w, acc);
-                    }
+        for (int j = 0; j < nt; ++j) {
+            const double wy = wys[j];
+            if (wy == 0.0) continue;
+            const int64_t iy = ty0 + j;
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+                if (i >= nt) break;
+                const double s = pm ? sbp(tx0 + i, iy, band, ab, amax) : sb(tx0 + i, iy, band);
+                const double wx = wxs[i];
+                if (wx != 0.0) {
+                    const double w = wx * wy;
+                    wsum += w;
+                    acc = fma(s, w, acc);
                 }
             }
         }
         return wsum > 0.0 ? acc / wsum : fill();
     }
+    // Bilinear taps (x0 + dx, y0 + dy), dx, dy in {0, 1}, every band of a tap
+    // read once: v[k][b] = sb(x0 + (k & 1), y0 + (k >> 1), b) for k = 0..3.
+    template <int NB>
+    __device__ void taps4(int64_t x0, int64_t y0, double (&v)[4][NB]) const {
+        const double f = fill();
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            bool ok;
+            const T* px = tap(x0 + (k & 1), y0 + (k >> 1), &ok);
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                const double s = (double)px[b];
+                v[k][b] = ok ? s : f;
+            }
+        }
+    }
+    __device__ static double bil4(double p00, double p01, double p10, double p11, double fx, double fy) {
+        const double top = fma(p01, fx, p00 * (1.0 - fx));
+        const double bottom = fma(p11, fx, p10 * (1.0 - fx));
+        return top * (1.0 - fy) + bottom * fy;
+    }
+    // pixel() for the bilinear kernel with NB == a.bands: the same arithmetic
+    // per band as sample() / sbp(), with each tap read once.
+    template <int NB>
+    __device__ void pixel_bilinear(double x, double y, double* out) const {
+        if (!isfinite(x) || !isfinite(y)) {
+#pragma unroll
+            for (int b = 0; b < NB; ++b) out[b] = fill();
+            return;
+        }
+        const int64_t x0 = trunc_i64(x), y0 = trunc_i64(y);
+        const double fx = x - (double)x0, fy = y - (double)y0;
+        double v[4][NB];
+        taps4<NB>(x0, y0, v);
+        if (NB == 4 && !a.premultiplied) {
+            constexpr int ab = NB - 1;
+            const double amax = sizeof(T) == 4 ? 1.0 : (sizeof(T) == 2 ? 65535.0 : 255.0);
+            double alpha = bil4(v[0][ab], v[1][ab], v[2][ab], v[3][ab], fx, fy);
+            alpha = alpha < 0.0 ? 0.0 : (alpha > amax ? amax : alpha);
+            const double na = alpha / amax;
+            double s[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) s[k] = v[k][ab] / amax;
+#pragma unroll
+            for (int b = 0; b < ab; ++b) {
+                const double p = bil4(v[0][b] * s[0], v[1][b] * s[1], v[2][b] * s[2], v[3][b] * s[3], fx, fy);
+                out[b] = na > 0.0 ? p / na : 0.0;
+            }
+            out[ab] = alpha;
+            return;
+        }
+#pragma unroll
+        for (int b = 0; b < NB; ++b) out[b] = bil4(v[0][b], v[1][b], v[2][b], v[3][b], fx, fy);
+    }
     // Affine::sample_pixel_at into out[0..bands)
     __device__ void pixel(double x, double y, double* out) const {
         const int bands = a.bands;
+        if (a.kernel == 1) {
+            switch (bands) {
+            case 1: pixel_bilinear<1>(x, y, out); return;
+            case 2: pixel_bilinear<2>(x, y, out); return;
+            case 3: pixel_bilinear<3>(x, y, out); return;
+            case 4: pixel_bilinear<4>(x, y, out); return;
+            default: break;
+            }
+        }
         if (bands == 4 && !a.premultiplied) {
             if (!isfinite(x) || !isfinite(y)) {
                 for (int b = 0; b < bands; ++b) out[b] = fill();
@@ -213,6 +296,21 @@ __device__ __forceinline__ T store_round(double v, bool u8_round_first) {
         return (T)(uint32_t)r;
     }
     return from_f64<T>(v);
+}
+
+// Output pixel (lx, ly) from its sampled values: round, unpremultiply (u8), store.
+template <typename T>
+__device__ __forceinline__ void affine_store(const AffineArgs& a, int64_t lx, int64_t ly, const double* v,
+                                             bool u8_round_first) {
+    const int bands = a.bands;
+    T* dst = reinterpret_cast<T*>(a.out.data + ly * a.out.pitch) + lx * bands;
+    T o[8];
+    for (int b = 0; b < bands; ++b) o[b] = store_round<T>(v[b], u8_round_first);
+    if (sizeof(T) == 1 && a.unpremul_out && bands >= 2) {
+        const uint32_t al = (uint32_t)o[bands - 1];
+        for (int b = 0; b < bands - 1; ++b) o[b] = (T)unpremultiply_u8((uint32_t)o[b], al);
+    }
+    for (int b = 0; b < bands; ++b) dst[b] = o[b];
 }
 
 // One output pixel (lx, ly) of the plane a.out.
@@ -306,18 +404,74 @@ __device__ void affine_pixel(const AffineArgs& a, int64_t lx, int64_t ly) {
         }
         c.pixel(x_in, y_in, v);
     }
-    T* dst = reinterpret_cast<T*>(a.out.data + ly * a.out.pitch) + lx * bands;
-    T o[8];
-    for (int b = 0; b < bands; ++b) o[b] = store_round<T>(v[b], u8_round_first);
-    if (sizeof(T) == 1 && a.unpremul_out && bands >= 2) {
-        const uint32_t al = (uint32_t)o[bands - 1];
-        for (int b = 0; b < bands - 1; ++b) o[b] = (T)unpremultiply_u8((uint32_t)o[b], al);
+    affine_store<T>(a, lx, ly, v, u8_round_first);
+}
+
+// General incremental walk for kAffineGroup consecutive output pixels of one
+// row: viprs's position of pixel X is the tile row's start plus m0 added
+// (X - X0) times, so a thread walking along its pixels adds m0 once per pixel
+// and restarts only where a new scheduler tile begins.
+constexpr int kAffineGroup = 8;
+
+// Walk state of one thread along its output row: the current scheduler tile
+// (its origin and whether the pixel lies inside the tile grid, which decide
+// the tile's input region) and the walked position.
+struct AffineWalk {
+    int64_t X0 = INT64_MIN;
+    int grid = -1;
+    double x = 0.0, y = 0.0;
+    // Position of pixel (X, Y), X advancing by one from the previous call (or
+    // any X on the first call); refreshes c's tile region when the tile changes.
+    template <typename T>
+    __device__ __forceinline__ void step(const AffineArgs& a, AffineCtx<T>& c, int64_t X, int64_t Y) {
+        const double* m = a.m;
+        const int64_t tX0 = tile_origin(X, a.tile_off_x, a.tile_w);
+        if (tX0 != X0) {
+            const int64_t Y0 = tile_origin(Y, a.tile_off_y, a.tile_h);
+            double rx = fma(m[1], (double)Y0, m[0] * (double)tX0) + a.tx;
+            double ry = fma(m[3], (double)Y0, m[2] * (double)tX0) + a.ty;
+            for (int64_t r = Y0; r < Y; ++r) { rx += m[1]; ry += m[3]; }
+            x = rx; y = ry;
+            for (int64_t q = tX0; q < X; ++q) { x += m[0]; y += m[2]; }
+        } else {
+            x += m[0];
+            y += m[2];
+        }
+        const int g = X >= a.tile_off_x && X < a.tile_off_x + (int64_t)a.final_w && Y >= a.tile_off_y &&
+                      Y < a.tile_off_y + (int64_t)a.final_h;
+        if (tX0 != X0 || g != grid) c.set_tile(X, Y);
+        X0 = tX0;
+        grid = g;
     }
-    for (int b = 0; b < bands; ++b) dst[b] = o[b];
+};
+
+template <typename T>
+__device__ void affine_walk_group(const AffineArgs& a, int64_t lx0, int64_t ly) {
+    const int64_t Y = a.out.y0 + ly;
+    AffineCtx<T> c(a);
+    AffineWalk w;
+    const int64_t lx1 = min((int64_t)a.out.w, lx0 + kAffineGroup);
+    for (int64_t lx = lx0; lx < lx1; ++lx) {
+        w.step<T>(a, c, a.out.x0 + lx, Y);
+        double v[8];
+        c.pixel(w.x, w.y, v);
+        affine_store<T>(a, lx, ly, v, false);
+    }
 }
 
 template <typename T>
 __global__ void __launch_bounds__(256) affine_kernel(AffineArgs a) {
+    const bool walk = a.fast == 0 && !(a.separable && a.xs != nullptr);
+    if (walk) {
+        // no fast path and no per-axis tables: every pixel, a downstream
+        // halo included, takes the incremental walk
+        const int64_t gw = (a.out.w + kAffineGroup - 1) / kAffineGroup;
+        const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        if (g >= gw * a.out.h) return;
+        const int64_t ly = g / gw, lx0 = (g - ly * gw) * kAffineGroup;
+        affine_walk_group<T>(a, lx0, ly);
+        return;
+    }
     const int64_t npx = (int64_t)a.out.w * a.out.h;
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= npx) return;
@@ -326,31 +480,35 @@ __global__ void __launch_bounds__(256) affine_kernel(AffineArgs a) {
 }
 
 // ---------------------------------------------------------------- mapim
+// Tap (ix, iy) of mapim's source read: its address (always readable) and
+// whether it reads the image (false: the background).
 template <typename T>
-__device__ __forceinline__ double mp_band(const MapimArgs& a, int64_t ix, int64_t iy, int band) {
-    int64_t x, y;
+__device__ __forceinline__ const T* mp_tap(const MapimArgs& a, int64_t ix, int64_t iy, bool* ok) {
     if (!a.extend_copy) {
-        if (ix < 0 || ix >= (int64_t)a.src_w || iy < 0 || iy >= (int64_t)a.src_h) return a.background;
-        x = ix; y = iy;
+        *ok = !(ix < 0 || ix >= (int64_t)a.src_w || iy < 0 || iy >= (int64_t)a.src_h);
     } else {
         int lp = 1, rp = 2;
         if (a.kernel == 0) { lp = 0; rp = 0; }
         else if (a.kernel == 1) { lp = 0; rp = 1; }
         else if (a.kernel == 9 || a.kernel == 4) { lp = 2; rp = 3; }
-        if (ix < -(int64_t)(lp + 1) || ix > (int64_t)a.src_w + rp || iy < -(int64_t)(lp + 1) || iy > (int64_t)a.src_h + rp)
-            return a.background;
-        x = clampi64(ix, 0, (int64_t)a.src_w - 1);
-        y = clampi64(iy, 0, (int64_t)a.src_h - 1);
+        *ok = !(ix < -(int64_t)(lp + 1) || ix > (int64_t)a.src_w + rp || iy < -(int64_t)(lp + 1) ||
+                iy > (int64_t)a.src_h + rp);
     }
-    return (double)load_sample<T>(a.src, x, y, a.bands, band);
+    const int64_t x = clampi64(ix, 0, (int64_t)a.src_w - 1), y = clampi64(iy, 0, (int64_t)a.src_h - 1);
+    return sample_ptr<T>(a.src, x, y, a.bands);
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) mapim_kernel(MapimArgs a) {
-    const int64_t npx = (int64_t)a.out.w * a.out.h;
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= npx) return;
-    const int64_t ly = p / a.out.w, lx = p - ly * a.out.w;
+__device__ __forceinline__ double mp_band(const MapimArgs& a, int64_t ix, int64_t iy, int band) {
+    bool ok;
+    const double v = (double)mp_tap<T>(a, ix, iy, &ok)[band];
+    return ok ? v : a.background;
+}
+
+// NT: taps per axis of the separable samplers (4: support 2, 6: Lanczos3);
+// 0 for the nearest / bilinear kernels.
+template <typename T, int NT>
+__device__ __forceinline__ void mapim_px(const MapimArgs& a, int64_t lx, int64_t ly) {
     const float2 idx = *reinterpret_cast<const float2*>(a.index.data + ly * a.index.pitch + lx * 8);
     const double rx = (double)idx.x, ry = (double)idx.y;
     const int bands = a.bands;
@@ -359,18 +517,27 @@ __global__ void __launch_bounds__(256) mapim_kernel(MapimArgs a) {
         for (int b = 0; b < bands; ++b) dst[b] = from_f64<T>(a.background);
         return;
     }
-    if (a.kernel == 0) {
-        const int64_t x0 = trunc_i64(floor(rx)), y0 = trunc_i64(floor(ry));
-        for (int b = 0; b < bands; ++b) dst[b] = from_f64<T>(mp_band<T>(a, x0, y0, b));
-        return;
-    }
-    if (a.kernel == 1) {
+    if (NT == 0) {
+        if (a.kernel == 0) {
+            const int64_t x0 = trunc_i64(floor(rx)), y0 = trunc_i64(floor(ry));
+            for (int b = 0; b < bands; ++b) dst[b] = from_f64<T>(mp_band<T>(a, x0, y0, b));
+            return;
+        }
         const int64_t x0 = trunc_i64(floor(rx)), y0 = trunc_i64(floor(ry));
         const double fx = rx - (double)x0, fy = ry - (double)y0;
         const bool interior = x0 >= 0 && x0 + 1 < (int64_t)a.src_w && y0 >= 0 && y0 + 1 < (int64_t)a.src_h;
+        bool ok[4];
+        const T* t[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) t[q] = mp_tap<T>(a, x0 + (q & 1), y0 + (q >> 1), &ok[q]);
         for (int b = 0; b < bands; ++b) {
-            const double p00 = mp_band<T>(a, x0, y0, b), p01 = mp_band<T>(a, x0 + 1, y0, b);
-            const double p10 = mp_band<T>(a, x0, y0 + 1, b), p11 = mp_band<T>(a, x0 + 1, y0 + 1, b);
+            double v[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const double s = (double)t[q][b];
+                v[q] = ok[q] ? s : a.background;
+            }
+            const double p00 = v[0], p01 = v[1], p10 = v[2], p11 = v[3];
             double top, bottom;
             if (interior) { top = fma(p01, fx, p00 * (1.0 - fx)); bottom = fma(p11, fx, p10 * (1.0 - fx)); }
             else { top = fma(p00, 1.0 - fx, p01 * fx); bottom = p10 * (1.0 - fx) + p11 * fx; }
@@ -378,32 +545,67 @@ __global__ void __launch_bounds__(256) mapim_kernel(MapimArgs a) {
         }
         return;
     }
-    // Affine sampler with Background(bg) over the source read region (mapim.rs:1178-1186, 1250-1271)
+    // Affine sampler with Background(bg) over the source read region
+    // (mapim.rs:1178-1186, 1250-1271): taps cx - (support - 1) .. cx + support
+    // per axis, weights evaluated once per axis, the weight sum (the same for
+    // every band) accumulated in the sampler's tap order.
+    constexpr int nt = NT > 0 ? NT : 1;
+    constexpr int support = nt / 2;
     const int k = a.kernel;
-    const int64_t support = k == 9 ? 3 : 2;
     const int64_t cx = trunc_i64(floor(rx)), cy = trunc_i64(floor(ry));
+    const int64_t tx0 = cx - (support - 1), ty0 = cy - (support - 1);
+    double wx[nt], wy[nt];
+#pragma unroll
+    for (int t = 0; t < nt; ++t) {
+        wx[t] = kernel_w(k, fabs((double)(tx0 + t) - rx));
+        wy[t] = kernel_w(k, fabs((double)(ty0 + t) - ry));
+    }
+    double wsum = 0.0;
+#pragma unroll
+    for (int j = 0; j < nt; ++j) {
+        if (wy[j] == 0.0) continue;
+#pragma unroll
+        for (int i = 0; i < nt; ++i)
+            if (wx[i] != 0.0) wsum += wx[i] * wy[j];
+    }
+    // per axis: in-bounds flags (background outside) and the clamped row
+    // pointers / column offsets, so that every tap loads from a readable address
+    bool okx[nt], oky[nt];
+    int32_t col[nt];
+    const T* rows[nt];
+#pragma unroll
+    for (int t = 0; t < nt; ++t) {
+        const int64_t ix = tx0 + t, iy = ty0 + t;
+        okx[t] = ix >= 0 && ix < (int64_t)a.src_w;
+        oky[t] = iy >= 0 && iy < (int64_t)a.src_h;
+        col[t] = (int32_t)clampi64(ix, 0, (int64_t)a.src_w - 1) * bands;
+        rows[t] = reinterpret_cast<const T*>(a.src.data + clampi64(iy, 0, (int64_t)a.src_h - 1) * a.src.pitch);
+    }
     for (int b = 0; b < bands; ++b) {
-        double acc = 0.0, wsum = 0.0;
-        for (int64_t ky = -(support - 1); ky <= support; ++ky) {
-            const int64_t iy = cy + ky;
-            const double wy = kernel_w(k, fabs((double)iy - ry));
-            if (wy != 0.0) {
-                for (int64_t kx = -(support - 1); kx <= support; ++kx) {
-                    const int64_t ix = cx + kx;
-                    const double wx = kernel_w(k, fabs((double)ix - rx));
-                    if (wx != 0.0) {
-                        const double w = wx * wy;
-                        wsum += w;
-                        double s = a.background;
-                        if (ix >= 0 && ix < (int64_t)a.src_w && iy >= 0 && iy < (int64_t)a.src_h)
-                            s = (double)load_sample<T>(a.src, ix, iy, bands, b);
-                        acc = fma(s, w, acc);
-                    }
-                }
+        double acc = 0.0;
+#pragma unroll
+        for (int j = 0; j < nt; ++j) {
+            double sv[nt];
+#pragma unroll
+            for (int i = 0; i < nt; ++i) sv[i] = (double)rows[j][col[i] + b];
+            if (wy[j] == 0.0) continue;
+#pragma unroll
+            for (int i = 0; i < nt; ++i) {
+                if (wx[i] == 0.0) continue;
+                const double s = okx[i] && oky[j] ? sv[i] : a.background;
+                acc = fma(s, wx[i] * wy[j], acc);
             }
         }
         dst[b] = from_f64<T>(wsum > 0.0 ? acc / wsum : a.background);
     }
+}
+
+// Threads along an output row, block rows over the output rows (grid-stride).
+template <typename T, int NT>
+__global__ void __launch_bounds__(256, 4) mapim_kernel(MapimArgs a) {
+    const int64_t lx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (lx >= a.out.w) return;
+    for (int64_t ly = blockIdx.y; ly < a.out.h; ly += gridDim.y) mapim_px<T, NT>(a, lx, ly);
 }
 
 }  // namespace dev

@@ -30,6 +30,22 @@ __device__ __forceinline__ T load_sample(const Plane& p, int64_t lx, int64_t ly,
     return row[lx * bands + b];
 }
 
+// Zeroed stand-in address for a tap of an empty plane.  The interpolators
+// load every tap of a pixel unconditionally, so that all of its loads are in
+// flight together, and select the fill value for taps outside the image
+// afterwards; a tap therefore always needs a readable address.
+__device__ __align__(16) static const unsigned char kNoSample[64] = {0};
+
+// Address of sample (lx, ly), band 0, of plane p with load_sample's clamp to
+// the plane; kNoSample for an empty plane.
+template <typename T>
+__device__ __forceinline__ const T* sample_ptr(const Plane& p, int64_t lx, int64_t ly, int bands) {
+    if (p.w <= 0 || p.h <= 0) return reinterpret_cast<const T*>(kNoSample);
+    lx = lx < 0 ? 0 : (lx >= p.w ? p.w - 1 : lx);
+    ly = ly < 0 ? 0 : (ly >= p.h ? p.h - 1 : ly);
+    return reinterpret_cast<const T*>(p.data + ly * p.pitch) + lx * bands;
+}
+
 __device__ __forceinline__ int64_t clampi64(int64_t v, int64_t lo, int64_t hi) {
     return v < lo ? lo : (v > hi ? hi : v);
 }
