@@ -26,7 +26,9 @@ namespace viprs {
 namespace dev {
 
 // One block row per input row (grid-stride over rows), threads over the row's
-// samples; 32-bit indexing (every plane holds fewer than 2^31 samples).
+// samples; 32-bit indexing (every plane holds fewer than 2^31 samples).  f32
+// weights and accumulation, as a backward pass computes: a sample gathers at
+// most a few dozen taps, so the rounding stays near f32 epsilon.
 __global__ void __launch_bounds__(256) reduce_adjoint_kernel(ReduceAdjArgs a) {
     const int32_t rowlen = a.in_w * a.bands;
     const int32_t t = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
@@ -47,18 +49,20 @@ __global__ void __launch_bounds__(256) reduce_adjoint_kernel(ReduceAdjArgs a) {
             r1 = r1 >= a.out_h ? a.out_h - 1 : r1;
         }
         const int32_t olo = a.lo[i], n = a.hi[i] - olo + 1;
-        const double* w = a.wt + (size_t)i * a.wstride;
-        double acc = 0.0;
+        const float* w = a.wt + (size_t)i * a.wstride;
+        float acc = 0.0f;
         if (a.horizontal) {
             for (int32_t r = r0; r <= r1; ++r) {
                 const float* g = a.g_out + (size_t)r * gstride + (size_t)olo * a.bands + b;
-                for (int32_t j = 0; j < n; ++j) acc = fma((double)g[j * a.bands], w[j], acc);
+#pragma unroll 4
+                for (int32_t j = 0; j < n; ++j) acc = fmaf(g[j * a.bands], w[j], acc);
             }
         } else {
             const float* g = a.g_out + (size_t)olo * gstride + t;
-            for (int32_t j = 0; j < n; ++j) acc = fma((double)g[(size_t)j * gstride], w[j], acc);
+#pragma unroll 4
+            for (int32_t j = 0; j < n; ++j) acc = fmaf(g[(size_t)j * gstride], w[j], acc);
         }
-        a.g_in[(size_t)iy * rowlen + t] = (float)acc;
+        a.g_in[(size_t)iy * rowlen + t] = acc;
     }
 }
 
@@ -67,9 +71,6 @@ __device__ __forceinline__ void scatter(float* g, unsigned long long* fx, double
     if (fx) atomicAdd(fx + idx, (unsigned long long)(long long)llrint(v * scale));
     else if (g) atomicAdd(g + idx, (float)v);
 }
-
-// Output pixels per thread of the affine gradient kernel.
-constexpr int kGradGroup = 8;
 
 // Bilinear forward of one band with derivative, from four samples.
 struct Bil {
@@ -172,35 +173,42 @@ __device__ __forceinline__ void affine_grad_px(const AffineGradArgs& g, const Af
     part[4] += dx; part[5] += dy;
 }
 
-// kGradGroup consecutive output pixels of one row per thread, positions by
-// the same walk as the forward kernel (AffineWalk), fixed per-thread order of
-// the matrix-gradient partial sums.
+// Threads over groups of a.group consecutive output pixels of a row, block
+// rows over the output rows (grid-stride); positions as the forward kernel
+// computes them (AffineRow's walk, the axis-aligned fast path or the per-axis
+// tables).  Each thread sums its pixels' matrix-gradient terms in a fixed
+// order, each block its threads' in a fixed tree.
 template <int NB>
-__global__ void __launch_bounds__(256) affine_grad_kernel(AffineGradArgs g) {
+__global__ void __launch_bounds__(256, 2) affine_grad_kernel(AffineGradArgs g) {
     const AffineArgs& a = g.fwd;
-    const int64_t gw = (a.out.w + kGradGroup - 1) / kGradGroup;
-    const int64_t gi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int G = a.group;
+    const int64_t lx0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * G;
     double part[6] = {0, 0, 0, 0, 0, 0};
-    if (gi < gw * a.out.h) {
-        const int64_t ly = gi / gw, lx0 = (gi - ly * gw) * kGradGroup;
-        const int64_t lx1 = min((int64_t)a.out.w, lx0 + kGradGroup);
-        const int64_t Y = a.out.y0 + ly;
+    if (lx0 < a.out.w) {
+        const int64_t lx1 = min((int64_t)a.out.w, lx0 + G);
         const double* m = a.m;
-        AffineCtx<float> c(a);
-        AffineWalk walk;
-        for (int64_t lx = lx0; lx < lx1; ++lx) {
-            const int64_t X = a.out.x0 + lx;
-            walk.step<float>(a, c, X, Y);
-            double x_in = walk.x, y_in = walk.y;
-            if (a.fast == 2 && X >= 0 && X < (int64_t)a.total_w && Y >= 0 && Y < (int64_t)a.total_h) {
-                x_in = fma(m[0], (double)X, a.tx);
-                y_in = fma(m[3], (double)Y, a.ty);
-            } else if (a.separable && a.xs != nullptr) {
-                x_in = a.xs[X];
-                y_in = a.ys[Y];
+        for (int64_t ly = blockIdx.y; ly < a.out.h; ly += gridDim.y) {
+            const int64_t Y = a.out.y0 + ly;
+            AffineCtx<float> c(a);
+            AffineRow row;
+            for (int64_t lx = lx0; lx < lx1; ++lx) {
+                const int64_t X = a.out.x0 + lx;
+                row.tile<float>(a, c, X, Y);
+                double x_in, y_in;
+                if (a.fast == 2 && X >= 0 && X < (int64_t)a.total_w && Y >= 0 && Y < (int64_t)a.total_h) {
+                    x_in = fma(m[0], (double)X, a.tx);
+                    y_in = fma(m[3], (double)Y, a.ty);
+                } else if (a.separable && a.xs != nullptr) {
+                    x_in = a.xs[X];
+                    y_in = a.ys[Y];
+                } else {
+                    row.walk(a, X, Y);
+                    x_in = row.x;
+                    y_in = row.y;
+                }
+                const float* gy = g.g_out + (ly * a.out.w + lx) * a.bands;
+                affine_grad_px<NB>(g, c, x_in, y_in, X, Y, gy, part);
             }
-            const float* gy = g.g_out + (ly * a.out.w + lx) * a.bands;
-            affine_grad_px<NB>(g, c, x_in, y_in, X, Y, gy, part);
         }
     }
     if (g.partial) {
@@ -214,7 +222,7 @@ __global__ void __launch_bounds__(256) affine_grad_kernel(AffineGradArgs g) {
         if (threadIdx.x < 6) {
             double s = 0.0;
             for (int w8 = 0; w8 < (int)(blockDim.x >> 5); ++w8) s += red[threadIdx.x][w8];
-            g.partial[(int64_t)blockIdx.x * 6 + threadIdx.x] = s;
+            g.partial[((int64_t)blockIdx.y * gridDim.x + blockIdx.x) * 6 + threadIdx.x] = s;
         }
     }
 }
@@ -239,6 +247,55 @@ __device__ __forceinline__ double kernel_dw(int k, double i_minus_x) {
             // d/dt [L sin(pi t) sin(pi t / L) / (pi t)^2]
             const double f = L * sin(p) * sin(p / L), df = L * pi * (cos(p) * sin(p / L) + sin(p) * cos(p / L) / L);
             dk = (df * p * p - f * 2.0 * pi * p) / (p * p * p * p);
+        }
+    }
+    return dk * s;
+}
+
+// f32 forms of the separable kernels and their derivatives (the mapim
+// gradient evaluates its weights in f32; sinpif / cospif give sin(pi t)).
+__device__ __forceinline__ float kernel_wf(int k, float x) {
+    x = fabsf(x);
+    switch (k) {
+    case 0: return x < 0.5f ? 1.0f : 0.0f;
+    case 1: return x < 1.0f ? 1.0f - x : 0.0f;
+    case 2: case 5: case 7:
+        if (x < 1.0f) return fmaf(2.5f * x, -x, 1.5f * x * x * x) + 1.0f;
+        if (x < 2.0f) return fmaf(4.0f, -x, fmaf(2.5f * x, x, -0.5f * x * x * x)) + 2.0f;
+        return 0.0f;
+    case 3:
+        if (x < 0.5f) return fmaf(2.0f * x, -x, 1.0f);
+        if (x < 1.5f) return fmaf(2.5f, -x, x * x) + 1.5f;
+        return 0.0f;
+    case 8: case 9: {
+        const float L = k == 9 ? 3.0f : 2.0f;
+        if (x < 1e-6f) return 1.0f;
+        if (x < L) return L * sinpif(x) * sinpif(x / L) / (9.8696044f * x * x);
+        return 0.0f;
+    }
+    default: return 0.0f;
+    }
+}
+
+__device__ __forceinline__ float kernel_dwf(int k, float i_minus_x) {
+    const float t = fabsf(i_minus_x);
+    const float s = i_minus_x > 0.0f ? -1.0f : (i_minus_x < 0.0f ? 1.0f : 0.0f);  // d|i-x|/dx
+    float dk = 0.0f;
+    if (k == 2 || k == 5 || k == 7) {
+        if (t < 1.0f) dk = 4.5f * t * t - 5.0f * t;
+        else if (t < 2.0f) dk = -1.5f * t * t + 5.0f * t - 4.0f;
+    } else if (k == 3) {
+        if (t < 0.5f) dk = -4.0f * t;
+        else if (t < 1.5f) dk = 2.0f * t - 2.5f;
+    } else if (k == 1) {
+        if (t < 1.0f) dk = -1.0f;
+    } else if (k == 8 || k == 9) {
+        const float L = k == 9 ? 3.0f : 2.0f;
+        if (t > 0.0f && t < L) {
+            const float pi = 3.14159265f, p = pi * t;
+            const float sa = sinpif(t), sb = sinpif(t / L);
+            const float f = L * sa * sb, df = L * pi * (cospif(t) * sb + sa * cospif(t / L) / L);
+            dk = df / (p * p) - f * 2.0f * pi / (p * p * p);
         }
     }
     return dk * s;
@@ -271,6 +328,16 @@ struct MapimSink {
             scatter(g->g_src, g->g_fixed, g->fixed_scale, gi, v);
         }
     }
+    // f32 contribution (fixed_scale is a power of two: the scaled value is exact)
+    __device__ __forceinline__ void add_at(int32_t li, int64_t gi, float v) const {
+        if (g->g_fixed) {
+            const unsigned long long q = (unsigned long long)llrintf(v * (float)g->fixed_scale);
+            if (local) atomicAdd(su + li, q);
+            else atomicAdd(g->g_fixed + gi, q);
+        } else {
+            atomicAdd(local ? sf + li : g->g_src + gi, v);
+        }
+    }
     __device__ __forceinline__ void add(int64_t rx, int64_t ry, int b, double v) const {
         add_at(((int32_t)(ry - by0) * bw + (int32_t)(rx - bx0)) * bands + b, ry * pitch_f + rx * bands + b, v);
     }
@@ -279,7 +346,7 @@ struct MapimSink {
 // NT: taps per axis of the separable samplers (4: support 2, 6: Lanczos3);
 // 0 for the nearest / bilinear kernels.
 template <int NT>
-__global__ void __launch_bounds__(256, 4) mapim_grad_kernel(MapimGradArgs g) {
+__global__ void __launch_bounds__(256, 3) mapim_grad_kernel(MapimGradArgs g) {
     extern __shared__ __align__(16) unsigned char mg_smem[];
     __shared__ int32_t box[4];  // min x, max x, min y, max y of the block's taps
     const MapimArgs& a = g.fwd;
@@ -301,7 +368,7 @@ __global__ void __launch_bounds__(256, 4) mapim_grad_kernel(MapimGradArgs g) {
     int64_t tx0 = 0, tx1 = -1, ty0 = 0, ty1 = -1;
     const int64_t W = a.src_w, H = a.src_h;
     if (valid && want_img) {
-        if (k == 0 || k == 1) {
+        if (NT == 0) {
             const int64_t x0 = trunc_i64(floor(x)), y0 = trunc_i64(floor(y)), d = k;
             tx0 = x0; tx1 = x0 + d; ty0 = y0; ty1 = y0 + d;
             if (a.extend_copy) {
@@ -349,7 +416,7 @@ __global__ void __launch_bounds__(256, 4) mapim_grad_kernel(MapimGradArgs g) {
     double gx = 0.0, gyy = 0.0;
     if (valid) {
         auto inb = [&](int64_t ix, int64_t iy) { return ix >= 0 && ix < W && iy >= 0 && iy < H; };
-        if (k == 0) {
+        if (NT == 0 && k == 0) {
             const int64_t ix = trunc_i64(floor(x)), iy = trunc_i64(floor(y));
             int64_t rx = ix, ry = iy;
             bool ok = inb(ix, iy);
@@ -360,7 +427,7 @@ __global__ void __launch_bounds__(256, 4) mapim_grad_kernel(MapimGradArgs g) {
             }
             if (ok && want_img)
                 for (int b = 0; b < bands; ++b) sink.add(rx, ry, b, gy[b]);
-        } else if (k == 1) {
+        } else if (NT == 0 && k == 1) {
             const int64_t x0 = trunc_i64(floor(x)), y0 = trunc_i64(floor(y));
             const double fx = x - (double)x0, fy = y - (double)y0;
             const double w[4] = {(1.0 - fx) * (1.0 - fy), fx * (1.0 - fy), (1.0 - fx) * fy, fx * fy};
@@ -392,65 +459,69 @@ __global__ void __launch_bounds__(256, 4) mapim_grad_kernel(MapimGradArgs g) {
             }
         } else if (NT > 0) {
             // separable sampler y = N / W with N = sum_ij wx_i wy_j s_ij and
-            // W = (sum_i wx_i)(sum_j wy_j); taps whose weight and derivative
-            // are both zero are skipped, as the forward skips zero weights
+            // W = (sum_i wx_i)(sum_j wy_j), evaluated in f32; taps whose weight
+            // and derivative are both zero are skipped, as the forward skips
+            // zero weights
             constexpr int64_t support = NT / 2;
             constexpr int nt = NT > 0 ? NT : 1;
-            const int64_t cx = trunc_i64(floor(x)), cy = trunc_i64(floor(y));
+            const float xf = (float)x, yf = (float)y;  // the f32 coordinates themselves
+            const int64_t cx = (int64_t)floorf(xf), cy = (int64_t)floorf(yf);
             const int64_t tx0 = cx - (support - 1), ty0 = cy - (support - 1);
-            double wx[nt], dwx[nt], wy[nt], dwy[nt];
+            float wx[nt], dwx[nt], wy[nt], dwy[nt];
             bool okx[nt];
             int32_t col[nt], lcol[nt];
-            double Sx = 0.0, Sdx = 0.0, Sy = 0.0, Sdy = 0.0;
+            float Sx = 0.0f, Sdx = 0.0f, Sy = 0.0f, Sdy = 0.0f;
 #pragma unroll
             for (int t = 0; t < nt; ++t) {
                 const int64_t ix = tx0 + t, iy = ty0 + t;
-                wx[t] = kernel_w(k, fabs((double)ix - x));
-                dwx[t] = kernel_dw(k, (double)ix - x);
-                wy[t] = kernel_w(k, fabs((double)iy - y));
-                dwy[t] = kernel_dw(k, (double)iy - y);
+                const float ex = (float)ix - xf, ey = (float)iy - yf;
+                wx[t] = kernel_wf(k, ex);
+                dwx[t] = kernel_dwf(k, ex);
+                wy[t] = kernel_wf(k, ey);
+                dwy[t] = kernel_dwf(k, ey);
                 Sx += wx[t]; Sdx += dwx[t]; Sy += wy[t]; Sdy += dwy[t];
                 okx[t] = ix >= 0 && ix < W;
                 col[t] = (int32_t)clampi64(ix, 0, W - 1) * bands;
                 lcol[t] = (int32_t)(ix - sink.bx0) * bands;
             }
-            const double Wt = Sx * Sy, Wx = Sdx * Sy, Wy = Sx * Sdy;
-            if (Wt > 0.0) {
-                const double inv = 1.0 / Wt;
+            const float Wt = Sx * Sy, Wx = Sdx * Sy, Wy = Sx * Sdy;
+            if (Wt > 0.0f) {
+                const float inv = 1.0f / Wt;
+                const float bg = (float)a.background;
                 for (int b = 0; b < bands; ++b) {
-                    double Nv = 0.0, Nx = 0.0, Ny = 0.0;
-                    const double gb = (double)gy[b];
+                    float Nv = 0.0f, Nx = 0.0f, Ny = 0.0f;
+                    const float gb = gy[b];
 #pragma unroll 1
                     for (int ty = 0; ty < nt; ++ty) {
-                        if (wy[ty] == 0.0 && dwy[ty] == 0.0) continue;
+                        if (wy[ty] == 0.0f && dwy[ty] == 0.0f) continue;
                         const int64_t iy = ty0 + ty;
                         const bool oky = iy >= 0 && iy < H;
                         const int64_t grow = clampi64(iy, 0, H - 1) * pitch_f + b;
                         // the row's taps load unconditionally (clamped addresses)
-                        double sv[nt];
+                        float sv[nt];
 #pragma unroll
-                        for (int tx = 0; tx < nt; ++tx) sv[tx] = (double)src[grow + col[tx]];
-                        double rv = 0.0, rd = 0.0;
+                        for (int tx = 0; tx < nt; ++tx) sv[tx] = src[grow + col[tx]];
+                        float rv = 0.0f, rd = 0.0f;
 #pragma unroll
                         for (int tx = 0; tx < nt; ++tx) {
-                            if (wx[tx] == 0.0 && dwx[tx] == 0.0) continue;
-                            const double s = okx[tx] && oky ? sv[tx] : a.background;
-                            rv += wx[tx] * s;
-                            rd += dwx[tx] * s;
+                            if (wx[tx] == 0.0f && dwx[tx] == 0.0f) continue;
+                            const float sval = okx[tx] && oky ? sv[tx] : bg;
+                            rv = fmaf(wx[tx], sval, rv);
+                            rd = fmaf(dwx[tx], sval, rd);
                         }
-                        Nv += wy[ty] * rv;
-                        Nx += wy[ty] * rd;
-                        Ny += dwy[ty] * rv;
-                        if (want_img && oky && wy[ty] != 0.0) {
-                            const double c = gb * inv * wy[ty];
+                        Nv = fmaf(wy[ty], rv, Nv);
+                        Nx = fmaf(wy[ty], rd, Nx);
+                        Ny = fmaf(dwy[ty], rv, Ny);
+                        if (want_img && oky && wy[ty] != 0.0f) {
+                            const float c = gb * inv * wy[ty];
                             const int32_t lrow = (int32_t)(iy - sink.by0) * sink.bw * bands + b;
 #pragma unroll
                             for (int tx = 0; tx < nt; ++tx)
-                                if (okx[tx] && wx[tx] != 0.0) sink.add_at(lrow + lcol[tx], grow + col[tx], c * wx[tx]);
+                                if (okx[tx] && wx[tx] != 0.0f) sink.add_at(lrow + lcol[tx], grow + col[tx], c * wx[tx]);
                         }
                     }
-                    gx += gb * (Nx * Wt - Nv * Wx) / (Wt * Wt);
-                    gyy += gb * (Ny * Wt - Nv * Wy) / (Wt * Wt);
+                    gx += (double)(gb * (Nx * Wt - Nv * Wx) * inv * inv);
+                    gyy += (double)(gb * (Ny * Wt - Nv * Wy) * inv * inv);
                 }
             }
         }
@@ -506,19 +577,28 @@ cudaError_t reduce_adjoint(const ReduceAdjArgs& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+static dim3 affine_grad_grid(int32_t out_w, int32_t out_h, int group) {
+    const int64_t gx = ((int64_t)out_w + group - 1) / group;
+    return dim3((unsigned)((gx + 255) / 256), (unsigned)std::min<int32_t>(out_h, 65535));
+}
+
 int affine_grad_blocks(int32_t out_w, int32_t out_h) {
-    const int64_t groups = ((int64_t)out_w + dev::kGradGroup - 1) / dev::kGradGroup * out_h;
-    return (int)((groups + 255) / 256);
+    const dim3 g = affine_grad_grid(out_w, out_h, affine_group((int64_t)out_w * out_h));
+    return (int)(g.x * g.y);
 }
 
 cudaError_t affine_grad(const AffineGradArgs& a, int blocks, cudaStream_t s) {
     if (blocks <= 0) return cudaSuccess;
     if (a.fwd.bands > 8) return cudaErrorInvalidValue;
+    AffineGradArgs k = a;
+    k.fwd.group = affine_group((int64_t)a.fwd.out.w * a.fwd.out.h);
+    const dim3 grid = affine_grad_grid(a.fwd.out.w, a.fwd.out.h, k.fwd.group);
+    if ((int)(grid.x * grid.y) != blocks) return cudaErrorInvalidValue;
     switch (a.fwd.bands) {
-    case 1: dev::affine_grad_kernel<1><<<blocks, 256, 0, s>>>(a); break;
-    case 3: dev::affine_grad_kernel<3><<<blocks, 256, 0, s>>>(a); break;
-    case 4: dev::affine_grad_kernel<4><<<blocks, 256, 0, s>>>(a); break;
-    default: dev::affine_grad_kernel<0><<<blocks, 256, 0, s>>>(a); break;
+    case 1: dev::affine_grad_kernel<1><<<grid, 256, 0, s>>>(k); break;
+    case 3: dev::affine_grad_kernel<3><<<grid, 256, 0, s>>>(k); break;
+    case 4: dev::affine_grad_kernel<4><<<grid, 256, 0, s>>>(k); break;
+    default: dev::affine_grad_kernel<0><<<grid, 256, 0, s>>>(k); break;
     }
     return cudaGetLastError();
 }

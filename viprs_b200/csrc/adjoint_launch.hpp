@@ -27,7 +27,7 @@ struct ReduceAdjArgs {
     int32_t bands = 1;
     const int32_t* lo = nullptr;   // per input index
     const int32_t* hi = nullptr;
-    const double* wt = nullptr;    // per input index, wstride weights
+    const float* wt = nullptr;     // per input index, wstride weights
     int32_t wstride = 1;
     // H pass of an H-then-V chain: input row r gathers mid row r - mid_y0, and
     // the edge rows also gather the virtual mid rows that the source read

@@ -119,14 +119,17 @@ PassTables pass_tables(const ReduceKernel& rk, int64_t out_origin, int64_t out_l
 }
 
 // The tables of a pass packed in one buffer: lo, hi (int32, in_len each), then
-// the weights (f64, 8-byte aligned).
+// the weights rounded to f32 (16-byte aligned).
 std::vector<uint8_t> pack_tables(const PassTables& t, size_t* wt_off) {
     const size_t n = t.lo.size();
-    *wt_off = (n * 8 + 7) / 8 * 8;
-    std::vector<uint8_t> buf(*wt_off + t.wt.size() * 8);
+    *wt_off = (n * 8 + 15) / 16 * 16;
+    std::vector<uint8_t> buf(*wt_off + t.wt.size() * 4);
     std::memcpy(buf.data(), t.lo.data(), n * 4);
     std::memcpy(buf.data() + n * 4, t.hi.data(), n * 4);
-    std::memcpy(buf.data() + *wt_off, t.wt.data(), t.wt.size() * 8);
+    for (size_t k = 0; k < t.wt.size(); ++k) {
+        const float w = float(t.wt[k]);
+        std::memcpy(buf.data() + *wt_off + k * 4, &w, 4);
+    }
     return buf;
 }
 
@@ -194,7 +197,7 @@ int launch_pass(Scratch& sc, const ReduceKernel& rk, int32_t kernel, double fact
     }
     a.lo = reinterpret_cast<const int32_t*>(d.data);
     a.hi = reinterpret_cast<const int32_t*>(d.data + size_t(in_len) * 4);
-    a.wt = reinterpret_cast<const double*>(d.data + d.wt_off);
+    a.wt = reinterpret_cast<const float*>(d.data + d.wt_off);
     a.wstride = d.wstride;
     return cuda_status(launch::reduce_adjoint(a, s));
 }

@@ -22,17 +22,25 @@
 namespace viprs {
 namespace launch {
 
+int affine_group(int64_t npx) {
+    // enough threads for a few waves of 2048 per SM on 148 SMs, then up to
+    // 8 pixels per thread (the walk and the tile region are shared along them)
+    const int64_t per = npx / (148ll * 2048 * 2);
+    return (int)std::max<int64_t>(1, std::min<int64_t>(8, per));
+}
+
 cudaError_t affine(const AffineArgs& a, cudaStream_t s) {
     const int64_t npx = (int64_t)a.out.w * a.out.h;
     if (npx <= 0) return cudaSuccess;
     if (a.bands > 8) return cudaErrorInvalidValue;
-    const bool walk = a.fast == 0 && !(a.separable && a.xs != nullptr);
-    const int64_t threads = walk ? ((int64_t)(a.out.w + dev::kAffineGroup - 1) / dev::kAffineGroup) * a.out.h : npx;
-    const unsigned grid = (unsigned)((threads + 255) / 256);
+    AffineArgs k = a;
+    k.group = affine_group(npx);
+    const int64_t gx = ((int64_t)a.out.w + k.group - 1) / k.group;
+    const dim3 grid((unsigned)((gx + 255) / 256), (unsigned)std::min<int64_t>(a.out.h, 65535));
     switch (a.fmt) {
-    case kU8: dev::affine_kernel<uint8_t><<<grid, 256, 0, s>>>(a); break;
-    case kU16: dev::affine_kernel<uint16_t><<<grid, 256, 0, s>>>(a); break;
-    default: dev::affine_kernel<float><<<grid, 256, 0, s>>>(a); break;
+    case kU8: dev::affine_kernel<uint8_t><<<grid, 256, 0, s>>>(k); break;
+    case kU16: dev::affine_kernel<uint16_t><<<grid, 256, 0, s>>>(k); break;
+    default: dev::affine_kernel<float><<<grid, 256, 0, s>>>(k); break;
     }
     return cudaGetLastError();
 }

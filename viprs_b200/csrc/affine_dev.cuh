@@ -51,6 +51,8 @@ __device__ __forceinline__ double kernel_w(int k, double x) {
 
 __device__ __forceinline__ int64_t tile_origin(int64_t v, int64_t off, int64_t t) {
     const int64_t d = v - off;
+    if (d >= 0 && d <= 0x7fffffff && t <= 0x7fffffff)  // 32-bit division covers real images
+        return off + (int64_t)((uint32_t)d / (uint32_t)t) * t;
     const int64_t q = d >= 0 ? d / t : -((-d + t - 1) / t);
     return off + q * t;
 }
@@ -313,13 +315,54 @@ __device__ __forceinline__ void affine_store(const AffineArgs& a, int64_t lx, in
     for (int b = 0; b < bands; ++b) dst[b] = o[b];
 }
 
-// One output pixel (lx, ly) of the plane a.out.
+// State of one thread walking along an output row: the scheduler tile it is
+// in (origin, and whether the pixel lies inside the tile grid -- together they
+// decide the tile's input region, refreshed only when they change) and the
+// incremental position walk.  viprs's position of pixel X of row Y is the
+// tile row's start (the tile origin's position plus m1 / m3 added Y - Y0
+// times) plus m0 / m2 added X - X0 times, so consecutive pixels of one tile
+// add one step each and the walk restarts only where a tile begins.
+struct AffineRow {
+    int64_t tX0 = INT64_MIN;
+    int grid = -1;
+    int64_t wX = INT64_MIN, wX0 = INT64_MIN;  // last walked pixel and its tile
+    double x = 0.0, y = 0.0;
+
+    template <typename T>
+    __device__ __forceinline__ void tile(const AffineArgs& a, AffineCtx<T>& c, int64_t X, int64_t Y) {
+        const int64_t X0 = tile_origin(X, a.tile_off_x, a.tile_w);
+        const int g = X >= a.tile_off_x && X < a.tile_off_x + (int64_t)a.final_w && Y >= a.tile_off_y &&
+                      Y < a.tile_off_y + (int64_t)a.final_h;
+        if (X0 != tX0 || g != grid) c.set_tile(X, Y);
+        tX0 = X0;
+        grid = g;
+    }
+    // position of (X, Y) by the walk; tile() has been called for X
+    __device__ __forceinline__ void walk(const AffineArgs& a, int64_t X, int64_t Y) {
+        const double* m = a.m;
+        if (wX0 == tX0 && X == wX + 1) {
+            x += m[0];
+            y += m[2];
+        } else {
+            const int64_t Y0 = tile_origin(Y, a.tile_off_y, a.tile_h);
+            double rx = fma(m[1], (double)Y0, m[0] * (double)tX0) + a.tx;
+            double ry = fma(m[3], (double)Y0, m[2] * (double)tX0) + a.ty;
+            for (int64_t r = Y0; r < Y; ++r) { rx += m[1]; ry += m[3]; }
+            x = rx; y = ry;
+            for (int64_t q = tX0; q < X; ++q) { x += m[0]; y += m[2]; }
+        }
+        wX = X;
+        wX0 = tX0;
+    }
+};
+
+// One output pixel (lx, ly) of the plane a.out; c and row carry the thread's
+// state along the row (pixels of one thread advance left to right).
 template <typename T>
-__device__ void affine_pixel(const AffineArgs& a, int64_t lx, int64_t ly) {
+__device__ void affine_pixel(const AffineArgs& a, AffineCtx<T>& c, AffineRow& row, int64_t lx, int64_t ly) {
     const int64_t X = a.out.x0 + lx, Y = a.out.y0 + ly;
     const int bands = a.bands;
-    AffineCtx<T> c(a);
-    c.set_tile(X, Y);
+    row.tile<T>(a, c, X, Y);
     double v[8];
     bool u8_round_first = false;
     const double* m = a.m;
@@ -395,89 +438,39 @@ __device__ void affine_pixel(const AffineArgs& a, int64_t lx, int64_t ly) {
             x_in = a.xs[X];
             y_in = a.ys[Y];
         } else {
-            const int64_t X0 = tile_origin(X, a.tile_off_x, a.tile_w), Y0 = tile_origin(Y, a.tile_off_y, a.tile_h);
-            double rx = fma(m[1], (double)Y0, m[0] * (double)X0) + a.tx;
-            double ry = fma(m[3], (double)Y0, m[2] * (double)X0) + a.ty;
-            for (int64_t r = Y0; r < Y; ++r) { rx += m[1]; ry += m[3]; }
-            x_in = rx; y_in = ry;
-            for (int64_t q = X0; q < X; ++q) { x_in += m[0]; y_in += m[2]; }
+            row.walk(a, X, Y);
+            x_in = row.x;
+            y_in = row.y;
         }
         c.pixel(x_in, y_in, v);
     }
     affine_store<T>(a, lx, ly, v, u8_round_first);
 }
 
-// General incremental walk for kAffineGroup consecutive output pixels of one
-// row: viprs's position of pixel X is the tile row's start plus m0 added
-// (X - X0) times, so a thread walking along its pixels adds m0 once per pixel
-// and restarts only where a new scheduler tile begins.
-constexpr int kAffineGroup = 8;
-
-// Walk state of one thread along its output row: the current scheduler tile
-// (its origin and whether the pixel lies inside the tile grid, which decide
-// the tile's input region) and the walked position.
-struct AffineWalk {
-    int64_t X0 = INT64_MIN;
-    int grid = -1;
-    double x = 0.0, y = 0.0;
-    // Position of pixel (X, Y), X advancing by one from the previous call (or
-    // any X on the first call); refreshes c's tile region when the tile changes.
-    template <typename T>
-    __device__ __forceinline__ void step(const AffineArgs& a, AffineCtx<T>& c, int64_t X, int64_t Y) {
-        const double* m = a.m;
-        const int64_t tX0 = tile_origin(X, a.tile_off_x, a.tile_w);
-        if (tX0 != X0) {
-            const int64_t Y0 = tile_origin(Y, a.tile_off_y, a.tile_h);
-            double rx = fma(m[1], (double)Y0, m[0] * (double)tX0) + a.tx;
-            double ry = fma(m[3], (double)Y0, m[2] * (double)tX0) + a.ty;
-            for (int64_t r = Y0; r < Y; ++r) { rx += m[1]; ry += m[3]; }
-            x = rx; y = ry;
-            for (int64_t q = tX0; q < X; ++q) { x += m[0]; y += m[2]; }
-        } else {
-            x += m[0];
-            y += m[2];
-        }
-        const int g = X >= a.tile_off_x && X < a.tile_off_x + (int64_t)a.final_w && Y >= a.tile_off_y &&
-                      Y < a.tile_off_y + (int64_t)a.final_h;
-        if (tX0 != X0 || g != grid) c.set_tile(X, Y);
-        X0 = tX0;
-        grid = g;
-    }
-};
-
+// One output pixel with fresh per-thread state (threads striding over a row).
 template <typename T>
-__device__ void affine_walk_group(const AffineArgs& a, int64_t lx0, int64_t ly) {
-    const int64_t Y = a.out.y0 + ly;
+__device__ void affine_pixel(const AffineArgs& a, int64_t lx, int64_t ly) {
     AffineCtx<T> c(a);
-    AffineWalk w;
-    const int64_t lx1 = min((int64_t)a.out.w, lx0 + kAffineGroup);
-    for (int64_t lx = lx0; lx < lx1; ++lx) {
-        w.step<T>(a, c, a.out.x0 + lx, Y);
-        double v[8];
-        c.pixel(w.x, w.y, v);
-        affine_store<T>(a, lx, ly, v, false);
-    }
+    AffineRow row;
+    affine_pixel<T>(a, c, row, lx, ly);
 }
 
+// Threads over groups of a.group consecutive pixels of a row, block rows over
+// the output rows (grid-stride): a thread's pixels share the tile region and
+// the incremental walk.
 template <typename T>
 __global__ void __launch_bounds__(256) affine_kernel(AffineArgs a) {
-    const bool walk = a.fast == 0 && !(a.separable && a.xs != nullptr);
-    if (walk) {
-        // no fast path and no per-axis tables: every pixel, a downstream
-        // halo included, takes the incremental walk
-        const int64_t gw = (a.out.w + kAffineGroup - 1) / kAffineGroup;
-        const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-        if (g >= gw * a.out.h) return;
-        const int64_t ly = g / gw, lx0 = (g - ly * gw) * kAffineGroup;
-        affine_walk_group<T>(a, lx0, ly);
-        return;
+    const int G = a.group;
+    const int64_t lx0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * G;
+    if (lx0 >= a.out.w) return;
+    const int64_t lx1 = min((int64_t)a.out.w, lx0 + G);
+    for (int64_t ly = blockIdx.y; ly < a.out.h; ly += gridDim.y) {
+        AffineCtx<T> c(a);
+        AffineRow row;
+        for (int64_t lx = lx0; lx < lx1; ++lx) affine_pixel<T>(a, c, row, lx, ly);
     }
-    const int64_t npx = (int64_t)a.out.w * a.out.h;
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= npx) return;
-    const int64_t ly = p / a.out.w, lx = p - ly * a.out.w;
-    affine_pixel<T>(a, lx, ly);
 }
+
 
 // ---------------------------------------------------------------- mapim
 // Tap (ix, iy) of mapim's source read: its address (always readable) and

@@ -32,6 +32,7 @@ struct AffineArgs {
     const double* xs = nullptr;  // per output column x_in (separable general path)
     const double* ys = nullptr;  // per output row y_in
     int32_t unpremul_out = 0;
+    int32_t group = 1;       // consecutive output pixels per thread (set by the launcher)
 };
 
 // MapImOp (resample/mapim.rs).
@@ -48,6 +49,8 @@ struct MapimArgs {
 };
 
 namespace launch {
+// output pixels per thread of the affine kernels for an npx-pixel output
+int affine_group(int64_t npx);
 cudaError_t affine(const AffineArgs& a, cudaStream_t s);
 cudaError_t mapim(const MapimArgs& a, cudaStream_t s);
 }  // namespace launch
