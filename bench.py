@@ -2,6 +2,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--no-cpu] [--no-others] [--cpu-seconds S]
+                    [--images N] [--only NAME]
 
 Headline workload (the metric "input Mpix/s batched vs per-image GPU (bit-exact
 u8); fwd+bwd GB/s vs HBM"): thumbnails of 512 u8 images of uneven size (width
@@ -49,6 +50,12 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 FALLBACK_HBM_GBS = 6650.0
+# DRAM bytes (read + write) of one batch step over its algorithmic bytes, from
+# the ncu capture of both persistent launches on the first 64 images
+# (profiles/batch_kernel_thumbnail64.md: 1.1922 GB / 1,156,046,596 B); every
+# image adds its input once and its shrunk intermediate once, so the ratio
+# carries over to the 512-image step
+BATCH_TRAFFIC_RATIO = 1.1922e9 / 1156046596
 METRIC = "input Mpix/s batched vs per-image GPU (bit-exact u8); fwd+bwd GB/s vs HBM"
 BATCH_N = 512
 BATCH_SEED = 0x5EED0003
@@ -178,6 +185,40 @@ def timed(fn, steps, warmup, stream):
     return statistics.mean(a.elapsed_time(b) for a, b in evs)
 
 
+def graph_timed(fn, steps):
+    """Mean CUDA-event ms of one replay of fn() captured in a CUDA graph: the
+    device time of its launches without the host's gaps between them.  fn must
+    read the current stream at call time.  Returns (ms, None) or (None, why)
+    when fn does not capture."""
+    import torch
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        fn()  # tables cached, allocations settled before the capture
+    torch.cuda.current_stream().wait_stream(side)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    try:
+        with torch.cuda.graph(g):
+            fn()
+    except Exception as e:  # reported, never hidden
+        torch.cuda.synchronize()
+        return None, f"{type(e).__name__}: {e}"[:200]
+    for _ in range(3):
+        g.replay()
+    torch.cuda.synchronize()
+    cur = torch.cuda.current_stream()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for a, b in evs:
+        a.record(cur)
+        g.replay()
+        b.record(cur)
+    torch.cuda.synchronize()
+    ms = statistics.mean(a.elapsed_time(b) for a, b in evs)
+    del g
+    return ms, None
+
+
 # ----------------------------------------------------------------------------- headline: batched thumbnails
 
 def make_batch_images(seed, n=BATCH_N, device="cuda"):
@@ -297,7 +338,9 @@ def run_batch(args, rank, ws, local):
         "e2e": {"value": round(e2e_value, 2), "unit": "Mpix/s", "h2d_bytes_per_step": in_bytes,
                 "d2h_bytes_per_step": out_bytes, "path": "ThumbnailBatch.run_host (pinned host buffers)"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
+                     "frac": round(achieved / peak, 4), "traffic": round(alg * BATCH_TRAFFIC_RATIO),
+                     "traffic_source": "ncu capture of the first 64 images, scaled by algorithmic bytes",
+                     "peak_kind": peak_kind,
                      "kernel": "batch_kernel", "kernel_ms": round(kernel_ms, 4), "algorithmic_bytes": alg},
         "clocks": clocks,
         "parity": "batched == per-image path (bit-exact)" if same else "MISMATCH",
@@ -321,14 +364,23 @@ def other_thumbnail_8192(stream, steps):
     out = torch.empty(plan.out_shape, dtype=torch.uint8, device="cuda")
     total = timed(lambda: plan(img, out), steps, 3, stream)
     shrink = timed(lambda: plan.run_stages(img, out, 0, 1), steps, 3, stream)
+    g_total, why = graph_timed(lambda: plan(img, out), steps)
+    g_shrink, _ = graph_timed(lambda: plan.run_stages(img, out, 0, 1), steps)
     need = (W // 19) * 19
     sb = need * need * 3 + (W // 19) * (H // 19) * 3
     peak, _ = measured_hbm_peak()
-    return {"workload": "thumbnail 8192x8192x3 u8 -> 400 px (shrink 19 + Lanczos3 1.0779)",
-            "mpix_per_s": round(H * W / 1e6 / (total / 1e3), 1), "ms": round(total, 4), "launches": plan.launches,
-            "shrink_kernel": {"ms": round(shrink, 4), "algorithmic_bytes": sb,
-                              "gbs": round(sb / (shrink / 1e3) / 1e9, 1),
-                              "frac": round(sb / (shrink / 1e3) / 1e9 / peak, 4)}}
+    r = {"workload": "thumbnail 8192x8192x3 u8 -> 400 px (shrink 19 + Lanczos3 1.0779)",
+         "mpix_per_s": round(H * W / 1e6 / (total / 1e3), 1), "ms": round(total, 4), "launches": plan.launches,
+         "shrink_kernel": {"ms": round(shrink, 4), "algorithmic_bytes": sb,
+                           "gbs": round(sb / (shrink / 1e3) / 1e9, 1),
+                           "frac": round(sb / (shrink / 1e3) / 1e9 / peak, 4)}}
+    if g_total is not None:
+        r["graph"] = {"ms": round(g_total, 4), "mpix_per_s": round(H * W / 1e6 / (g_total / 1e3), 1),
+                      "shrink_ms": round(g_shrink, 4), "shrink_gbs": round(sb / (g_shrink / 1e3) / 1e9, 1),
+                      "shrink_frac": round(sb / (g_shrink / 1e3) / 1e9 / peak, 4)}
+    else:
+        r["graph"] = {"unavailable": why}
+    return r
 
 
 def other_reduce_1024(stream, steps):
@@ -339,10 +391,13 @@ def other_reduce_1024(stream, steps):
     plan = api.PipelineBuilder(1024, 768, 3, torch.uint8).reduce_h(4.0).reduce_v(4.0).build()
     out = torch.empty(plan.out_shape, dtype=torch.uint8, device="cuda")
     ms = timed(lambda: plan(img, out), steps, 3, stream)
+    gms, why = graph_timed(lambda: plan(img, out), steps)
     b = 1024 * 768 * 3 + 256 * 192 * 3
-    return {"workload": "reduce_h(4)+reduce_v(4) Lanczos3 1024x768x3 u8 (single launch, latency-bound)",
-            "mpix_per_s": round(0.786432 / (ms / 1e3), 1), "us": round(ms * 1e3, 2), "algorithmic_bytes": b,
-            "gbs": round(b / (ms / 1e3) / 1e9, 1)}
+    r = {"workload": "reduce_h(4)+reduce_v(4) Lanczos3 1024x768x3 u8 (single launch, latency-bound)",
+         "mpix_per_s": round(0.786432 / (ms / 1e3), 1), "us": round(ms * 1e3, 2), "algorithmic_bytes": b,
+         "gbs": round(b / (ms / 1e3) / 1e9, 1)}
+    r["graph"] = {"us": round(gms * 1e3, 2), "gbs": round(b / (gms / 1e3) / 1e9, 1)} if gms else {"unavailable": why}
+    return r
 
 
 def other_resize_f32(stream, steps):
@@ -390,9 +445,9 @@ def other_reduce_affine_grad(stream, steps):
         bm, btx, bty = api.forward_affine_to_backward(M, tx, ty)
         mats.append(((ctypes.c_double * 4)(*bm), btx, bty))
     L = N.lib()
-    sp = api._stream()
 
     def fwd():
+        sp = api._stream()
         for i in range(n):
             plan(xs[i], zs[i])
             m, btx, bty = mats[i]
@@ -400,6 +455,7 @@ def other_reduce_affine_grad(stream, steps):
                                                    0, 0, sp), "affine")
 
     def bwd():
+        sp = api._stream()
         for i in range(n):
             m, btx, bty = mats[i]
             N.check(L.viprs_affine_grad(api.image(zs[i]), api.image(gys[i]), api.image(gzs[i]), m, btx, bty, 1, 2,
@@ -409,13 +465,22 @@ def other_reduce_affine_grad(stream, steps):
 
     fwd_ms = timed(fwd, steps, 3, stream)
     bwd_ms = timed(bwd, steps, 3, stream)
+    g_fwd, why = graph_timed(fwd, steps)
+    g_bwd, why_b = graph_timed(bwd, steps)
     alg = 738197504
     peak, _ = measured_hbm_peak()
     gbs = alg / ((fwd_ms + bwd_ms) / 1e3) / 1e9
-    return {"workload": "16 x 1024^2x4 f32: reduce_h(2)+reduce_v(2) L3 -> affine(s R(theta), t) bilinear 512^2, "
-                        "fwd + bwd (image and matrix gradients, f32-atomic scatter)",
-            "fwd_ms": round(fwd_ms, 4), "bwd_ms": round(bwd_ms, 4), "algorithmic_bytes_fwd_bwd": alg,
-            "gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}
+    r = {"workload": "16 x 1024^2x4 f32: reduce_h(2)+reduce_v(2) L3 -> affine(s R(theta), t) bilinear 512^2, "
+                     "fwd + bwd (image and matrix gradients, f32-atomic scatter)",
+         "fwd_ms": round(fwd_ms, 4), "bwd_ms": round(bwd_ms, 4), "algorithmic_bytes_fwd_bwd": alg,
+         "gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}
+    if g_fwd is not None and g_bwd is not None:
+        gg = alg / ((g_fwd + g_bwd) / 1e3) / 1e9
+        r["graph"] = {"fwd_ms": round(g_fwd, 4), "bwd_ms": round(g_bwd, 4), "gbs": round(gg, 1),
+                      "frac": round(gg / peak, 4)}
+    else:
+        r["graph"] = {"unavailable": why or why_b}
+    return r
 
 
 def other_mapim_grad(stream, steps):
@@ -442,14 +507,13 @@ def other_mapim_grad(stream, steps):
     gs = torch.empty_like(src)
     gi = torch.empty_like(index)
     L = N.lib()
-    sp = api._stream()
 
     def fwd():
-        N.check(L.viprs_mapim(api.image(src), api.image(index), api.image(out), 2, 0, 0.0, 0, sp), "mapim")
+        N.check(L.viprs_mapim(api.image(src), api.image(index), api.image(out), 2, 0, 0.0, 0, api._stream()), "mapim")
 
     def bwd(det):
         N.check(L.viprs_mapim_grad(api.image(src), api.image(index), api.image(gy), api.image(gs), api.image(gi),
-                                   2, 0, 0.0, 0, det, sp), "mapim_grad")
+                                   2, 0, 0.0, 0, det, api._stream()), "mapim_grad")
 
     fwd_ms = timed(fwd, steps, 3, stream)
     bwd_ms = timed(lambda: bwd(0), steps, 3, stream)
@@ -464,13 +528,18 @@ def other_mapim_grad(stream, steps):
             "forward_only_gbs": round(268435456 / (fwd_ms / 1e3) / 1e9, 1)}
 
 
-def run_others(steps):
+OTHERS = (("thumbnail_8192", other_thumbnail_8192), ("reduce_1024x768", other_reduce_1024),
+          ("resize_f32_6000x4000", other_resize_f32), ("reduce_affine_fwd_bwd", other_reduce_affine_grad),
+          ("mapim_fwd_bwd", other_mapim_grad))
+
+
+def run_others(steps, only=None):
     import torch
     stream = torch.cuda.current_stream()
     out = {}
-    for name, fn in (("thumbnail_8192", other_thumbnail_8192), ("reduce_1024x768", other_reduce_1024),
-                     ("resize_f32_6000x4000", other_resize_f32), ("reduce_affine_fwd_bwd", other_reduce_affine_grad),
-                     ("mapim_fwd_bwd", other_mapim_grad)):
+    for name, fn in OTHERS:
+        if only is not None and name != only:
+            continue
         try:
             out[name] = fn(stream, steps)
         except Exception as e:  # reported, never hidden
@@ -529,6 +598,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--images", type=int, default=BATCH_N, help="first N images of the batch (profiling cases)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default kernel configuration")
+    ap.add_argument("--only", default=None, choices=[n for n, _ in OTHERS],
+                    help="run one of the other configurations alone, --steps timed steps (profiling cases)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     args.steps = max(args.steps, 1)
@@ -538,6 +609,11 @@ def main():
         line = run_reference(args, rank, ws)
         if line is not None:
             print(json.dumps(line), flush=True)
+        return
+    if args.only is not None:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps({"only": args.only, **run_others(args.steps, args.only)}), flush=True)
         return
     rank, ws, local = dist_setup()
     line = run_batch(args, rank, ws, local)
