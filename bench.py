@@ -51,10 +51,11 @@ if ROOT not in sys.path:
 
 FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (read + write) of one batch step over its algorithmic bytes, from
-# the ncu capture of both persistent launches on the first 64 images
-# (profiles/batch_kernel_thumbnail64.md: 1.1922 GB / 1,156,046,596 B); every
-# image adds its input once and its shrunk intermediate once, so the ratio
-# carries over to the 512-image step
+# an ncu capture of both persistent launches on the first 64 images
+# (`ncu --set full -k regex:batch_kernel -s 2 -c 2 python bench.py --images 64
+# --steps 2 --warmup 3 --no-cpu --no-others --no-autotune`: 1.1922 GB against
+# 1,156,046,596 B); every image adds its input once and its shrunk
+# intermediate once, so the ratio carries over to the 512-image step
 BATCH_TRAFFIC_RATIO = 1.1922e9 / 1156046596
 METRIC = "input Mpix/s batched vs per-image GPU (bit-exact u8); fwd+bwd GB/s vs HBM"
 BATCH_N = 512
