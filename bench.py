@@ -151,12 +151,17 @@ def barrier(ws):
         dist.barrier()
 
 
+def _rank_device():
+    import torch.distributed as dist
+    return "cuda" if dist.get_backend() == "nccl" else "cpu"
+
+
 def max_over_ranks(x, ws):
     if ws <= 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_rank_device())
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -166,7 +171,7 @@ def sum_over_ranks(x, ws):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_rank_device())
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 

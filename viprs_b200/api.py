@@ -368,6 +368,25 @@ class PipelineBuilder:
         return self.build()(src)
 
 
+def partition_batch(shapes, parts):
+    """Split a batch of (h, w, bands) images over `parts` GPUs by byte
+    weight: largest image first, each to the part with the fewest bytes so far
+    (ties to the lowest part).  Returns one ascending index list per part.
+    Every rank computes the same split from the same shapes, so no exchange
+    is needed: each GPU copies its own images in and its thumbnails out."""
+    if parts < 1:
+        raise ValueError("parts must be >= 1")
+    order = sorted(range(len(shapes)), key=lambda i: (-shapes[i][0] * shapes[i][1] * shapes[i][2], i))
+    load = [0] * parts
+    out = [[] for _ in range(parts)]
+    for i in order:
+        p = min(range(parts), key=lambda k: (load[k], k))
+        h, w, b = shapes[i]
+        load[p] += h * w * b
+        out[p].append(i)
+    return [sorted(o) for o in out]
+
+
 def sm_count():
     return torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
 
