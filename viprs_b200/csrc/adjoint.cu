@@ -25,16 +25,20 @@
 namespace viprs {
 namespace dev {
 
-// One block row per input row (grid-stride over rows), threads over the row's
-// samples; 32-bit indexing (every plane holds fewer than 2^31 samples).  f32
-// weights and accumulation, as a backward pass computes: a sample gathers at
-// most a few dozen taps, so the rounding stays near f32 epsilon.
+// NB bands of one input pixel per thread (NB == 0: a.bands at run time),
+// block rows over the input rows (grid-stride); 32-bit indexing (every plane
+// holds fewer than 2^31 samples).  Each tap's weight is read once for the
+// pixel's bands, 4-band pixels move as one 16-byte load.  f32 weights and
+// accumulation, as a backward pass computes: a sample gathers at most a few
+// dozen taps, so the rounding stays near f32 epsilon.
+template <int NB>
 __global__ void __launch_bounds__(256) reduce_adjoint_kernel(ReduceAdjArgs a) {
-    const int32_t rowlen = a.in_w * a.bands;
-    const int32_t t = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
-    if (t >= rowlen) return;
-    const int32_t ix = t / a.bands, b = t - ix * a.bands;
-    const int32_t gstride = a.out_w * a.bands;  // g_out row length
+    constexpr int NBm = NB > 0 ? NB : 1;
+    const int B = NB > 0 ? NB : a.bands;
+    const int32_t ix = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (ix >= a.in_w) return;
+    const int32_t gstride = a.out_w * B;  // g_out row length (samples)
+    const int32_t rowlen = a.in_w * B;
     for (int32_t iy = (int32_t)blockIdx.y; iy < a.in_h; iy += (int32_t)gridDim.y) {
         const int32_t i = a.horizontal ? ix : iy;  // index along the folded axis
         // rows of g_out this input row gathers (H pass: one row, or the
@@ -50,19 +54,54 @@ __global__ void __launch_bounds__(256) reduce_adjoint_kernel(ReduceAdjArgs a) {
         }
         const int32_t olo = a.lo[i], n = a.hi[i] - olo + 1;
         const float* w = a.wt + (size_t)i * a.wstride;
-        float acc = 0.0f;
-        if (a.horizontal) {
-            for (int32_t r = r0; r <= r1; ++r) {
-                const float* g = a.g_out + (size_t)r * gstride + (size_t)olo * a.bands + b;
+        float* dst = a.g_in + (size_t)iy * rowlen + (size_t)ix * B;
+        if constexpr (NB > 0) {
+            float acc[NBm];
+#pragma unroll
+            for (int b = 0; b < NBm; ++b) acc[b] = 0.0f;
+            // tap j of this pixel: g + j * step (H: the next output pixel of
+            // the row; V: the next output row, same column)
+            const size_t step = a.horizontal ? (size_t)NB : (size_t)gstride;
+            for (int32_t r = (a.horizontal ? r0 : 0); r <= (a.horizontal ? r1 : 0); ++r) {
+                const float* g = a.horizontal ? a.g_out + (size_t)r * gstride + (size_t)olo * NB
+                                              : a.g_out + (size_t)olo * gstride + (size_t)ix * NB;
 #pragma unroll 4
-                for (int32_t j = 0; j < n; ++j) acc = fmaf(g[j * a.bands], w[j], acc);
+                for (int32_t j = 0; j < n; ++j) {
+                    const float wj = w[j];
+                    const float* q = g + (size_t)j * step;
+                    if constexpr (NB == 4) {
+                        const float4 v = *reinterpret_cast<const float4*>(q);
+                        acc[0] = fmaf(v.x, wj, acc[0]);
+                        acc[1] = fmaf(v.y, wj, acc[1]);
+                        acc[2] = fmaf(v.z, wj, acc[2]);
+                        acc[3] = fmaf(v.w, wj, acc[3]);
+                    } else {
+#pragma unroll
+                        for (int b = 0; b < NBm; ++b) acc[b] = fmaf(q[b], wj, acc[b]);
+                    }
+                }
+            }
+            if constexpr (NB == 4) {
+                *reinterpret_cast<float4*>(dst) = make_float4(acc[0], acc[1], acc[2], acc[3]);
+            } else {
+#pragma unroll
+                for (int b = 0; b < NBm; ++b) dst[b] = acc[b];
             }
         } else {
-            const float* g = a.g_out + (size_t)olo * gstride + t;
-#pragma unroll 4
-            for (int32_t j = 0; j < n; ++j) acc = fmaf(g[(size_t)j * gstride], w[j], acc);
+            for (int b = 0; b < B; ++b) {
+                float acc = 0.0f;
+                if (a.horizontal) {
+                    for (int32_t r = r0; r <= r1; ++r) {
+                        const float* g = a.g_out + (size_t)r * gstride + (size_t)olo * B + b;
+                        for (int32_t j = 0; j < n; ++j) acc = fmaf(g[j * B], w[j], acc);
+                    }
+                } else {
+                    const float* g = a.g_out + (size_t)olo * gstride + (size_t)ix * B + b;
+                    for (int32_t j = 0; j < n; ++j) acc = fmaf(g[(size_t)j * gstride], w[j], acc);
+                }
+                dst[b] = acc;
+            }
         }
-        a.g_in[(size_t)iy * rowlen + t] = acc;
     }
 }
 
@@ -572,8 +611,18 @@ cudaError_t reduce_adjoint(const ReduceAdjArgs& a, cudaStream_t s) {
     if (rowlen <= 0 || a.in_h <= 0) return cudaSuccess;
     if (rowlen * a.in_h >= ((int64_t)1 << 31) || (int64_t)a.out_w * a.bands * a.out_h >= ((int64_t)1 << 31))
         return cudaErrorInvalidValue;
-    const dim3 grid((unsigned)((rowlen + 255) / 256), (unsigned)std::min<int64_t>(a.in_h, 65535));
-    dev::reduce_adjoint_kernel<<<grid, 256, 0, s>>>(a);
+    const dim3 grid((unsigned)((a.in_w + 255) / 256), (unsigned)std::min<int64_t>(a.in_h, 65535));
+    // 16-byte loads of 4-band pixels need 16-byte aligned planes
+    const bool al16 = (reinterpret_cast<uintptr_t>(a.g_out) & 15) == 0 && (reinterpret_cast<uintptr_t>(a.g_in) & 15) == 0;
+    switch (a.bands) {
+    case 1: dev::reduce_adjoint_kernel<1><<<grid, 256, 0, s>>>(a); break;
+    case 3: dev::reduce_adjoint_kernel<3><<<grid, 256, 0, s>>>(a); break;
+    case 4:
+        if (al16) dev::reduce_adjoint_kernel<4><<<grid, 256, 0, s>>>(a);
+        else dev::reduce_adjoint_kernel<0><<<grid, 256, 0, s>>>(a);
+        break;
+    default: dev::reduce_adjoint_kernel<0><<<grid, 256, 0, s>>>(a); break;
+    }
     return cudaGetLastError();
 }
 

@@ -22,6 +22,17 @@
 namespace viprs {
 namespace launch {
 
+// the band count as a template parameter for the common counts
+template <typename T>
+static void launch_affine(const AffineArgs& k, dim3 grid, cudaStream_t s) {
+    switch (k.bands) {
+    case 1: dev::affine_kernel<T, 1><<<grid, 256, 0, s>>>(k); break;
+    case 3: dev::affine_kernel<T, 3><<<grid, 256, 0, s>>>(k); break;
+    case 4: dev::affine_kernel<T, 4><<<grid, 256, 0, s>>>(k); break;
+    default: dev::affine_kernel<T, 0><<<grid, 256, 0, s>>>(k); break;
+    }
+}
+
 int affine_group(int64_t npx) {
     // enough threads for a few waves of 2048 per SM on 148 SMs, then up to
     // 8 pixels per thread (the walk and the tile region are shared along them)
@@ -38,9 +49,9 @@ cudaError_t affine(const AffineArgs& a, cudaStream_t s) {
     const int64_t gx = ((int64_t)a.out.w + k.group - 1) / k.group;
     const dim3 grid((unsigned)((gx + 255) / 256), (unsigned)std::min<int64_t>(a.out.h, 65535));
     switch (a.fmt) {
-    case kU8: dev::affine_kernel<uint8_t><<<grid, 256, 0, s>>>(k); break;
-    case kU16: dev::affine_kernel<uint16_t><<<grid, 256, 0, s>>>(k); break;
-    default: dev::affine_kernel<float><<<grid, 256, 0, s>>>(k); break;
+    case kU8: launch_affine<uint8_t>(k, grid, s); break;
+    case kU16: launch_affine<uint16_t>(k, grid, s); break;
+    default: launch_affine<float>(k, grid, s); break;
     }
     return cudaGetLastError();
 }

@@ -243,8 +243,15 @@ struct AffineCtx {
         for (int b = 0; b < NB; ++b) out[b] = bil4(v[0][b], v[1][b], v[2][b], v[3][b], fx, fy);
     }
     // Affine::sample_pixel_at into out[0..bands)
+    // NB: compile-time band count (0: a.bands at run time) -- with it the
+    // caller's per-band arrays stay in registers
+    template <int NB = 0>
     __device__ void pixel(double x, double y, double* out) const {
-        const int bands = a.bands;
+        const int bands = NB > 0 ? NB : a.bands;
+        if (NB > 0 && a.kernel == 1) {
+            pixel_bilinear<(NB > 0 ? NB : 1)>(x, y, out);
+            return;
+        }
         if (a.kernel == 1) {
             switch (bands) {
             case 1: pixel_bilinear<1>(x, y, out); return;
@@ -301,12 +308,12 @@ __device__ __forceinline__ T store_round(double v, bool u8_round_first) {
 }
 
 // Output pixel (lx, ly) from its sampled values: round, unpremultiply (u8), store.
-template <typename T>
+template <typename T, int NB = 0>
 __device__ __forceinline__ void affine_store(const AffineArgs& a, int64_t lx, int64_t ly, const double* v,
                                              bool u8_round_first) {
-    const int bands = a.bands;
+    const int bands = NB > 0 ? NB : a.bands;
     T* dst = reinterpret_cast<T*>(a.out.data + ly * a.out.pitch) + lx * bands;
-    T o[8];
+    T o[NB > 0 ? NB : 8];
     for (int b = 0; b < bands; ++b) o[b] = store_round<T>(v[b], u8_round_first);
     if (sizeof(T) == 1 && a.unpremul_out && bands >= 2) {
         const uint32_t al = (uint32_t)o[bands - 1];
@@ -358,12 +365,12 @@ struct AffineRow {
 
 // One output pixel (lx, ly) of the plane a.out; c and row carry the thread's
 // state along the row (pixels of one thread advance left to right).
-template <typename T>
+template <typename T, int NB = 0>
 __device__ void affine_pixel(const AffineArgs& a, AffineCtx<T>& c, AffineRow& row, int64_t lx, int64_t ly) {
     const int64_t X = a.out.x0 + lx, Y = a.out.y0 + ly;
-    const int bands = a.bands;
+    const int bands = NB > 0 ? NB : a.bands;
     row.tile<T>(a, c, X, Y);
-    double v[8];
+    double v[NB > 0 ? NB : 8];
     bool u8_round_first = false;
     const double* m = a.m;
     // fast paths and per-axis tables cover the affine's own output rectangle; a
@@ -406,7 +413,7 @@ __device__ void affine_pixel(const AffineArgs& a, AffineCtx<T>& c, AffineRow& ro
             if (sizeof(T) == 1) {
                 for (int b = 0; b < bands; ++b) v[b] = c.sample(cxr, cyr, b, false, 0, 1.0);
             } else {
-                c.pixel(cxr, cyr, v);
+                c.template pixel<NB>(cxr, cyr, v);
                 u8_round_first = false;
             }
         } else {
@@ -442,9 +449,9 @@ __device__ void affine_pixel(const AffineArgs& a, AffineCtx<T>& c, AffineRow& ro
             x_in = row.x;
             y_in = row.y;
         }
-        c.pixel(x_in, y_in, v);
+        c.template pixel<NB>(x_in, y_in, v);
     }
-    affine_store<T>(a, lx, ly, v, u8_round_first);
+    affine_store<T, NB>(a, lx, ly, v, u8_round_first);
 }
 
 // One output pixel with fresh per-thread state (threads striding over a row).
@@ -458,7 +465,7 @@ __device__ void affine_pixel(const AffineArgs& a, int64_t lx, int64_t ly) {
 // Threads over groups of a.group consecutive pixels of a row, block rows over
 // the output rows (grid-stride): a thread's pixels share the tile region and
 // the incremental walk.
-template <typename T>
+template <typename T, int NB>
 __global__ void __launch_bounds__(256) affine_kernel(AffineArgs a) {
     const int G = a.group;
     const int64_t lx0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * G;
@@ -467,7 +474,7 @@ __global__ void __launch_bounds__(256) affine_kernel(AffineArgs a) {
     for (int64_t ly = blockIdx.y; ly < a.out.h; ly += gridDim.y) {
         AffineCtx<T> c(a);
         AffineRow row;
-        for (int64_t lx = lx0; lx < lx1; ++lx) affine_pixel<T>(a, c, row, lx, ly);
+        for (int64_t lx = lx0; lx < lx1; ++lx) affine_pixel<T, NB>(a, c, row, lx, ly);
     }
 }
 
