@@ -111,21 +111,34 @@ __device__ __forceinline__ void scatter(float* g, unsigned long long* fx, double
     else if (g) atomicAdd(g + idx, (float)v);
 }
 
+// f32 contribution to the image gradient (fixed_scale is a power of two: the
+// scaled value is exact).
+__device__ __forceinline__ void scatter_f(float* g, unsigned long long* fx, double scale, int64_t idx, float v) {
+    if (fx) atomicAdd(fx + idx, (unsigned long long)llrintf(v * (float)scale));
+    else if (g) atomicAdd(g + idx, v);
+}
+
 // Bilinear forward of one band with derivative, from four samples.
+template <typename R>
 struct Bil {
-    double out, dfx, dfy;
+    R out, dfx, dfy;
 };
-__device__ __forceinline__ Bil bil(double p00, double p01, double p10, double p11, double fx, double fy) {
-    Bil r;
-    const double top = fma(p01, fx, p00 * (1.0 - fx)), bottom = fma(p11, fx, p10 * (1.0 - fx));
-    r.out = top * (1.0 - fy) + bottom * fy;
-    r.dfx = (1.0 - fy) * (p01 - p00) + fy * (p11 - p10);
+template <typename R>
+__device__ __forceinline__ Bil<R> bil(R p00, R p01, R p10, R p11, R fx, R fy) {
+    Bil<R> r;
+    const R one = R(1);
+    const R top = fma(p01, fx, p00 * (one - fx)), bottom = fma(p11, fx, p10 * (one - fx));
+    r.out = top * (one - fy) + bottom * fy;
+    r.dfx = (one - fy) * (p01 - p00) + fy * (p11 - p10);
     r.dfy = bottom - top;
     return r;
 }
 
 // Gradient contributions of one output pixel at position (x_in, y_in); NB
-// bands (NB == 0: a.bands, up to 8, read at run time).
+// bands (NB == 0: a.bands, up to 8, read at run time).  The position and the
+// matrix-gradient sums are f64; the per-pixel interpolation derivative is
+// f32 arithmetic (the samples and gradients are f32), as a backward pass
+// computes.
 template <int NB>
 __device__ __forceinline__ void affine_grad_px(const AffineGradArgs& g, const AffineCtx<float>& c, double x_in,
                                                double y_in, int64_t X, int64_t Y, const float* gy, double* part) {
@@ -134,60 +147,63 @@ __device__ __forceinline__ void affine_grad_px(const AffineGradArgs& g, const Af
     const int bands = NB > 0 ? NB : a.bands;
     if (!isfinite(x_in) || !isfinite(y_in)) return;
     const int64_t x0 = trunc_i64(x_in), y0 = trunc_i64(y_in);
-    const double fx = x_in - (double)x0, fy = y_in - (double)y0;
-    const double w[4] = {(1.0 - fx) * (1.0 - fy), fx * (1.0 - fy), (1.0 - fx) * fy, fx * fy};
-    // element offset of each tap's first band in the input plane (-1: the constant fill)
+    const float fx = (float)(x_in - (double)x0), fy = (float)(y_in - (double)y0);
+    const float w[4] = {(1.0f - fx) * (1.0f - fy), fx * (1.0f - fy), (1.0f - fx) * fy, fx * fy};
+    // element offset of each tap's first band in the input plane (-1: the
+    // constant fill); every tap loads from a readable address
     const float* src = reinterpret_cast<const float*>(a.in.data);
-    const int64_t pitch_f = a.in.pitch / 4;
     int64_t e[4];
-    double sv[4][NBmax];
-    const double fill = c.fill();
+    float sv[4][NBmax];
+    const float fill = (float)c.fill();
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        int64_t rx, ry;
-        const bool ok = c.resolve(x0 + (k & 1), a.src_w, &rx) && c.resolve(y0 + (k >> 1), a.src_h, &ry) &&
-                        rx >= c.rx0 && rx <= c.rx1 && ry >= c.ry0 && ry <= c.ry1;
-        e[k] = ok ? (ry - a.in.y0) * pitch_f + (rx - a.in.x0) * bands : -1;
+        bool ok;
+        const float* px = c.tap(x0 + (k & 1), y0 + (k >> 1), &ok);
+        e[k] = ok ? (int64_t)(px - src) : -1;
 #pragma unroll
-        for (int b = 0; b < NBmax; ++b)
-            if (b < bands) sv[k][b] = ok ? (double)src[e[k] + b] : fill;
+        for (int b = 0; b < NBmax; ++b) {
+            if (b >= bands) break;
+            const float v = px[b];
+            sv[k][b] = ok ? v : fill;
+        }
     }
-    double dx = 0.0, dy = 0.0;
+    float dx = 0.0f, dy = 0.0f;
     if (bands == 4 && !a.premultiplied) {
         // alpha-premultiplied sampler (affine/core.rs:988-1019), alpha_max = 1
-        double al[4], pm[3][4];
+        float al[4], pm[3][4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) al[k] = sv[k][3];
 #pragma unroll
         for (int b = 0; b < 3; ++b)
 #pragma unroll
             for (int k = 0; k < 4; ++k) pm[b][k] = sv[k][b] * al[k];
-        const Bil A = bil(al[0], al[1], al[2], al[3], fx, fy);
-        Bil P[3];
+        const Bil<float> A = bil<float>(al[0], al[1], al[2], al[3], fx, fy);
+        Bil<float> P[3];
 #pragma unroll
-        for (int b = 0; b < 3; ++b) P[b] = bil(pm[b][0], pm[b][1], pm[b][2], pm[b][3], fx, fy);
-        double dP[3] = {0, 0, 0}, dA = 0.0;
-        if (A.out > 0.0 && A.out < 1.0) {
+        for (int b = 0; b < 3; ++b) P[b] = bil<float>(pm[b][0], pm[b][1], pm[b][2], pm[b][3], fx, fy);
+        float dP[3] = {0, 0, 0}, dA = 0.0f;
+        if (A.out > 0.0f && A.out < 1.0f) {
+            const float inv = 1.0f / A.out;
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
-                dP[b] = (double)gy[b] / A.out;
-                dA -= (double)gy[b] * P[b].out / (A.out * A.out);
+                dP[b] = gy[b] * inv;
+                dA -= gy[b] * P[b].out * inv * inv;
             }
-            dA += (double)gy[3];
-        } else if (A.out >= 1.0) {
+            dA += gy[3];
+        } else if (A.out >= 1.0f) {
 #pragma unroll
-            for (int b = 0; b < 3; ++b) dP[b] = (double)gy[b];
+            for (int b = 0; b < 3; ++b) dP[b] = gy[b];
         }
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             if (e[k] < 0) continue;
-            double da = dA * w[k];
+            float da = dA * w[k];
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
-                scatter(g.g_in, g.g_fixed, g.fixed_scale, e[k] + b, dP[b] * w[k] * al[k]);
+                scatter_f(g.g_in, g.g_fixed, g.fixed_scale, e[k] + b, dP[b] * w[k] * al[k]);
                 da += dP[b] * w[k] * sv[k][b];
             }
-            scatter(g.g_in, g.g_fixed, g.fixed_scale, e[k] + 3, da);
+            scatter_f(g.g_in, g.g_fixed, g.fixed_scale, e[k] + 3, da);
         }
 #pragma unroll
         for (int b = 0; b < 3; ++b) { dx += dP[b] * P[b].dfx; dy += dP[b] * P[b].dfy; }
@@ -197,19 +213,19 @@ __device__ __forceinline__ void affine_grad_px(const AffineGradArgs& g, const Af
 #pragma unroll
         for (int b = 0; b < NBmax; ++b) {
             if (b >= bands) break;
-            const double gb = (double)gy[b];
-            const Bil v = bil(sv[0][b], sv[1][b], sv[2][b], sv[3][b], fx, fy);
+            const float gb = gy[b];
+            const Bil<float> v = bil<float>(sv[0][b], sv[1][b], sv[2][b], sv[3][b], fx, fy);
             dx += gb * v.dfx;
             dy += gb * v.dfy;
 #pragma unroll
             for (int k = 0; k < 4; ++k)
-                if (e[k] >= 0) scatter(g.g_in, g.g_fixed, g.fixed_scale, e[k] + b, gb * w[k]);
+                if (e[k] >= 0) scatter_f(g.g_in, g.g_fixed, g.fixed_scale, e[k] + b, gb * w[k]);
         }
     }
     // x_in = m0 X + m1 Y + tx, y_in = m2 X + m3 Y + ty
-    part[0] += dx * (double)X; part[1] += dx * (double)Y;
-    part[2] += dy * (double)X; part[3] += dy * (double)Y;
-    part[4] += dx; part[5] += dy;
+    part[0] += (double)dx * (double)X; part[1] += (double)dx * (double)Y;
+    part[2] += (double)dy * (double)X; part[3] += (double)dy * (double)Y;
+    part[4] += (double)dx; part[5] += (double)dy;
 }
 
 // Threads over groups of a.group consecutive output pixels of a row, block
@@ -492,7 +508,7 @@ __global__ void __launch_bounds__(256, 3) mapim_grad_kernel(MapimGradArgs g) {
                     sq[q] = okq[q] ? raw : a.background;
                     if (okq[q] && want_img) sink.add(rxq[q], ryq[q], b, (double)gy[b] * w[q]);
                 }
-                const Bil v = bil(sq[0], sq[1], sq[2], sq[3], fx, fy);
+                const Bil<double> v = bil<double>(sq[0], sq[1], sq[2], sq[3], fx, fy);
                 gx += (double)gy[b] * v.dfx;
                 gyy += (double)gy[b] * v.dfy;
             }
