@@ -293,8 +293,12 @@ int32_t viprs_reduce_noalloc(const viprs_image *in, const viprs_image *out, doub
    viprs's resample operators are forward only, so these have no reference
    counterpart; each is the exact transpose / derivative of the forward entry
    point named beside it, as this library evaluates it (same coefficient
-   tables, positions and extend rules).  Scratch is allocated stream-ordered on
-   `stream`.  Gradients are overwritten, not accumulated. */
+   tables, positions and extend rules; the per-pixel derivative arithmetic is
+   f32, positions and matrix sums f64).  Scratch is allocated stream-ordered on
+   `stream` from a memory pool the library keeps per device (its memory stays
+   mapped between calls).  The reduce adjoints keep each geometry's transposed
+   tables on the device after the first call for it, which uploads them with a
+   synchronous copy.  Gradients are overwritten, not accumulated. */
 
 /* Transpose of viprs_reduceh (horizontal != 0) / viprs_reducev on f32: for
    every input sample, a gather over the outputs whose taps read it; taps that
