@@ -1,7 +1,7 @@
 """Benchmark of the resample hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--no-cpu] [--no-others] [--cpu-seconds S]
+                    [--no-cpu] [--no-others]
                     [--images N] [--only NAME]
 
 Headline workload (the metric "input Mpix/s batched vs per-image GPU (bit-exact
@@ -25,19 +25,19 @@ copied in, the graph run, thumbnails copied out, every step.  `roofline` is the
 batch kernel's algorithmic bytes (each image's input read once + output written
 once) over its CUDA-event time per launch, against MEASURED_PEAKS.json.
 `cpu_baseline` is the oracle (the C restatement of viprs's CPU path) on all
-host cores over a bounded sample of the batch.  `others` holds the remaining
+host cores over the whole batch once; its thumbnails are compared byte for
+byte with the GPU batch's (`parity`).  `others` holds the remaining
 configurations: the 8192x8192x3 thumbnail, the 1024x768x3 reduce, the f32
 6000x4000x4 resize, and the fwd+bwd GB/s of the reduce+affine and mapim
 gradient workloads.
 
 `--impl reference` times the reference arm: viprs's CPU path as restated in C
-(viprs itself needs a Rust toolchain this image lacks), all host cores, on a
-bounded sample of the same batch per step.
+(viprs itself needs a Rust toolchain this image lacks), all host cores, the
+whole batch -- the same shapes and seeded generator as the GPU arm -- per step.
 """
 import argparse
 import ctypes
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -52,8 +52,8 @@ if ROOT not in sys.path:
 FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (read + write) of one batch step over its algorithmic bytes, from
 # an ncu capture of both persistent launches on the first 64 images
-# (`ncu --set full -k regex:batch_kernel -s 2 -c 2 python bench.py --images 64
-# --steps 2 --warmup 3 --no-cpu --no-others --no-autotune`: 1.1922 GB against
+# (`ncu --set full --clock-control none -k regex:batch_kernel -s 2 -c 2 python bench.py
+# --images 64 --steps 2 --warmup 3 --no-cpu --no-others --no-autotune`: 1.1922 GB against
 # 1,156,046,596 B); every image adds its input once and its shrunk
 # intermediate once, so the ratio carries over to the 512-image step
 BATCH_TRAFFIC_RATIO = 1.1922e9 / 1156046596
@@ -61,8 +61,16 @@ METRIC = "input Mpix/s batched vs per-image GPU (bit-exact u8); fwd+bwd GB/s vs 
 BATCH_N = 512
 BATCH_SEED = 0x5EED0003
 BATCH_BOX = 256
-WORKLOAD = (f"{BATCH_N} uneven u8 images (w log-U[256,6000], w/h U[0.5,2], 3|4 bands) -> "
-            f"thumbnail FitBox {BATCH_BOX}x{BATCH_BOX} Lanczos3, persistent launches per stage level via CUDA graph")
+WORKLOAD = f"{BATCH_N} uneven u8 images (w logU[256,6000], w/h U[0.5,2], 3|4 bands) -> thumbnail FitBox {BATCH_BOX} Lanczos3"
+
+
+def batch_config(shapes):
+    """The `config` of both arms: the workload and its exact size (identical
+    for the GPU arm and the reference arm, which process the same images)."""
+    return {"workload": WORKLOAD if len(shapes) == BATCH_N else f"first {len(shapes)} of: {WORKLOAD}",
+            "images": len(shapes), "seed": BATCH_SEED,
+            "input_mpix": round(sum(h * w for h, w, _ in shapes) / 1e6, 2),
+            "input_bytes": sum(h * w * b for h, w, b in shapes)}
 
 
 def measured_hbm_peak():
@@ -234,25 +242,34 @@ def make_batch_images(seed, n=BATCH_N, device="cuda"):
     return shapes, imgs
 
 
-def cpu_baseline_batch(host_imgs, seconds):
-    """The oracle (CPU restatement of viprs) on all host cores, image by image
-    over the batch in order, until `seconds` of work."""
+def cpu_batch_step(host_imgs, threads, outs=None):
+    """One step of the CPU arm: the oracle (the C restatement of viprs's CPU
+    path) thumbnails every image of the batch in order, each on `threads`
+    host threads.  Returns the thumbnails when `outs` is a list."""
     from oracle import oracle as O
+    for img in host_imgs:
+        r = O.thumbnail(img, "fitbox", BATCH_BOX, BATCH_BOX, threads=threads)
+        if outs is not None:
+            outs.append(r)
+
+
+def cpu_baseline_batch(srcs, dsts):
+    """The oracle on all host cores over the whole batch, once, timed; every
+    thumbnail it makes is compared byte for byte with the GPU batch's."""
+    import numpy as np
     threads = os.cpu_count() or 1
-    O.thumbnail(host_imgs[0], "fitbox", BATCH_BOX, BATCH_BOX, threads=threads)  # warm
-    n, mpix = 0, 0.0
+    host_imgs = [s.cpu().numpy() for s in srcs]
+    mpix = sum(im.shape[0] * im.shape[1] for im in host_imgs) / 1e6
+    outs = []
+    cpu_batch_step(host_imgs[:1], threads)  # warm
     t0 = time.perf_counter()
-    while True:
-        img = host_imgs[n % len(host_imgs)]
-        O.thumbnail(img, "fitbox", BATCH_BOX, BATCH_BOX, threads=threads)
-        n += 1
-        mpix += img.shape[0] * img.shape[1] / 1e6
-        el = time.perf_counter() - t0
-        if el >= seconds:
-            break
-    return {"value": round(mpix / el, 3), "unit": "Mpix/s", "cores": threads, "kind": "port",
-            "sample": f"{n} images of the batch ({mpix:.1f} Mpix), one after another, each on all {threads} "
-                      f"threads, {el:.1f} s"}
+    cpu_batch_step(host_imgs, threads, outs)
+    el = time.perf_counter() - t0
+    same = sum(int(o.shape == tuple(d.shape) and np.array_equal(o, d.cpu().numpy())) for o, d in zip(outs, dsts))
+    line = {"value": round(mpix / el, 3), "unit": "Mpix/s", "cores": threads, "kind": "port",
+            "sample": f"the whole batch ({len(host_imgs)} images, {mpix:.1f} Mpix) once, image after image, "
+                      f"each on all {threads} threads, {el:.1f} s"}
+    return line, same, len(outs)
 
 
 def run_batch(args, rank, ws, local):
@@ -331,12 +348,10 @@ def run_batch(args, rank, ws, local):
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic (seeded smooth sinusoids + uniform noise, generated on device)",
-        "config": {"workload": WORKLOAD if args.images == BATCH_N else f"first {args.images} images of: {WORKLOAD}",
-                   "persistent_launches_per_step": batched_launches,
-                   "images_per_gpu": args.images, "input_bytes_per_gpu": in_bytes,
-                   "input_mpix_per_gpu": round(mpix, 2), "parallelism": f"independent batch per GPU x{ws}",
-                   "l2": f"inputs {in_bytes / 1e9:.1f} GB >> 126 MB L2 (no flush needed)",
-                   "autotuned": tuned, "work_items": items, "stages": stages, "grid": grid},
+        "config": batch_config(shapes),
+        "batch_plan": {"persistent_launches_per_step": batched_launches, "parallelism": f"independent batch per GPU x{ws}",
+                       "l2": f"inputs {in_bytes / 1e9:.1f} GB >> 126 MB L2 (no flush needed)",
+                       "autotuned": tuned, "work_items": items, "stages": stages, "grid": grid},
         "gpu_launches": args.steps * batched_launches,
         "per_image": {"value": round(per_value, 2), "unit": "Mpix/s", "ms_per_step": round(per_ms, 4),
                       "launches_per_step": per_launches},
@@ -349,12 +364,14 @@ def run_batch(args, rank, ws, local):
                      "peak_kind": peak_kind,
                      "kernel": "batch_kernel", "kernel_ms": round(kernel_ms, 4), "algorithmic_bytes": alg},
         "clocks": clocks,
-        "parity": "batched == per-image path (bit-exact)" if same else "MISMATCH",
+        "parity": "batched == per-image path (bit-exact)" if same else "MISMATCH batched vs per-image",
     }
-    if rank == 0 and not args.no_cpu:
-        sample = [s.cpu().numpy() for s in srcs[:64]]
-        line["cpu_baseline"] = cpu_baseline_batch(sample, args.cpu_seconds)
     del host_srcs, host_dsts
+    if rank == 0 and not args.no_cpu:
+        line["cpu_baseline"], n_same, n_cpu = cpu_baseline_batch(srcs, dsts)
+        line["parity"] = (f"oracle bit-exact on {n_same}/{n_cpu} images; " + line["parity"]
+                          if n_same == n_cpu else f"MISMATCH oracle on {n_cpu - n_same}/{n_cpu} images; "
+                          + line["parity"])
     return line
 
 
@@ -429,7 +446,6 @@ def other_reduce_affine_grad(stream, steps):
     from viprs_b200 import _native as N
     from viprs_b200 import api, synth
     n = 16
-    g = torch.Generator().manual_seed(0x5EED0004)
     xs = [synth.uniform_f32(1024, 1024, 4, 0x5EED0004 + i) for i in range(n)]
     gys = [torch.randn((512, 512, 4), device="cuda") for _ in range(n)]
     plan = api.PipelineBuilder(1024, 1024, 4, torch.float32).reduce_h(2.0).reduce_v(2.0).build()
@@ -439,15 +455,7 @@ def other_reduce_affine_grad(stream, steps):
     gxs = [torch.empty((1024, 1024, 4), device="cuda") for _ in range(n)]
     gms = torch.empty((n, 6), dtype=torch.float64, device="cuda")
     mats = []
-    for _ in range(n):
-        th = math.radians(-30 + 60 * float(torch.rand(1, generator=g)))
-        s = 0.8 + 0.6 * float(torch.rand(1, generator=g))
-        t = (-20 + 40 * torch.rand(2, generator=g)).tolist()
-        M = [s * math.cos(th), -s * math.sin(th), s * math.sin(th), s * math.cos(th)]
-        # about the image centre: output centre = M (input centre) + translation
-        c = 256.0
-        tx = c + t[0] - (M[0] * c + M[1] * c)
-        ty = c + t[1] - (M[2] * c + M[3] * c)
+    for M, tx, ty in synth.rotation_matrices(n, 0x5EED0004):
         bm, btx, bty = api.forward_affine_to_backward(M, tx, ty)
         mats.append(((ctypes.c_double * 4)(*bm), btx, bty))
     L = N.lib()
@@ -492,22 +500,12 @@ def other_reduce_affine_grad(stream, steps):
 def other_mapim_grad(stream, steps):
     """4096^2 f32 source, identity grid + smooth displacement (max 8 px), bicubic, fwd + bwd."""
     import torch
-    import torch.nn.functional as F
 
     from viprs_b200 import _native as N
     from viprs_b200 import api, synth
     S = 4096
     src = synth.uniform_f32(S, S, 1, 0x5EED0005)
-    g = torch.Generator(device="cuda").manual_seed(0x5EED0005)
-    noise = torch.randn((2, 1, S, S), generator=g, device="cuda")
-    sigma, r = 32.0, 96
-    k = torch.exp(-0.5 * (torch.arange(-r, r + 1, device="cuda", dtype=torch.float32) / sigma) ** 2)
-    k = (k / k.sum()).view(1, 1, 1, -1)
-    d = F.conv2d(F.conv2d(noise, k, padding=(0, r)), k.view(1, 1, -1, 1), padding=(r, 0))[:, 0]
-    d = d * (8.0 / d.abs().max())
-    yy, xx = torch.meshgrid(torch.arange(S, device="cuda", dtype=torch.float32),
-                            torch.arange(S, device="cuda", dtype=torch.float32), indexing="ij")
-    index = torch.stack([xx + d[0], yy + d[1]], dim=2).contiguous()
+    index = synth.displacement_index(S, 0x5EED0005)
     out = torch.empty((S, S, 1), device="cuda")
     gy = torch.randn((S, S, 1), device="cuda")
     gs = torch.empty_like(src)
@@ -558,35 +556,30 @@ def run_others(steps, only=None):
 
 def run_reference(args, rank, ws):
     """Reference arm: viprs's CPU path restated in C (viprs itself needs a Rust
-    toolchain that this image lacks), on all host cores.  Each step is a bounded
-    sample of the batch: 16 of its images, generated on the host."""
+    toolchain that this image lacks), on all host cores.  Each step is the
+    whole batch -- the same 512 images, shapes and seeds as the GPU arm,
+    generated on the host -- each image's thumbnail on all threads."""
     if rank != 0:
         return None
-    from oracle import oracle as O
     from viprs_b200 import synth
-    shapes = synth.uneven_batch_shapes(BATCH_N, BATCH_SEED)
-    picks = list(range(0, BATCH_N, BATCH_N // 16))[:16]
-    imgs = [synth.smooth_u8(*shapes[i], BATCH_SEED * 1000 + i, device="cpu").numpy() for i in picks]
+    shapes = synth.uneven_batch_shapes(BATCH_N, BATCH_SEED)[:args.images]
+    imgs = [synth.smooth_u8(*shapes[i], BATCH_SEED * 1000 + i, device="cpu").numpy() for i in range(len(shapes))]
     mpix = sum(im.shape[0] * im.shape[1] for im in imgs) / 1e6
     threads = os.cpu_count() or 1
-
-    def step():
-        for im in imgs:
-            O.thumbnail(im, "fitbox", BATCH_BOX, BATCH_BOX, threads=threads)
-
     for _ in range(args.warmup):
-        step()
+        cpu_batch_step(imgs, threads)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        step()
+        cpu_batch_step(imgs, threads)
     el = time.perf_counter() - t0
     v = mpix * args.steps / el
-    sample = f"16 of the 512 batch images ({mpix:.1f} Mpix) per step, each on all {threads} threads"
+    sample = f"the whole batch ({len(imgs)} images, {mpix:.1f} Mpix) per step, image after image, each on all " \
+             f"{threads} threads"
     return {
         "metric": METRIC, "value": round(v, 3), "unit": "Mpix/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(el * 1e3 / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded smooth sinusoids + noise)",
-        "config": {"workload": WORKLOAD, "parallelism": "host threads", "sample": sample},
+        "config": batch_config(shapes),
         "impl": "reference",
         "cpu_baseline": {"value": round(v, 3), "unit": "Mpix/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": round(v, 3), "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -601,7 +594,6 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-others", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--images", type=int, default=BATCH_N, help="first N images of the batch (profiling cases)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default kernel configuration")
     ap.add_argument("--only", default=None, choices=[n for n, _ in OTHERS],

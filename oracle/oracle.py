@@ -296,12 +296,17 @@ def affine(img, matrix, tx, ty, out_w, out_h, kernel="bilinear", threads=1):
 
 def mapim(img, index, kernel="bilinear", extend_copy=False, background=0.0, premultiplied=False,
           threads=1):
+    """MapImOp over whole images: `index` is (h, w, 2) of uint8, uint16 or
+    float32 source coordinates (read as f64).  2/4-band sources take the
+    alpha-premultiplying sampler unless `premultiplied` (mapim.rs:993-1040)."""
     a = _as_image(img)
     sh, sw, b = a.shape
-    idx = np.ascontiguousarray(index, dtype=np.float32)
+    idx = np.ascontiguousarray(index)
+    if idx.dtype not in FORMATS:
+        idx = idx.astype(np.float32)
     ih, iw = idx.shape[:2]
     out = np.zeros((ih, iw, b), a.dtype)
-    st = lib().or_mapim_run(_ptr(a), sw, sh, b, FORMATS[a.dtype], _ptr(idx), iw, ih,
+    st = lib().or_mapim_run(_ptr(a), sw, sh, b, FORMATS[a.dtype], _ptr(idx), FORMATS[idx.dtype], iw, ih,
                             _kernel(kernel), int(extend_copy), ctypes.c_double(background),
                             int(premultiplied), int(threads), _ptr(out))
     if st:

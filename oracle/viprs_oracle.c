@@ -1531,9 +1531,20 @@ int32_t or_resize_run(const void *src, uint32_t w, uint32_t h, uint32_t bands, i
 /* ------------------------------------------------------------------ */
 typedef struct {
     const void *src; uint32_t sw, sh, bands; int32_t fmt;
-    const float *index; uint32_t iw, ih; int32_t kernel, extend_copy; double bg; int32_t premultiplied;
+    const void *index; int32_t index_fmt; uint32_t iw, ih; int32_t kernel, extend_copy; double bg;
+    int32_t premultiplied;
     void *dst; int64_t next_row; pthread_mutex_t mu;
 } mapim_ctx;
+
+/* Index sample i read as f64 whatever its format (mapim.rs:1135-1274 reads the
+   index through ToF64 for every BandFormatId). */
+static double mp_index(const mapim_ctx *c, size_t i) {
+    switch (c->index_fmt) {
+    case OR_U8: return (double)((const uint8_t *)c->index)[i];
+    case OR_U16: return (double)((const uint16_t *)c->index)[i];
+    default: return (double)((const float *)c->index)[i];
+    }
+}
 
 static double mp_band(const mapim_ctx *c, const tile_t *s, int64_t ix, int64_t iy, int32_t band) {
     /* MapImOp::resolve_source_coord / sample_source_band (mapim.rs:306-384) */
@@ -1549,6 +1560,71 @@ static double mp_band(const mapim_ctx *c, const tile_t *s, int64_t ix, int64_t i
         x = clampi(ix, 0, (int64_t)c->sw - 1); y = clampi(iy, 0, (int64_t)c->sh - 1);
     }
     return tget(s, ((size_t)y * c->sw + (size_t)x) * c->bands + (size_t)band);
+}
+
+/* sample_source_band_premultiplied (mapim.rs:616-636): colour bands scaled by
+   the tap's alpha over alpha_max; out-of-range taps read the background for
+   both the band and the alpha. */
+static double mp_band_pm(const mapim_ctx *c, const tile_t *s, int64_t ix, int64_t iy, int32_t band,
+                         int32_t ab, double amax) {
+    double v = mp_band(c, s, ix, iy, band);
+    if (band == ab) return v;
+    return v * (mp_band(c, s, ix, iy, ab) / amax);
+}
+
+/* sample_at_premultiplied (mapim.rs:638-931) for the kernels this path
+   carries: nearest and bilinear at floor(), the separable kernels over
+   cx - (support - 1) .. cx + support with the weight-sum renormalisation
+   (sample_at_premultiplied_separable, :935-991). */
+static double mp_sample_pm(const mapim_ctx *c, const tile_t *s, double x, double y, int32_t band,
+                           int32_t ab, double amax) {
+    if (!isfinite(x) || !isfinite(y)) return c->bg;
+    int32_t k = c->kernel;
+    if (k == OR_K_NEAREST) return mp_band_pm(c, s, f2i(floor(x)), f2i(floor(y)), band, ab, amax);
+    if (k == OR_K_BILINEAR) {
+        int64_t x0 = f2i(floor(x)), y0 = f2i(floor(y));
+        double fx = x - (double)x0, fy = y - (double)y0;
+        return bilinear_mix(mp_band_pm(c, s, x0, y0, band, ab, amax), mp_band_pm(c, s, x0 + 1, y0, band, ab, amax),
+                            mp_band_pm(c, s, x0, y0 + 1, band, ab, amax),
+                            mp_band_pm(c, s, x0 + 1, y0 + 1, band, ab, amax), fx, fy);
+    }
+    int64_t support = k == OR_K_LANCZOS3 ? 3 : 2;
+    int64_t cx = f2i(floor(x)), cy = f2i(floor(y));
+    double acc = 0.0, wsum = 0.0;
+    for (int64_t ky = -(support - 1); ky <= support; ky++) {
+        int64_t iy = cy + ky;
+        double wy = or_kernel_weight(k, fabs((double)iy - y));
+        if (wy == 0.0) continue;
+        for (int64_t kx = -(support - 1); kx <= support; kx++) {
+            int64_t ix = cx + kx;
+            double wx = or_kernel_weight(k, fabs((double)ix - x));
+            if (wx != 0.0) {
+                double w = wx * wy;
+                wsum += w;
+                acc = fma(mp_band_pm(c, s, ix, iy, band, ab, amax), w, acc);
+            }
+        }
+    }
+    return wsum > 0.0 ? acc / wsum : c->bg;
+}
+
+/* sample_source_with_premultiplied_alpha_into (mapim.rs:993-1040): the alpha
+   band sampled from the premultiplied stencil and clamped to [0, alpha_max],
+   each colour band sampled premultiplied and divided by the normalised alpha. */
+static void mp_pixel_pm(const mapim_ctx *c, const tile_t *s, double x, double y, tile_t *o, size_t px) {
+    const int32_t bands = (int32_t)c->bands, ab = bands - 1;
+    if (!isfinite(x) || !isfinite(y)) {
+        for (int32_t b = 0; b < bands; b++) tset_f64(o, px + (size_t)b, c->bg);
+        return;
+    }
+    double amax = aff_alpha_max(c->fmt);
+    double alpha = clampd(mp_sample_pm(c, s, x, y, ab, ab, amax), 0.0, amax);
+    double na = alpha / amax;
+    for (int32_t b = 0; b < ab; b++) {
+        double p = mp_sample_pm(c, s, x, y, b, ab, amax);
+        tset_f64(o, px + (size_t)b, na > 0.0 ? p / na : 0.0);
+    }
+    tset_f64(o, px + (size_t)ab, alpha);
 }
 
 static void *mapim_worker(void *arg) {
@@ -1572,7 +1648,11 @@ static void *mapim_worker(void *arg) {
         for (size_t col = 0; col < c->iw; col++) {
             size_t px = ((size_t)row * c->iw + col) * bands;
             size_t ix = ((size_t)row * c->iw + col) * 2;
-            double rx = (double)c->index[ix], ry = (double)c->index[ix + 1];
+            double rx = mp_index(c, ix), ry = mp_index(c, ix + 1);
+            if (!c->premultiplied && (bands == 2 || bands == 4)) {
+                mp_pixel_pm(c, &s, rx, ry, &o, px);
+                continue;
+            }
             if (!isfinite(rx) || !isfinite(ry)) {
                 for (size_t b2 = 0; b2 < bands; b2++) tset_f64(&o, px + b2, c->bg);
                 continue;
@@ -1602,14 +1682,16 @@ static void *mapim_worker(void *arg) {
 }
 
 int32_t or_mapim_run(const void *src, uint32_t sw, uint32_t sh, uint32_t bands, int32_t fmt,
-                     const float *index, uint32_t iw, uint32_t ih, int32_t kernel, int32_t extend_copy,
-                     double background, int32_t premultiplied, int32_t threads, void *dst) {
+                     const void *index, int32_t index_fmt, uint32_t iw, uint32_t ih, int32_t kernel,
+                     int32_t extend_copy, double background, int32_t premultiplied, int32_t threads,
+                     void *dst) {
     if (!src || !index || !dst || bands == 0) return OR_EINVAL;
-    if (!premultiplied && (bands == 2 || bands == 4)) return OR_EFORMAT; /* alpha path not restated */
+    if (index_fmt != OR_U8 && index_fmt != OR_U16 && index_fmt != OR_F32) return OR_EFORMAT;
     if (kernel == OR_K_NOHALO || kernel == OR_K_LBB || kernel == OR_K_VSQBS) return OR_EFORMAT;
     mapim_ctx c;
     memset(&c, 0, sizeof(c));
-    c.src = src; c.sw = sw; c.sh = sh; c.bands = bands; c.fmt = fmt; c.index = index; c.iw = iw; c.ih = ih;
+    c.src = src; c.sw = sw; c.sh = sh; c.bands = bands; c.fmt = fmt; c.index = index;
+    c.index_fmt = index_fmt; c.iw = iw; c.ih = ih;
     c.kernel = kernel; c.extend_copy = extend_copy; c.bg = background; c.premultiplied = premultiplied; c.dst = dst;
     pthread_mutex_init(&c.mu, NULL);
     int32_t nt = threads > 0 ? threads : 1;

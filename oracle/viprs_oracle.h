@@ -139,9 +139,12 @@ int32_t or_resize_run(const void *src, uint32_t w, uint32_t h, uint32_t bands,
                       int32_t fmt, double hscale, double vscale, int32_t kernel,
                       int32_t threads, void *dst, uint32_t *out_w, uint32_t *out_h);
 
-/* ---- mapim (mapim.rs:1135-1274), full-image form ---- */
+/* ---- mapim (mapim.rs:1135-1274), full-image form ----
+   index: 2-band image of index_fmt (OR_U8 / OR_U16 / OR_F32), read as f64.
+   2/4-band sources with premultiplied == 0 take the alpha-premultiplying
+   sampler (mapim.rs:993-1040). */
 int32_t or_mapim_run(const void *src, uint32_t sw, uint32_t sh, uint32_t bands, int32_t fmt,
-                     const float *index, uint32_t iw, uint32_t ih, int32_t kernel,
+                     const void *index, int32_t index_fmt, uint32_t iw, uint32_t ih, int32_t kernel,
                      int32_t extend_copy, double background, int32_t premultiplied,
                      int32_t threads, void *dst);
 

@@ -1,0 +1,160 @@
+"""Parity at the full sizes of the benchmark configurations.
+
+The small-shape parity tests do not reach every tiling of the kernels: the
+fused reduce fits its tile to the image, the shrink ring chunks columns by the
+ring slot size and the batch splits items by image size.  These tests run the
+exact workloads the benchmark times -- the same seeded generators, shapes and
+parameters -- through the C ABI and compare with the CPU restatement of viprs:
+u8 bit-exact, f32 within a floored relative error of 1e-5.  The gradient
+workloads are checked at full size by the adjoint identity
+<A x, y> = <x, A^T y> with f64 dot products taken on the device.
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from gpu_helpers import assert_same, max_rel_err
+from oracle_chain import run_chain
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from viprs_b200 import _native as N  # noqa: E402
+from viprs_b200 import api, synth  # noqa: E402
+
+THREADS = os.cpu_count() or 1
+BATCH_SEED = 0x5EED0003
+
+
+def host(t):
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+def test_reduce_1024x768x3_quarter(oracle):
+    img = synth.smooth_u8(768, 1024, 3, 0x5EED0000)
+    plan = api.PipelineBuilder(1024, 768, 3, torch.uint8).reduce_h(4.0).reduce_v(4.0).build()
+    got = host(plan(img))
+    exp = run_chain(host(img), [("reduce_h", dict(factor=4.0, kernel="lanczos3")),
+                                ("reduce_v", dict(factor=4.0, kernel="lanczos3"))], threads=THREADS)
+    assert got.shape == (192, 256, 3)
+    assert_same(got, exp, np.uint8)
+
+
+def test_thumbnail_8192x8192x3_to_400(oracle):
+    img = synth.smooth_u8(8192, 8192, 3, 0x5EED0001)
+    plan = api.thumbnail_plan(8192, 8192, 3, torch.uint8, "width", 400)
+    got = host(plan(img))
+    exp = oracle.thumbnail(host(img), "width", 400, 0, "lanczos3", threads=THREADS)
+    assert got.shape == (400, 400, 3)
+    assert_same(got, exp, np.uint8)
+
+
+def test_resize_6000x4000x4_f32(oracle):
+    img = synth.uniform_f32(4000, 6000, 4, 0x5EED0002)
+    plan = api.resize_plan(6000, 4000, 4, torch.float32, 0.37)
+    got = host(plan(img))
+    exp = oracle.resize(host(img), 0.37, 0.37, "lanczos3", threads=THREADS)
+    assert got.shape == (1480, 2220, 4)
+    assert max_rel_err(got, exp) <= 1e-5
+
+
+def test_batch_512_uneven_thumbnails(oracle):
+    """Every thumbnail of the 512-image batch, bit-exact against the oracle."""
+    shapes = synth.uneven_batch_shapes(512, BATCH_SEED)
+    srcs = [synth.smooth_u8(h, w, b, BATCH_SEED * 1000 + i) for i, (h, w, b) in enumerate(shapes)]
+    batch = api.ThumbnailBatch(shapes, "fitbox", 256, 256)
+    dsts = batch.run(srcs, graph=True)
+    torch.cuda.synchronize()
+    assert batch.status() == 0
+    bad = []
+    for i, (s, d) in enumerate(zip(srcs, dsts)):
+        exp = oracle.thumbnail(host(s), "fitbox", 256, 256, "lanczos3", threads=THREADS)
+        got = host(d)
+        if got.shape != exp.shape or not np.array_equal(got, exp):
+            bad.append((i, shapes[i]))
+    assert not bad, f"{len(bad)} of 512 thumbnails differ: {bad[:8]}"
+
+
+def _cfg4(n):
+    plan = api.PipelineBuilder(1024, 1024, 4, torch.float32).reduce_h(2.0).reduce_v(2.0).build()
+    mats = [api.forward_affine_to_backward(m, tx, ty) for m, tx, ty in synth.rotation_matrices(16, 0x5EED0004)]
+    return plan, mats[:n]
+
+
+def test_reduce_affine_forward_16x1024x1024x4(oracle):
+    plan, mats = _cfg4(16)
+    worst = 0.0
+    for i, (bm, btx, bty) in enumerate(mats):
+        x = synth.uniform_f32(1024, 1024, 4, 0x5EED0004 + i)
+        z = plan(x)
+        y = api.affine_backward_matrix(z, bm, btx, bty, 512, 512, "bilinear", "background", 0.0, False)
+        zx = run_chain(host(x), [("reduce_h", dict(factor=2.0, kernel="lanczos3")),
+                                 ("reduce_v", dict(factor=2.0, kernel="lanczos3"))], threads=THREADS)
+        assert max_rel_err(host(z), zx) <= 1e-5
+        ey = oracle.affine_backward(host(z), bm, btx, bty, 512, 512, kernel="bilinear", extend="background",
+                                    background=0.0, premultiplied=False, threads=THREADS)
+        worst = max(worst, max_rel_err(host(y), ey))
+    assert worst <= 1e-5
+
+
+def test_mapim_bicubic_4096_forward(oracle):
+    src = synth.uniform_f32(4096, 4096, 1, 0x5EED0005)
+    index = synth.displacement_index(4096, 0x5EED0005)
+    out = api.mapim(src, index, "bicubic")
+    exp = oracle.mapim(host(src), host(index), "bicubic", threads=THREADS)
+    assert max_rel_err(host(out), exp) <= 1e-5
+
+
+def _ddot(a, b):
+    return float((a.double() * b.double()).sum())
+
+
+def _identity_err(ax, y, x, aty):
+    lhs, rhs = _ddot(ax, y), _ddot(x, aty)
+    return abs(lhs - rhs) / max(float((ax.double() * y.double()).abs().sum()), 1e-30)
+
+
+def test_reduce_affine_adjoint_identity_full_size():
+    """<A x, y> = <x, A^T y> for reduce_h(2)+reduce_v(2) then the bilinear
+    affine in its linear (premultiplied) form, 1024^2 x 4 -> 512^2 x 4."""
+    L = N.lib()
+    plan, mats = _cfg4(4)
+    g = torch.Generator(device="cuda").manual_seed(11)
+    for i, (bm, btx, bty) in enumerate(mats):
+        x = synth.uniform_f32(1024, 1024, 4, 0x5EED0004 + i)
+        z = plan(x)
+        y = api.affine_backward_matrix(z, bm, btx, bty, 512, 512, "bilinear", "background", 0.0, True)
+        gy = torch.randn((512, 512, 4), generator=g, device="cuda")
+        gz = torch.empty_like(z)
+        gx = torch.empty_like(x)
+        g6 = torch.empty(6, dtype=torch.float64, device="cuda")
+        mm = (ctypes.c_double * 4)(*bm)
+        N.check(L.viprs_affine_grad(api.image(z), api.image(gy), api.image(gz), mm, btx, bty, 1, 2, 0.0, 1, 0, 0,
+                                    0, ctypes.c_void_p(g6.data_ptr()), api._stream()), "affine_grad")
+        N.check(L.viprs_reduce_hv_adjoint(api.image(gz), api.image(gx), 2.0, 2.0, 9, api._stream()),
+                "reduce_hv_adjoint")
+        torch.cuda.synchronize()
+        assert _identity_err(y, gy, x, gx) <= 1e-5
+
+
+@pytest.mark.parametrize("det", [0, 1])
+def test_mapim_adjoint_identity_full_size(det):
+    """<mapim(x), y> = <x, mapim^T y> for the 4096^2 bicubic workload
+    (Background 0: mapim is linear in the source), atomic and deterministic
+    scatter."""
+    L = N.lib()
+    src = synth.uniform_f32(4096, 4096, 1, 0x5EED0005)
+    index = synth.displacement_index(4096, 0x5EED0005)
+    out = api.mapim(src, index, "bicubic")
+    gy = torch.randn((4096, 4096, 1), generator=torch.Generator(device="cuda").manual_seed(5), device="cuda")
+    gs = torch.empty_like(src)
+    N.check(L.viprs_mapim_grad(api.image(src), api.image(index), api.image(gy), api.image(gs), None, 2, 0, 0.0, 0,
+                               det, api._stream()), "mapim_grad")
+    torch.cuda.synchronize()
+    assert _identity_err(out, gy, src, gs) <= 1e-5

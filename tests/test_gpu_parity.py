@@ -6,6 +6,8 @@ import pytest
 
 from golden_cases import CASES, expected
 from gpu_helpers import assert_same, rand_image, smooth_image, to_dev, to_host
+from kat_vectors import AFFINE as AFFINE_KAT
+from kat_vectors import MAPIM as MAPIM_KAT
 from oracle_chain import run_chain
 
 pytestmark = pytest.mark.gpu
@@ -220,6 +222,60 @@ def test_mapim(oracle, fmt, kernel, bands):
             assert d.max() <= 1 and (d > 0).mean() < 1e-3
         else:
             assert_same(got, exp, fmt)
+
+
+@pytest.mark.parametrize("fmt", [np.uint8, np.float32])
+@pytest.mark.parametrize("kernel", ["nearest", "bilinear", "bicubic", "lanczos3"])
+@pytest.mark.parametrize("bands", [2, 4])
+def test_mapim_alpha_sampler(oracle, fmt, kernel, bands):
+    # MapImOp's default for 2/4-band sources: taps premultiplied by their own
+    # alpha, the result divided by the interpolated alpha (mapim.rs:993-1040)
+    rng = np.random.default_rng(bands * 31 + len(kernel))
+    src = rand_image(rng, 48, 57, bands, fmt)
+    if fmt == np.uint8:
+        src[::5, ::3, -1] = 0    # transparent pixels keep their colour bytes
+        src[1::4, ::2, -1] = 255
+    yy, xx = np.mgrid[0:40, 0:52].astype(np.float32)
+    idx = np.stack([xx * 1.09 - 2.6 + rng.normal(0, 1.5, xx.shape), yy * 1.17 - 1.9 + rng.normal(0, 1.5, yy.shape)],
+                   -1).astype(np.float32)
+    idx[2, 4, 0] = np.nan
+    for extend_copy in (False, True):
+        got = to_host(api.mapim(to_dev(src), to_dev(idx), kernel, extend_copy, 3.0))
+        exp = oracle.mapim(src, idx, kernel, extend_copy, 3.0)
+        if kernel == "lanczos3" and fmt == np.uint8:
+            d = np.abs(got.astype(int) - exp.astype(int))
+            assert d.max() <= 1 and (d > 0).mean() < 1e-3
+        else:
+            assert_same(got, exp, fmt)
+
+
+@pytest.mark.parametrize("ifmt", [np.uint8, np.uint16])
+@pytest.mark.parametrize("bands", [1, 3, 4])
+def test_mapim_integer_index(oracle, ifmt, bands):
+    # any index format is read as f64 (mapim.rs:1135-1274)
+    rng = np.random.default_rng(bands + 100)
+    src = rand_image(rng, 70, 90, bands, np.uint8)
+    idx = np.stack([rng.integers(0, 95, (33, 41)), rng.integers(0, 75, (33, 41))], -1).astype(ifmt)
+    for kernel in ("nearest", "bilinear", "bicubic"):
+        got = to_host(api.mapim(to_dev(src), to_dev(idx), kernel))
+        assert_same(got, oracle.mapim(src, idx, kernel), np.uint8)
+
+
+@pytest.mark.parametrize("case", MAPIM_KAT, ids=[c[0] for c in MAPIM_KAT])
+def test_mapim_reference_vectors_on_gpu(case):
+    name, src, idx, kernel, copy, bg, pm, expected = case
+    got = to_host(api.mapim(to_dev(src), to_dev(idx), kernel, copy, bg, pm)).ravel()
+    if src.dtype == np.float32:
+        assert np.array_equal(got, expected.astype(np.float32))
+    else:
+        assert got.tolist() == expected.tolist()
+
+
+@pytest.mark.parametrize("case", AFFINE_KAT, ids=[c[0] for c in AFFINE_KAT])
+def test_affine_reference_vectors_on_gpu(case):
+    name, src, m, tx, ty, ow, oh, kernel, extend, bg, pm, expected = case
+    got = to_host(api.affine_backward_matrix(to_dev(src), m, tx, ty, ow, oh, kernel, extend, bg, pm)).ravel()
+    assert got.tolist() == expected.tolist()
 
 
 def test_errors_are_statuses():

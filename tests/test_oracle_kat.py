@@ -125,3 +125,45 @@ def test_affine_identity_nearest(oracle):
     img = rng.integers(0, 256, (20, 30, 3), dtype=np.uint8)
     out = oracle.affine(img, [1, 0, 0, 1], 0, 0, 30, 20, kernel="nearest")
     assert np.array_equal(out, img)
+
+
+# ---- affine and mapim unit-test vectors of the reference (tests/kat_vectors.py)
+
+from kat_vectors import AFFINE, AFFINE_WHITE_EDGES, MAPIM  # noqa: E402
+
+
+@pytest.mark.parametrize("case", AFFINE, ids=[c[0] for c in AFFINE])
+def test_affine_reference_vectors(oracle, case):
+    name, src, m, tx, ty, ow, oh, kernel, extend, bg, pm, expected = case
+    out = oracle.affine_backward(src, m, tx, ty, ow, oh, kernel=kernel, extend=extend, background=bg,
+                                 premultiplied=pm)
+    assert out.ravel().tolist() == expected.tolist()
+
+
+def test_affine_reference_white_extend(oracle):
+    name, src, m, tx, ty, ow, oh, kernel, extend, parts = AFFINE_WHITE_EDGES
+    out = oracle.affine_backward(src, m, tx, ty, ow, oh, kernel=kernel, extend=extend).ravel()
+    for sl, exp in parts.items():
+        assert out[sl].tolist() == exp
+
+
+@pytest.mark.parametrize("case", MAPIM, ids=[c[0] for c in MAPIM])
+def test_mapim_reference_vectors(oracle, case):
+    name, src, idx, kernel, copy, bg, pm, expected = case
+    out = oracle.mapim(src, idx, kernel, copy, bg, pm)
+    if src.dtype == np.float32:
+        assert np.array_equal(out.ravel(), expected.astype(np.float32))
+    else:
+        assert out.ravel().tolist() == expected.tolist()
+
+
+def test_mapim_alpha_opaque_matches_premultiplied(oracle):
+    # mapim.rs:1949-1989: with alpha 255 everywhere the alpha-premultiplying
+    # sampler and the linear one agree
+    rng = np.random.default_rng(5)
+    src = rng.integers(0, 256, (9, 11, 4), dtype=np.uint8)
+    src[..., 3] = 255
+    yy, xx = np.mgrid[0:7, 0:8].astype(np.float32)
+    idx = np.stack([xx * 1.2 + 0.3, yy * 1.1 + 0.45], -1).astype(np.float32)
+    for kernel in ("nearest", "bilinear"):
+        assert np.array_equal(oracle.mapim(src, idx, kernel), oracle.mapim(src, idx, kernel, premultiplied=True))

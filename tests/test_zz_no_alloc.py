@@ -61,6 +61,46 @@ def test_reduce_noalloc_matches_reduce_on_back_to_back_calls():
     assert_same(to_host(again), to_host(outs[0]), CASES[0][3])
 
 
+def test_reduce_noalloc_intermediate_plane():
+    # a 181-tap vertical pass does not fit the fused tile: the call stages the
+    # horizontal pass's plane in the scratch after the tables
+    h, w, b, dt, hf, vf, k = CASES[2]
+    plan = api.PipelineBuilder(w, h, b, torch.uint8).reduce(hf, vf, k).build()
+    assert plan.workspace_bytes > 0
+    t = to_dev(rand_image(np.random.default_rng(9), h, w, b, dt))
+    out = _out_like(t, hf, vf)
+    assert _noalloc(t, out, hf, vf, k) == 0
+    assert_same(to_host(out), to_host(api.reduce(t, hf, vf, k)), dt)
+
+
+def test_reduce_noalloc_at_the_scratch_limit():
+    # the tables plus the intermediate plane grow with the height: find the
+    # tallest image that still fits the array, check its result against
+    # viprs_reduce, and that one row more is refused
+    w, b, hf, vf, k = 900, 3, 3.3, 30.0, "lanczos3"
+    rng = np.random.default_rng(17)
+
+    def status(h):
+        t = torch.zeros((h, w, b), dtype=torch.uint8, device="cuda")
+        return _noalloc(t, _out_like(t, hf, vf), hf, vf, k)
+
+    lo, hi = 700, 8000
+    assert status(lo) == 0 and status(hi) == SCRATCH_LIMIT
+    while hi - lo > 1:
+        mid = (lo + hi) // 2
+        if status(mid) == 0:
+            lo = mid
+        else:
+            hi = mid
+    plan = api.PipelineBuilder(w, lo, b, torch.uint8).reduce(hf, vf, k).build()
+    assert plan.workspace_bytes > (3 << 20), "the plane dominates the scratch at the limit"
+    t = to_dev(rand_image(rng, lo, w, b, np.uint8))
+    out = _out_like(t, hf, vf)
+    assert _noalloc(t, out, hf, vf, k) == 0
+    assert_same(to_host(out), to_host(api.reduce(t, hf, vf, k)), np.uint8)
+    assert status(lo + 1) == SCRATCH_LIMIT
+
+
 def test_reduce_noalloc_rejects_work_beyond_its_scratch():
     # a 2,000,000-pixel-wide row needs ~6.7 MB of position tables: more than the 4 MiB array
     t = torch.zeros((1, 2_000_000, 1), dtype=torch.uint8, device="cuda")

@@ -172,11 +172,15 @@ def forward_affine_to_backward(matrix, tx, ty):
 
 
 def mapim(src, index, kernel="bilinear", extend_copy=False, background=0.0, premultiplied=False):
-    """MapImOp: index is a (h, w, 2) float32 tensor of source coordinates."""
+    """MapImOp (resample/mapim.rs): index is a (h, w, 2) uint8, uint16 or
+    float32 tensor of source coordinates, read as f64.  2- and 4-band sources
+    are alpha-premultiplied inside the sampler unless `premultiplied` says
+    they already are (MapImOp::with_premultiplied, viprs's default false)."""
     src = _as_hwc(src)
     index = _as_hwc(index)
-    if index.dtype != torch.float32 or index.shape[2] != 2:
-        raise ValueError("index must be a (h, w, 2) float32 tensor")
+    if index.shape[2] != 2:
+        raise ValueError("index must be a (h, w, 2) tensor")
+    _dtype_format(index.dtype)
     out = _empty(index.shape[0], index.shape[1], src.shape[2], src)
     N.check(N.lib().viprs_mapim(image(src), image(index), image(out), _kernel(kernel), int(extend_copy),
                                 float(background), int(premultiplied), _stream()), "mapim")

@@ -14,7 +14,8 @@
 //   sample_at / separable ......... affine/core.rs:640-760
 //   extend modes .................. affine/interpolation.rs:43-137
 //   MapImOp::process_typed ........ mapim.rs:1135-1274 (bilinear 1043-1096,
-//                                   nearest 1099-1132, extend 306-384)
+//                                   nearest 1099-1132, extend 306-384,
+//                                   alpha sampler 616-1040)
 #include <algorithm>
 
 #include "affine_dev.cuh"
@@ -62,6 +63,14 @@ cudaError_t mapim(const MapimArgs& a, cudaStream_t s) {
     const dim3 grid((unsigned)((a.out.w + 255) / 256), (unsigned)std::min<int64_t>(a.out.h, 65535));
     // the kernels index a source row with 32-bit element offsets
     if ((int64_t)a.src_w * a.bands >= ((int64_t)1 << 31)) return cudaErrorInvalidValue;
+    if (a.alpha) {
+        switch (a.fmt) {
+        case kU8: dev::mapim_alpha_kernel<uint8_t><<<grid, 256, 0, s>>>(a); break;
+        case kU16: dev::mapim_alpha_kernel<uint16_t><<<grid, 256, 0, s>>>(a); break;
+        default: dev::mapim_alpha_kernel<float><<<grid, 256, 0, s>>>(a); break;
+        }
+        return cudaGetLastError();
+    }
     const int nt = (a.kernel == 0 || a.kernel == 1) ? 0 : (a.kernel == 9 ? 6 : 4);
     switch (a.fmt * 8 + nt) {
     case kU8 * 8 + 0: dev::mapim_kernel<uint8_t, 0><<<grid, 256, 0, s>>>(a); break;

@@ -505,12 +505,27 @@ __device__ __forceinline__ double mp_band(const MapimArgs& a, int64_t ix, int64_
     return ok ? v : a.background;
 }
 
+// Coordinates of output pixel (lx, ly) from the index image, read as f64
+// whatever the index format (mapim.rs:1135-1274 reads them through ToF64).
+__device__ __forceinline__ void mp_coords(const MapimArgs& a, int64_t lx, int64_t ly, double* rx, double* ry) {
+    const uint8_t* row = a.index.data + ly * a.index.pitch;
+    if (a.index_fmt == kF32) {
+        const float2 v = *reinterpret_cast<const float2*>(row + lx * 8);
+        *rx = (double)v.x; *ry = (double)v.y;
+    } else if (a.index_fmt == kU16) {
+        const ushort2 v = *reinterpret_cast<const ushort2*>(row + lx * 4);
+        *rx = (double)v.x; *ry = (double)v.y;
+    } else {
+        *rx = (double)row[lx * 2]; *ry = (double)row[lx * 2 + 1];
+    }
+}
+
 // NT: taps per axis of the separable samplers (4: support 2, 6: Lanczos3);
 // 0 for the nearest / bilinear kernels.
 template <typename T, int NT>
 __device__ __forceinline__ void mapim_px(const MapimArgs& a, int64_t lx, int64_t ly) {
-    const float2 idx = *reinterpret_cast<const float2*>(a.index.data + ly * a.index.pitch + lx * 8);
-    const double rx = (double)idx.x, ry = (double)idx.y;
+    double rx, ry;
+    mp_coords(a, lx, ly, &rx, &ry);
     const int bands = a.bands;
     T* dst = reinterpret_cast<T*>(a.out.data + ly * a.out.pitch) + lx * bands;
     if (!isfinite(rx) || !isfinite(ry)) {
@@ -606,6 +621,88 @@ __global__ void __launch_bounds__(256, 4) mapim_kernel(MapimArgs a) {
     const int64_t lx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (lx >= a.out.w) return;
     for (int64_t ly = blockIdx.y; ly < a.out.h; ly += gridDim.y) mapim_px<T, NT>(a, lx, ly);
+}
+
+// ---------------------------------------------------------------- mapim, alpha sampler
+// 2/4-band sources that are not premultiplied (MapImOp's default): every tap
+// is premultiplied by its own alpha / alpha_max before interpolation, the
+// interpolated alpha is clamped to [0, alpha_max] and each colour band is
+// divided by it (sample_source_with_premultiplied_alpha_into,
+// mapim.rs:993-1040; taps through sample_source_band_premultiplied, :616-636,
+// and mapim's own extend rules, :306-384).
+
+template <typename T>
+__device__ __forceinline__ double mp_band_pm(const MapimArgs& a, int64_t ix, int64_t iy, int band, int ab,
+                                             double amax) {
+    bool ok;
+    const T* px = mp_tap<T>(a, ix, iy, &ok);
+    const double v = ok ? (double)px[band] : a.background;
+    if (band == ab) return v;
+    const double al = ok ? (double)px[ab] : a.background;
+    return v * (al / amax);
+}
+
+// sample_at_premultiplied (mapim.rs:638-931) for nearest, bilinear (both at
+// floor()) and the separable kernels (sample_at_premultiplied_separable,
+// :935-991: taps cx - (support - 1) .. cx + support, zero weights skipped,
+// renormalised by the weight sum).
+template <typename T>
+__device__ double mp_sample_pm(const MapimArgs& a, double x, double y, int band, int ab, double amax) {
+    const int k = a.kernel;
+    const int64_t cx = trunc_i64(floor(x)), cy = trunc_i64(floor(y));
+    if (k == 0) return mp_band_pm<T>(a, cx, cy, band, ab, amax);
+    if (k == 1) {
+        const double fx = x - (double)cx, fy = y - (double)cy;
+        const double p00 = mp_band_pm<T>(a, cx, cy, band, ab, amax);
+        const double p01 = mp_band_pm<T>(a, cx + 1, cy, band, ab, amax);
+        const double p10 = mp_band_pm<T>(a, cx, cy + 1, band, ab, amax);
+        const double p11 = mp_band_pm<T>(a, cx + 1, cy + 1, band, ab, amax);
+        const double top = fma(p01, fx, p00 * (1.0 - fx));
+        const double bottom = fma(p11, fx, p10 * (1.0 - fx));
+        return top * (1.0 - fy) + bottom * fy;
+    }
+    const int support = k == 9 ? 3 : 2;
+    double acc = 0.0, wsum = 0.0;
+    for (int ky = -(support - 1); ky <= support; ++ky) {
+        const int64_t iy = cy + ky;
+        const double wy = kernel_w(k, fabs((double)iy - y));
+        if (wy == 0.0) continue;
+        for (int kx = -(support - 1); kx <= support; ++kx) {
+            const int64_t ix = cx + kx;
+            const double wx = kernel_w(k, fabs((double)ix - x));
+            if (wx != 0.0) {
+                const double w = wx * wy;
+                wsum += w;
+                acc = fma(mp_band_pm<T>(a, ix, iy, band, ab, amax), w, acc);
+            }
+        }
+    }
+    return wsum > 0.0 ? acc / wsum : a.background;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) mapim_alpha_kernel(MapimArgs a) {
+    const int64_t lx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (lx >= a.out.w) return;
+    const int bands = a.bands, ab = bands - 1;
+    const double amax = sizeof(T) == 4 ? 1.0 : (sizeof(T) == 2 ? 65535.0 : 255.0);
+    for (int64_t ly = blockIdx.y; ly < a.out.h; ly += gridDim.y) {
+        double rx, ry;
+        mp_coords(a, lx, ly, &rx, &ry);
+        T* dst = reinterpret_cast<T*>(a.out.data + ly * a.out.pitch) + lx * bands;
+        if (!isfinite(rx) || !isfinite(ry)) {
+            for (int b = 0; b < bands; ++b) dst[b] = from_f64<T>(a.background);
+            continue;
+        }
+        double alpha = mp_sample_pm<T>(a, rx, ry, ab, ab, amax);
+        alpha = alpha < 0.0 ? 0.0 : (alpha > amax ? amax : alpha);
+        const double na = alpha / amax;
+        for (int b = 0; b < ab; ++b) {
+            const double p = mp_sample_pm<T>(a, rx, ry, b, ab, amax);
+            dst[b] = from_f64<T>(na > 0.0 ? p / na : 0.0);
+        }
+        dst[ab] = from_f64<T>(alpha);
+    }
 }
 
 }  // namespace dev

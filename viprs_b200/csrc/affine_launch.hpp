@@ -38,12 +38,14 @@ struct AffineArgs {
 // MapImOp (resample/mapim.rs).
 struct MapimArgs {
     PlaneArg src;
-    PlaneArg index;  // 2-band f32
+    PlaneArg index;  // 2-band coordinates of index_fmt (u8, u16 or f32), read as f64
     OutPlaneArg out;
     int32_t bands = 1;
     int32_t fmt = kF32;
+    int32_t index_fmt = kF32;
     int32_t kernel = 1;
     int32_t extend_copy = 0;
+    int32_t alpha = 0;  // 2/4 bands, not premultiplied: the alpha-premultiplying sampler
     double background = 0.0;
     uint32_t src_w = 0, src_h = 0;
 };

@@ -785,12 +785,11 @@ int32_t viprs_mapim(const viprs_image* src, const viprs_image* index, const vipr
     if (st) return st;
     st = check_image(out);
     if (st) return st;
-    if (index->format != VIPRS_F32 || index->bands != 2) return VIPRS_ERR_UNSUPPORTED_FORMAT;
+    // any index format is read as f64 (mapim.rs:1135-1274)
+    if (index->bands != 2) return VIPRS_ERR_UNSUPPORTED_FORMAT;
     if (out->format != src->format || out->bands != src->bands) return VIPRS_ERR_SIZE_MISMATCH;
     if (index->width != out->width || index->height != out->height) return VIPRS_ERR_SIZE_MISMATCH;
     if (kernel < 0 || kernel > 9 || !affine_kernel_supported(Kernel(kernel))) return VIPRS_ERR_INVALID_KERNEL;
-    // the 2/4-band alpha-premultiplied sampler of mapim.rs:993-1040 is not on this path
-    if (!premultiplied && (src->bands == 2 || src->bands == 4)) return VIPRS_ERR_UNSUPPORTED_FORMAT;
     if (src->bands > 8) return VIPRS_ERR_INVALID_ARGUMENT;
     MapimArgs a;
     a.src.data = static_cast<const uint8_t*>(src->data);
@@ -801,6 +800,10 @@ int32_t viprs_mapim(const viprs_image* src, const viprs_image* index, const vipr
     a.out.data = static_cast<uint8_t*>(out->data);
     a.out.w = int32_t(out->width); a.out.h = int32_t(out->height); a.out.pitch = pitch_of(out);
     a.bands = int32_t(src->bands); a.fmt = src->format; a.kernel = kernel; a.extend_copy = extend_copy != 0;
+    a.index_fmt = index->format;
+    // 2/4-band sources are alpha-premultiplied inside the sampler unless the
+    // caller says they already are (MapImOp::has_alpha, mapim.rs:157-159)
+    a.alpha = !premultiplied && (src->bands == 2 || src->bands == 4);
     a.background = background; a.src_w = src->width; a.src_h = src->height;
     return cuda_status(launch::mapim(a, static_cast<cudaStream_t>(stream)));
 }

@@ -87,6 +87,9 @@ extern "C" int32_t viprs_reduce_noalloc(const viprs_image* in, const viprs_image
     st = scratch_on_current_device(&scratch);
     if (st) return st;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // The tables come from pageable host memory (the plan's vector, freed when
+    // this call returns): the runtime stages a pageable host-to-device copy
+    // before cudaMemcpyAsync returns, so the vector may go away afterwards.
     if (!plan.host_tables.empty()) {
         const cudaError_t e =
             cudaMemcpyAsync(scratch, plan.host_tables.data(), plan.host_tables.size(), cudaMemcpyHostToDevice, s);

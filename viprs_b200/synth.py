@@ -47,3 +47,38 @@ def uneven_batch_shapes(n, seed, wmin=256, wmax=6000):
         b = 3 if float(torch.rand(1, generator=g)) < 0.5 else 4
         shapes.append((h, w, b))
     return shapes
+
+
+def rotation_matrices(n, seed, centre=256.0):
+    """Per image a forward affine of the reduce+affine workload: rotation
+    theta ~ U(-30, 30) degrees, scale s ~ U(0.8, 1.4) about the centre of a
+    512 x 512 image, translation t ~ U(-20, 20)^2 px.  Returns (M, tx, ty)
+    tuples, M = s R(theta) row-major, so that out = M in + (tx, ty)."""
+    g = torch.Generator().manual_seed(int(seed))
+    out = []
+    for _ in range(n):
+        th = math.radians(-30 + 60 * float(torch.rand(1, generator=g)))
+        s = 0.8 + 0.6 * float(torch.rand(1, generator=g))
+        t = (-20 + 40 * torch.rand(2, generator=g)).tolist()
+        m = [s * math.cos(th), -s * math.sin(th), s * math.sin(th), s * math.cos(th)]
+        tx = centre + t[0] - (m[0] * centre + m[1] * centre)
+        ty = centre + t[1] - (m[2] * centre + m[3] * centre)
+        out.append((m, tx, ty))
+    return out
+
+
+def displacement_index(size, seed, amplitude=8.0, sigma=32.0, device="cuda"):
+    """2-band f32 coordinate image of the mapim workload: the identity grid
+    plus a displacement made of N(0, 1) noise, Gaussian-filtered (sigma px,
+    separable, zero padding) and scaled to `amplitude` px at its maximum."""
+    import torch.nn.functional as F
+    g = torch.Generator(device=device).manual_seed(int(seed))
+    noise = torch.randn((2, 1, size, size), generator=g, device=device)
+    r = int(3 * sigma)
+    k = torch.exp(-0.5 * (torch.arange(-r, r + 1, device=device, dtype=torch.float32) / sigma) ** 2)
+    k = (k / k.sum()).view(1, 1, 1, -1)
+    d = F.conv2d(F.conv2d(noise, k, padding=(0, r)), k.view(1, 1, -1, 1), padding=(r, 0))[:, 0]
+    d = d * (amplitude / d.abs().max())
+    yy, xx = torch.meshgrid(torch.arange(size, device=device, dtype=torch.float32),
+                            torch.arange(size, device=device, dtype=torch.float32), indexing="ij")
+    return torch.stack([xx + d[0], yy + d[1]], dim=2).contiguous()
