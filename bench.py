@@ -1,7 +1,7 @@
 """Benchmark of the resample hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--no-cpu] [--no-others]
+                    [--no-cpu] [--no-others] [--split]
                     [--images N] [--only NAME]
 
 Headline workload (the metric "input Mpix/s batched vs per-image GPU (bit-exact
@@ -18,7 +18,9 @@ images, and the batch output is checked bit-exact against it.
 
 Every rank runs its own 512-image batch (different seeds): `value` is the
 input Mpix/s of all ranks over the max-over-ranks time, scaling "weak"; no
-data crosses between GPUs.
+data crosses between GPUs.  With `--split` the ranks divide ONE batch by byte
+weight (api.partition_batch, computed identically on every rank), scaling
+"strong".
 
 `e2e` is the same batch through ThumbnailBatch.run_host: pinned host images
 copied in, the graph run, thumbnails copied out, every step.  `roofline` is the
@@ -235,11 +237,15 @@ def graph_timed(fn, steps):
 
 # ----------------------------------------------------------------------------- headline: batched thumbnails
 
-def make_batch_images(seed, n=BATCH_N, device="cuda"):
+def make_batch_images(seed, n=BATCH_N, device="cuda", indices=None):
+    """Shapes and pixels of the batch (its first n images, or the images
+    `indices` of them), each image seeded by its index in the batch."""
     from viprs_b200 import synth
     shapes = synth.uneven_batch_shapes(BATCH_N, seed)[:n]
-    imgs = [synth.smooth_u8(h, w, b, seed * 1000 + i, device=device) for i, (h, w, b) in enumerate(shapes)]
-    return shapes, imgs
+    if indices is None:
+        indices = range(len(shapes))
+    imgs = [synth.smooth_u8(*shapes[i], seed * 1000 + i, device=device) for i in indices]
+    return [shapes[i] for i in indices], imgs
 
 
 def cpu_batch_step(host_imgs, threads, outs=None):
@@ -280,13 +286,21 @@ def run_batch(args, rank, ws, local):
 
     torch.cuda.set_device(local)
     stream = torch.cuda.current_stream()
-    shapes, srcs = make_batch_images(BATCH_SEED + 7919 * rank, args.images)
+    if args.split and ws > 1:
+        # one batch divided over the ranks by byte weight (strong scaling)
+        from viprs_b200 import synth
+        every = synth.uneven_batch_shapes(BATCH_N, BATCH_SEED)[:args.images]
+        shapes, srcs = make_batch_images(BATCH_SEED, args.images, indices=api.partition_batch(every, ws)[rank])
+    else:
+        # an independent batch per rank (weak scaling)
+        shapes, srcs = make_batch_images(BATCH_SEED + 7919 * rank, args.images)
     batch = api.ThumbnailBatch(shapes, "fitbox", BATCH_BOX, BATCH_BOX)
     dsts = batch.alloc_outputs()
     in_bytes = sum(h * w * b for h, w, b in shapes)
     out_bytes = sum(h * w * b for h, w, b in batch.out_shapes)
     mpix = sum(h * w for h, w, _ in shapes) / 1e6
 
+    split = bool(args.split and ws > 1)
     # the project's autotuner picks the ring size, work-list lag and blocks per SM
     tuned = batch.autotune(srcs, dsts, repeats=2)[0] if not args.no_autotune else batch.config()
     items, stages, grid = batch.work()
@@ -346,10 +360,12 @@ def run_batch(args, rank, ws, local):
     line = {
         "metric": METRIC, "value": round(value, 2), "unit": "Mpix/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "scaling": "strong" if split else "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic (seeded smooth sinusoids + uniform noise, generated on device)",
-        "config": batch_config(shapes),
-        "batch_plan": {"persistent_launches_per_step": batched_launches, "parallelism": f"independent batch per GPU x{ws}",
+        "config": batch_config(every if split else shapes),
+        "batch_plan": {"persistent_launches_per_step": batched_launches,
+                       "parallelism": (f"one batch split over {ws} GPUs by byte weight" if split
+                                       else f"independent batch per GPU x{ws}"),
                        "l2": f"inputs {in_bytes / 1e9:.1f} GB >> 126 MB L2 (no flush needed)",
                        "autotuned": tuned, "work_items": items, "stages": stages, "grid": grid},
         "gpu_launches": args.steps * batched_launches,
@@ -596,6 +612,9 @@ def main():
     ap.add_argument("--no-others", action="store_true")
     ap.add_argument("--images", type=int, default=BATCH_N, help="first N images of the batch (profiling cases)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default kernel configuration")
+    ap.add_argument("--split", action="store_true",
+                    help="with several GPUs: divide ONE batch over them by byte weight (strong scaling) instead of "
+                         "giving each GPU its own batch")
     ap.add_argument("--only", default=None, choices=[n for n, _ in OTHERS],
                     help="run one of the other configurations alone, --steps timed steps (profiling cases)")
     args = ap.parse_args()

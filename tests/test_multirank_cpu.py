@@ -3,9 +3,13 @@
 bench.py runs one rank per GPU: each rank takes its own images, no data
 crosses between ranks, and only the timing is combined (max of the ranks'
 times, sum of their megapixels).  These tests run that plumbing with two CPU
-processes: the byte-weighted split of one batch over the ranks, and the rank
-reductions the bench reports.
+processes: the byte-weighted split of one batch over the ranks, the rank
+reductions the bench reports, and a split batch whose per-rank thumbnails
+(computed with the CPU restatement of viprs on each rank) together equal the
+single-process result.
 """
+import zlib
+
 import os
 import socket
 
@@ -44,6 +48,58 @@ def _rank_main(rank, ws, port, result_dir):
             f.write(f"{total!r} {slowest!r} {len(mine)}\n")
     finally:
         dist.destroy_process_group()
+
+
+SPLIT_SEED = 0x5EED0013
+
+
+def _split_shapes():
+    from viprs_b200 import synth
+    return synth.uneven_batch_shapes(24, SPLIT_SEED, wmin=48, wmax=700)
+
+
+def _thumb_digest(i, shape):
+    from oracle import oracle as O
+    from viprs_b200 import synth
+    img = synth.smooth_u8(*shape, SPLIT_SEED * 1000 + i, device="cpu").numpy()
+    out = O.thumbnail(img, "fitbox", 64, 64)
+    return out.shape, zlib.crc32(out.tobytes())
+
+
+def _split_rank_main(rank, ws, port, result_dir):
+    import datetime
+    import json
+
+    from viprs_b200 import api
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=ws,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        shapes = _split_shapes()
+        mine = api.partition_batch(shapes, ws)[rank]
+        local = {i: _thumb_digest(i, shapes[i]) for i in mine}
+        gathered = [None] * ws
+        dist.all_gather_object(gathered, local)
+        if rank == 0:
+            union = {}
+            for part in gathered:
+                assert not set(part) & set(union), "an image was thumbnailed on two ranks"
+                union.update(part)
+            with open(os.path.join(result_dir, "union.json"), "w") as f:
+                json.dump({str(k): [list(v[0]), v[1]] for k, v in union.items()}, f)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_split_batch_union_equals_single_process(tmp_path):
+    import json
+    ws = 2
+    mp.spawn(_split_rank_main, args=(ws, _free_port(), str(tmp_path)), nprocs=ws, join=True)
+    union = json.load(open(tmp_path / "union.json"))
+    shapes = _split_shapes()
+    assert sorted(int(k) for k in union) == list(range(len(shapes)))
+    for i, shape in enumerate(shapes):
+        out_shape, crc = _thumb_digest(i, shape)
+        assert union[str(i)] == [list(out_shape), crc], f"image {i} differs between the split and one process"
 
 
 def test_partition_is_a_balanced_cover():

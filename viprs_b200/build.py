@@ -18,7 +18,8 @@ OBJ_DIR = os.path.join(ROOT, "_build", "obj")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
-CU_SOURCES = ["resample.cu", "affine.cu", "adjoint.cu", "batch.cu", "noalloc.cu"]
+CU_SOURCES = ["resample.cu", "affine.cu", "affine_u8.cu", "affine_u16.cu", "affine_f32.cu", "adjoint.cu", "batch.cu",
+              "noalloc.cu"]
 CPP_SOURCES = ["plan.cpp", "affine_plan.cpp", "capi.cpp", "batch_plan.cpp", "adjoint_plan.cpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -30,19 +31,31 @@ def _sources_present():
     return cu, cpp
 
 
-def _stale(obj, deps):
+def _deps(obj):
+    """Files the compiler recorded as inputs of `obj` (its -MD file), or None."""
+    path = obj + ".d"
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        text = f.read().replace("\\\n", " ")
+    _, _, rest = text.partition(":")
+    return [d for d in rest.split() if d]
+
+
+def _stale(obj, src):
     if not os.path.exists(obj):
         return True
+    deps = _deps(obj)
+    if deps is None:
+        return True
     t = os.path.getmtime(obj)
-    return any(os.path.getmtime(d) > t for d in deps)
+    return any(not os.path.exists(d) or os.path.getmtime(d) > t for d in [src] + deps)
 
 
 def build(force=False, verbose=False, jobs=8):
     os.makedirs(OUT_DIR, exist_ok=True)
     os.makedirs(OBJ_DIR, exist_ok=True)
     cu, cpp = _sources_present()
-    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".hpp", ".cuh", ".h"))]
-    headers.append(os.path.join(ROOT, "include", "viprs_b200.h"))
     inc = ["-I", os.path.join(ROOT, "include"), "-I", CSRC]
     cmds = []
     objs = []
@@ -50,18 +63,18 @@ def build(force=False, verbose=False, jobs=8):
         src = os.path.join(CSRC, s)
         obj = os.path.join(OBJ_DIR, s + ".o")
         objs.append(obj)
-        if force or _stale(obj, [src] + headers):
+        if force or _stale(obj, src):
             cmds.append([NVCC, *ARCH, "-lineinfo", "-O3", "--fmad=false", "-std=c++17",
                          "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", *inc,
-                         "-c", src, "-o", obj])
+                         "-MD", "-MF", obj + ".d", "-c", src, "-o", obj])
     for s in cpp:
         src = os.path.join(CSRC, s)
         obj = os.path.join(OBJ_DIR, s + ".o")
         objs.append(obj)
-        if force or _stale(obj, [src] + headers):
+        if force or _stale(obj, src):
             cmds.append(["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
                          "-Wall", "-Wno-unused-function", *inc, "-I", os.path.join(CUDA_HOME, "include"),
-                         "-c", src, "-o", obj])
+                         "-MD", "-MF", obj + ".d", "-c", src, "-o", obj])
     procs = []
     for c in cmds:
         if verbose:

@@ -1,8 +1,10 @@
 // affine.cu -- sm_100a kernels for viprs's affine and mapim interpolators.
 //
-// One thread per output pixel (all bands).  All coordinate and weight
-// arithmetic is f64 in viprs's operation order (this TU is compiled with
-// --fmad=false; fma() appears exactly where viprs calls mul_add), so u8 and
+// One thread per output pixel (all bands); the kernels of each sample format
+// are instantiated in affine_u8.cu, affine_u16.cu and affine_f32.cu.  All
+// coordinate and weight arithmetic is f64 in viprs's operation order (these
+// TUs are compiled with --fmad=false; fma() appears exactly where viprs calls
+// mul_add), so u8 and
 // f32 outputs reproduce viprs bit for bit except for kernels that evaluate
 // sin() on the device (Lanczos2/3, Nohalo), whose weights can differ from
 // glibc's by an ulp.
@@ -18,21 +20,10 @@
 //                                   alpha sampler 616-1040)
 #include <algorithm>
 
-#include "affine_dev.cuh"
+#include "affine_fmt.hpp"
 
 namespace viprs {
 namespace launch {
-
-// the band count as a template parameter for the common counts
-template <typename T>
-static void launch_affine(const AffineArgs& k, dim3 grid, cudaStream_t s) {
-    switch (k.bands) {
-    case 1: dev::affine_kernel<T, 1><<<grid, 256, 0, s>>>(k); break;
-    case 3: dev::affine_kernel<T, 3><<<grid, 256, 0, s>>>(k); break;
-    case 4: dev::affine_kernel<T, 4><<<grid, 256, 0, s>>>(k); break;
-    default: dev::affine_kernel<T, 0><<<grid, 256, 0, s>>>(k); break;
-    }
-}
 
 int affine_group(int64_t npx) {
     // enough threads for a few waves of 2048 per SM on 148 SMs, then up to
@@ -50,9 +41,9 @@ cudaError_t affine(const AffineArgs& a, cudaStream_t s) {
     const int64_t gx = ((int64_t)a.out.w + k.group - 1) / k.group;
     const dim3 grid((unsigned)((gx + 255) / 256), (unsigned)std::min<int64_t>(a.out.h, 65535));
     switch (a.fmt) {
-    case kU8: launch_affine<uint8_t>(k, grid, s); break;
-    case kU16: launch_affine<uint16_t>(k, grid, s); break;
-    default: launch_affine<float>(k, grid, s); break;
+    case kU8: affine_u8(k, grid, s); break;
+    case kU16: affine_u16(k, grid, s); break;
+    default: affine_f32(k, grid, s); break;
     }
     return cudaGetLastError();
 }
@@ -63,28 +54,13 @@ cudaError_t mapim(const MapimArgs& a, cudaStream_t s) {
     const dim3 grid((unsigned)((a.out.w + 255) / 256), (unsigned)std::min<int64_t>(a.out.h, 65535));
     // the kernels index a source row with 32-bit element offsets
     if ((int64_t)a.src_w * a.bands >= ((int64_t)1 << 31)) return cudaErrorInvalidValue;
-    if (a.alpha) {
-        switch (a.fmt) {
-        case kU8: dev::mapim_alpha_kernel<uint8_t><<<grid, 256, 0, s>>>(a); break;
-        case kU16: dev::mapim_alpha_kernel<uint16_t><<<grid, 256, 0, s>>>(a); break;
-        default: dev::mapim_alpha_kernel<float><<<grid, 256, 0, s>>>(a); break;
-        }
-        return cudaGetLastError();
-    }
     const int nt = (a.kernel == 0 || a.kernel == 1) ? 0 : (a.kernel == 9 ? 6 : 4);
-    switch (a.fmt * 8 + nt) {
-    case kU8 * 8 + 0: dev::mapim_kernel<uint8_t, 0><<<grid, 256, 0, s>>>(a); break;
-    case kU8 * 8 + 4: dev::mapim_kernel<uint8_t, 4><<<grid, 256, 0, s>>>(a); break;
-    case kU8 * 8 + 6: dev::mapim_kernel<uint8_t, 6><<<grid, 256, 0, s>>>(a); break;
-    case kU16 * 8 + 0: dev::mapim_kernel<uint16_t, 0><<<grid, 256, 0, s>>>(a); break;
-    case kU16 * 8 + 4: dev::mapim_kernel<uint16_t, 4><<<grid, 256, 0, s>>>(a); break;
-    case kU16 * 8 + 6: dev::mapim_kernel<uint16_t, 6><<<grid, 256, 0, s>>>(a); break;
-    case kF32 * 8 + 0: dev::mapim_kernel<float, 0><<<grid, 256, 0, s>>>(a); break;
-    case kF32 * 8 + 4: dev::mapim_kernel<float, 4><<<grid, 256, 0, s>>>(a); break;
-    case kF32 * 8 + 6: dev::mapim_kernel<float, 6><<<grid, 256, 0, s>>>(a); break;
+    switch (a.fmt) {
+    case kU8: return mapim_u8(a, grid, nt, s);
+    case kU16: return mapim_u16(a, grid, nt, s);
+    case kF32: return mapim_f32(a, grid, nt, s);
     default: return cudaErrorInvalidValue;
     }
-    return cudaGetLastError();
 }
 
 }  // namespace launch

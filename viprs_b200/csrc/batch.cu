@@ -149,8 +149,8 @@ __device__ bool consume_shrink(const BatchArgs& g, const BatchStage& st, int32_t
     ShrinkChunk c;
     shrink_item_geom(st, a, index, &oy0, &oy1, &c);
     if ((reinterpret_cast<uintptr_t>(a.in.data) & 15) == 0)
-        return ws_consume<B, 1>(a, oy0, oy1, c, &ctl->ring, bufs, g.ring_stage_bytes, g.ring_slots, slot, ph,
-                                reinterpret_cast<volatile int32_t*>(&ctl->cstop));
+        return ws_consume<B>(a, oy0, oy1, c, &ctl->ring, bufs, g.ring_stage_bytes, g.ring_slots, slot, ph,
+                             reinterpret_cast<volatile int32_t*>(&ctl->cstop));
     // unaligned source: clamped plain loads, a few columns at a time
     const int32_t per_col = int32_t(a.fv) * int32_t(a.fh) * B;
     const int32_t step = max(1, int32_t((g.work_bytes - 64) / (per_col + B)));
@@ -245,7 +245,7 @@ __device__ void batch_consumers(const BatchArgs& g, BatchCtl* ctl, const BatchSt
 // RING: a launch of shrink items (the ring in shared memory); otherwise a
 // launch of the other item kinds (the work region in shared memory).
 template <bool RING>
-__global__ void __launch_bounds__(kWsThreads, RING ? 5 : 3) batch_kernel(BatchArgs g) {
+__global__ void __launch_bounds__(kWsThreads, RING ? 4 : 3) batch_kernel(BatchArgs g) {
     extern __shared__ __align__(128) uint8_t smem_b[];
     BatchCtl* ctl = reinterpret_cast<BatchCtl*>(smem_b);
     const size_t ctl_bytes = (sizeof(BatchCtl) + 127) / 128 * 128;

@@ -121,7 +121,10 @@ int plan_stages(viprs_batch* b, int image, std::vector<std::vector<BatchStage>>*
             const int64_t row_src = int64_t(bs.chunk_cols) * per_col * bs.sh.fv;
             bs.rows_per_item = int32_t(std::max<int64_t>(1, std::min<int64_t>(outp.h, b->item_bytes / std::max<int64_t>(row_src, 1))));
             bs.n_items = ((outp.h + bs.rows_per_item - 1) / bs.rows_per_item) * bs.n_chunks;
-            b->ring_stage_bytes = std::max(b->ring_stage_bytes, ws_slot_bytes(int64_t(bs.chunk_cols) * per_col));
+            // ring slots of about `ring_target` bytes: several source rows per
+            // slot when the chunk's rows are short
+            b->ring_stage_bytes =
+                std::max(b->ring_stage_bytes, launch::shrink_ring_setup(&bs.sh, bs.chunk_cols, b->ring_target));
             // the plain-load routine (unaligned sources) stages fv x fh source
             // pixels of at least one output column in the work region
             const int64_t edge = int64_t(bs.sh.fv) * per_col + p->bands + 64;

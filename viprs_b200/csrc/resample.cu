@@ -17,6 +17,7 @@
 // the (L2-resident) shrunk plane with coefficient tables in shared memory.
 #include <algorithm>
 #include <cstdio>
+#include <numeric>
 
 #include "resample_dev.cuh"
 
@@ -84,6 +85,50 @@ static void round_consts(uint32_t f, int bands, bool horizontal, int32_t* mode, 
     if (!horizontal) *mult = (uint32_t)*mult;
 }
 
+// The same rounding as (s * mul + add) >> 24 in 32 bits, exact for every box
+// sum s <= 255 f: factor 1 copies (mul 2^24), 2 rounds up a half (2^23, 2^23),
+// the ShrinkH factor-5 division is (s + 2) * ceil(2^24 / 5) >> 24, and the
+// multiplier rule ((s + f/2) * m) >> 24 distributes (its product stays below
+// 2^32 because m = floor(2^32 / (256 f))).
+static void round_consts32(uint32_t f, int32_t mode, uint32_t* mul, uint32_t* add) {
+    switch (mode) {
+    case 0: *mul = 1u << 24; *add = 0; break;
+    case 1: *mul = 1u << 23; *add = 1u << 23; break;
+    case 2: *mul = 3355444u; *add = 2u * 3355444u; break;
+    default: {
+        const uint32_t m = uint32_t((1ull << 32) / (256ull * f));
+        *mul = m;
+        *add = (f / 2) * m;
+    }
+    }
+}
+
+static void shrink_round_all(ShrinkArgs* a) {
+    round_consts(a->fh, a->bands, true, &a->hmode, &a->hmult);
+    round_consts(a->fv, a->bands, false, &a->vmode, &a->vmult);
+    round_consts32(a->fh, a->hmode, &a->hmul, &a->hadd);
+    round_consts32(a->fv, a->vmode, &a->vmul, &a->vadd);
+}
+
+uint32_t shrink_ring_setup(ShrinkArgs* a, int64_t chunk_cols, uint32_t slot_target) {
+    const int64_t per_col = int64_t(a->fh) * a->bands;
+    a->row_cap = ws_slot_bytes(chunk_cols * per_col);
+    int64_t r = int64_t(slot_target) / a->row_cap;
+    r = std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(r, int64_t(a->fv)), int64_t(kMaxSlotRows)));
+    a->slot_rows = int32_t(r);
+    // boxes a multiple of 4 bytes long start in the same bank for lanes
+    // 32 / g apart (g = gcd(box words, 32)): start those lanes' walks at
+    // different words
+    int shift = 5;
+    if (per_col % 4 == 0) {
+        int64_t g = std::gcd<int64_t>(per_col / 4, 32);
+        shift = 0;
+        while ((int64_t(32) >> shift) > g) ++shift;
+    }
+    a->rot_shift = shift;
+    return uint32_t(r * a->row_cap);
+}
+
 // Interior output columns [lo, hi): their source span lies inside the plane
 // and its 16-byte aligned cover lies inside the buffer for every row.
 static void interior_columns(const ShrinkArgs& a, int32_t* lo, int32_t* hi) {
@@ -104,29 +149,28 @@ static void interior_columns(const ShrinkArgs& a, int32_t* lo, int32_t* hi) {
 }
 
 void shrink_prepare(ShrinkArgs* a, int32_t* lo, int32_t* hi) {
-    round_consts(a->fh, a->bands, true, &a->hmode, &a->hmult);
-    round_consts(a->fv, a->bands, false, &a->vmode, &a->vmult);
+    shrink_round_all(a);
     interior_columns(*a, lo, hi);
 }
 
 cudaError_t shrink2d(ShrinkArgs a, cudaStream_t s) {
     if (a.out.w <= 0 || a.out.h <= 0) return cudaSuccess;
-    round_consts(a.fh, a.bands, true, &a.hmode, &a.hmult);
-    round_consts(a.fv, a.bands, false, &a.vmode, &a.vmult);
+    shrink_round_all(&a);
     if (a.fmt == kU8 && a.hv_order && (reinterpret_cast<uintptr_t>(a.in.data) & 15) == 0 && a.bands <= 4 &&
-        int64_t(a.fh) * a.bands <= 16384) {
+        int64_t(a.fh) * a.bands <= 8192) {
         // One consumer thread per output column of a chunk: the fewest chunks
         // (widest row segments, least per-row overhead), three ring slots of
-        // one row segment, and as many blocks per SM as fit -- the consumers
-        // are latency-bound, so resident warps set the rate.
+        // about 16 KB (several source rows each for narrow images), and as many
+        // blocks per SM as fit.
         const int64_t per_col = int64_t(a.fh) * a.bands;
         const int64_t chunks = std::max<int64_t>(1, (a.out.w + dev::kCThreads - 1) / dev::kCThreads);
         const int64_t nxf = (a.out.w + chunks - 1) / chunks;
         const int stages = 3;
-        const uint32_t stage_bytes = ws_slot_bytes(nxf * per_col);
-        void (*kern)(ShrinkArgs) = a.bands == 1 ? dev::shrink_hv_u8_ws<1, 1>
-                                  : a.bands == 2 ? dev::shrink_hv_u8_ws<2, 1>
-                                  : a.bands == 3 ? dev::shrink_hv_u8_ws<3, 1> : dev::shrink_hv_u8_ws<4, 1>;
+        ShrinkArgs f = a;
+        const uint32_t stage_bytes = shrink_ring_setup(&f, nxf, 16384);
+        void (*kern)(ShrinkArgs) = a.bands == 1 ? dev::shrink_hv_u8_ws<1>
+                                  : a.bands == 2 ? dev::shrink_hv_u8_ws<2>
+                                  : a.bands == 3 ? dev::shrink_hv_u8_ws<3> : dev::shrink_hv_u8_ws<4>;
         const size_t ctl = (sizeof(dev::WsRing) + 4 + 127) / 128 * 128;
         const size_t smem = ctl + size_t(stages) * stage_bytes;
         if (smem <= 200 * 1024 && int64_t(a.out.h) * chunks < (int64_t(1) << 30)) {
@@ -134,7 +178,6 @@ cudaError_t shrink2d(ShrinkArgs a, cudaStream_t s) {
             int bps = 0;
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, dev::kWsThreads, smem);
             bps = std::max(1, bps);
-            ShrinkArgs f = a;
             f.chunks = int32_t(chunks);
             f.nxf = int32_t(nxf);
             f.stages = stages;

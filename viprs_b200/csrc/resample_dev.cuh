@@ -247,74 +247,6 @@ __global__ void __launch_bounds__(kShrinkThreads) shrink2d_kernel(ShrinkArgs a) 
     }
 }
 
-// Box sums of one output pixel's fh source pixels (B bands, u8) from shared
-// memory at any byte alignment: words are realigned with a funnel shift and
-// the bands are summed four bytes at a time with dp4a masks.  Words go in
-// groups of G (3 for 3 bands: the band pattern repeats every 12 bytes, else 1);
-// the last group is masked to the box and may read up to 12 bytes past it (the
-// stage buffers carry 32 bytes of slack).  Alternate groups feed two sets of
-// accumulators, so the dp4a chains are half as long.
-template <int B>
-__device__ __forceinline__ void box_sums_u8(const uint8_t* p, int fh, uint32_t (&sums)[B]) {
-    constexpr int G = B == 3 ? 3 : 1;
-    const int o = int(reinterpret_cast<uintptr_t>(p) & 3);
-    const uint32_t* wp = reinterpret_cast<const uint32_t*>(p - o);
-    const int nbytes = fh * B;
-    const int K = (nbytes + 3) >> 2;             // realigned words, the last one partial
-    const int Kp = (K + G - 1) / G * G;          // whole groups
-    const uint32_t sh = 8u * uint32_t(o);
-    uint32_t sa[B], sb[B];
-#pragma unroll
-    for (int b = 0; b < B; ++b) { sa[b] = 0; sb[b] = 0; }
-    uint32_t lo = wp[0];
-    auto next = [&](int k) {
-        const uint32_t hi = wp[k + 1];
-        const uint32_t w = __funnelshift_r(lo, hi, sh);
-        lo = hi;
-        return w;
-    };
-    // word of phase `ph` within a group -> band sums
-    auto acc = [&](uint32_t (&s)[B], uint32_t w, int ph) {
-        if (B == 1) {
-            s[0] = __dp4a(w, 0x01010101u, s[0]);
-        } else if (B == 2) {
-            s[0] = __dp4a(w, 0x00010001u, s[0]);
-            s[1 % B] = __dp4a(w, 0x01000100u, s[1 % B]);
-        } else if (B == 3) {
-            const uint32_t m0 = ph == 0 ? 0x01000001u : (ph == 1 ? 0x00010000u : 0x00000100u);
-            const uint32_t m1 = ph == 0 ? 0x00000100u : (ph == 1 ? 0x01000001u : 0x00010000u);
-            const uint32_t m2 = ph == 0 ? 0x00010000u : (ph == 1 ? 0x00000100u : 0x01000001u);
-            s[0] = __dp4a(w, m0, s[0]);
-            s[1 % B] = __dp4a(w, m1, s[1 % B]);
-            s[2 % B] = __dp4a(w, m2, s[2 % B]);
-        } else {
-#pragma unroll
-            for (int b = 0; b < B; ++b) s[b] = __dp4a(w, 1u << (8 * b), s[b]);
-        }
-    };
-    int k = 0;
-    const int kfull = Kp - G;  // words before the (masked) last group
-    for (; k + 2 * G <= kfull; k += 2 * G) {
-#pragma unroll
-        for (int j = 0; j < G; ++j) acc(sa, next(k + j), j);
-#pragma unroll
-        for (int j = 0; j < G; ++j) acc(sb, next(k + G + j), j);
-    }
-    if (k < kfull) {
-#pragma unroll
-        for (int j = 0; j < G; ++j) acc(sa, next(k + j), j);
-        k += G;
-    }
-#pragma unroll
-    for (int j = 0; j < G; ++j) {
-        const int valid = nbytes - 4 * (k + j);
-        const uint32_t m = valid >= 4 ? 0xFFFFFFFFu : (valid <= 0 ? 0u : ((1u << (8 * valid)) - 1u));
-        acc(sb, next(k + j) & m, j);
-    }
-#pragma unroll
-    for (int b = 0; b < B; ++b) sums[b] = sa[b] + sb[b];
-}
-
 // Premultiply<U8> in place over `npx` staged pixels of B bands (alpha last).
 template <int B>
 __device__ __forceinline__ void premultiply_pixels(uint8_t* seg, int npx) {
@@ -370,28 +302,6 @@ __device__ void shrink_edge_item_u8(const ShrinkArgs& a, int32_t oy, int32_t c0,
     csync();
 }
 
-// Box sums of output pixels whose box leaves the plane (the reduce halo):
-// byte loads with columns clamped to the plane, from the staged span whose
-// first staged column is `c_lo`.
-template <int B>
-__device__ __forceinline__ void box_sums_clamped_u8(const uint8_t* span, int64_t first_col, int fh, int64_t c_lo,
-                                                    int64_t w, uint32_t (&sums)[B]) {
-#pragma unroll
-    for (int b = 0; b < B; ++b) sums[b] = 0;
-    for (int j = 0; j < fh; ++j) {
-        int64_t c = first_col + j;
-        c = c < 0 ? 0 : (c >= w ? w - 1 : c);
-        const uint8_t* px = span + (c - c_lo) * B;
-#pragma unroll
-        for (int b = 0; b < B; ++b) sums[b] += px[b];
-    }
-}
-
-// u8 ShrinkH rounding for the multiplier case without a mode switch.
-__device__ __forceinline__ uint32_t round_mult_u8(uint32_t sum, uint32_t half, uint64_t mult) {
-    return (uint32_t)(((unsigned long long)(sum + half) * mult) >> 24);
-}
-
 // Column chunk `c` of a shrink item: output columns [lx0, lx0 + ncols) and the
 // plane columns [s_lo, s_hi) its boxes read (clamped into the plane).
 struct ShrinkChunk {
@@ -416,15 +326,17 @@ __device__ __forceinline__ ShrinkChunk shrink_chunk(const ShrinkArgs& a, int32_t
 //
 // ShrinkH then ShrinkV over u8, streaming source row segments through a ring
 // of shared-memory slots.  A producer warp (thread kCThreads, one elected
-// thread) issues one TMA bulk copy (`cp.async.bulk`, no multicast) per source
-// row segment into the next free slot; eight consumer warps (threads 0..255)
-// each own one output pixel of the current column chunk and sum its box as
-// rows land.  Slots hand over through mbarriers only -- `full` (the copy's
+// thread) fills a slot with `slot_rows` consecutive source rows of the current
+// column chunk, one TMA bulk copy (`cp.async.bulk`, no multicast) per row, all
+// completing on the slot's `full` mbarrier; eight consumer warps (threads
+// 0..255) each own one output pixel of the chunk and add its box of every row
+// in the slot.  Slots hand over through mbarriers only -- `full` (the copies'
 // transaction bytes) and `empty` (one arrival per consumer warp) -- so there
-// is no block-wide barrier per row and the ring runs across item boundaries.
-// Every wait is bounded; a consumer that gives up stops waiting (and raises
-// `stop`), the producer stops issuing, and before it exits the producer waits
-// (bounded) for the copies it still has in flight.
+// is no block-wide barrier and the ring runs across item boundaries.  Several
+// rows per slot keep enough bytes in flight for narrow images and pay one
+// wait per slot.  Every wait is bounded; a consumer that gives up stops
+// waiting (and raises `stop`), the producer stops issuing, and before it
+// exits the producer waits (bounded) for the copies it still has in flight.
 
 constexpr int kWsThreads = kCThreads + 32;
 constexpr int kConsumerWarps = kCThreads / 32;
@@ -433,7 +345,7 @@ constexpr int kMaxRing = 16;
 struct WsRing {
     uint64_t full[kMaxRing];
     uint64_t empty[kMaxRing];
-    int32_t lead[kMaxRing];  // offset of the row's first byte within its slot
+    int32_t lead[kMaxRing][kMaxSlotRows];  // offset of each row's first byte within its row region
 };
 
 __device__ __forceinline__ void ws_ring_init(WsRing* r, int S) {
@@ -443,75 +355,124 @@ __device__ __forceinline__ void ws_ring_init(WsRing* r, int S) {
     }
 }
 
-// Producer: plane bytes [s0, s0 + n) -> slot `dst`, completing on `bar`.  The
-// 16-byte aligned cover goes by one bulk copy; bytes whose cover would pass
-// the end of the buffer go by plain loads first.  `lead` gets s0's offset in
-// the slot before the arrival publishes it.
-__device__ __forceinline__ void ws_issue_row(const uint8_t* base, int64_t total_bytes, int64_t s0, int64_t n,
-                                             uint8_t* dst, uint64_t* bar, int32_t* lead) {
-    const int64_t e0 = s0 + n;
-    const int64_t as = s0 & ~int64_t(15);
-    int64_t ae = (e0 + 15) & ~int64_t(15);
-    if (ae > total_bytes) {
-        const int64_t ab = e0 & ~int64_t(15);
-        for (int64_t q = ab > as ? ab : as; q < e0; ++q) dst[q - as] = base[q];
-        ae = ab > as ? ab : as;
-    }
-    *lead = int32_t(s0 - as);
-    fence_proxy_async_smem();
-    mbar_arrive_expect_tx(bar, uint32_t(ae - as));
-    if (ae > as) bulk_load(dst, base + as, uint32_t(ae - as), bar);
-}
-
 // Producer: wait (bounded) for the copies of the last min(issued, S) issues.
 __device__ __forceinline__ void ws_drain(WsRing* r, int S, int64_t issued) {
     const int64_t first = issued > S ? issued - S : 0;
     for (int64_t i = first; i < issued; ++i) mbar_wait(&r->full[int(i % S)], uint32_t((i / S) & 1));
 }
 
-// Box sums of fh premultiplied pixels (Premultiply<U8> applied to each source
-// pixel before the sum, as the separate Premultiply op would): 4 bands, any
-// byte alignment.  Bands 0 and 2 go through one multiply in 16-bit lanes:
-// c * a + 128 <= 65153 and t + (t >> 8) <= 65407 never carry into the next lane.
-__device__ __forceinline__ void box_sums_premul4_u8(const uint8_t* p, int fh, uint32_t (&sums)[4]) {
+// 32-bit rounding of a box sum: (s * mul + add) >> 24 reproduces every u8
+// rounding rule of ShrinkH / ShrinkV (shrinkh.rs:323-397, shrinkv.rs:191-339)
+// with host-computed constants, and never overflows (s <= 255 f).
+__device__ __forceinline__ uint32_t round_box(uint32_t s, uint32_t mul, uint32_t add) {
+    return (s * mul + add) >> 24;
+}
+
+// Box sums of one output pixel's fh source pixels (B bands, u8) from shared
+// memory at any byte alignment: words are realigned with a funnel shift and
+// the bands are summed four bytes at a time with dp4a masks.  Words go in
+// groups of G (3 for 3 bands: the band pattern repeats every 12 bytes, else
+// 1), starting at group q0 and wrapping around: lanes start at different
+// groups so that a warp's reads spread over the shared-memory banks even when
+// the lanes' boxes lie a multiple of 128 bytes apart.  The last group is
+// masked to the box and may read up to 16 bytes past it (row regions carry
+// 32 bytes of slack).
+template <int B>
+__device__ __forceinline__ void box_sums_rot_u8(const uint8_t* p, int fh, int q0, uint32_t (&sums)[B]) {
+    constexpr int G = B == 3 ? 3 : 1;
     const int o = int(reinterpret_cast<uintptr_t>(p) & 3);
     const uint32_t* wp = reinterpret_cast<const uint32_t*>(p - o);
+    const int nbytes = fh * B;
+    const int K = (nbytes + 3) >> 2;  // realigned words, the last one partial
+    const int Kg = (K + G - 1) / G;   // groups, the last one masked
     const uint32_t sh = 8u * uint32_t(o);
-    uint32_t lo = wp[0];
-    uint32_t s0 = 0, s2 = 0, s1 = 0, s3 = 0;
-    // one premultiplied pixel into the packed (bands 0, 2) sum and the band-1 sum
-    auto pix = [&](uint32_t w, uint32_t& s02, uint32_t& s1x) {
-        const uint32_t al = w >> 24;
-        const uint32_t t02 = (w & 0x00FF00FFu) * al + 0x00800080u;
-        s02 += ((t02 + ((t02 >> 8) & 0x00FF00FFu)) >> 8) & 0x00FF00FFu;
-        const uint32_t t1 = ((w >> 8) & 0xFFu) * al + 128u;
-        s1x += (t1 + (t1 >> 8)) >> 8;
-        s3 += al;
+    uint32_t sa[B], sb[B];
+#pragma unroll
+    for (int b = 0; b < B; ++b) { sa[b] = 0; sb[b] = 0; }
+    // realigned word of phase `ph` within a group -> band sums
+    auto acc = [&](uint32_t (&s)[B], uint32_t w, int ph) {
+        if (B == 1) {
+            s[0] = __dp4a(w, 0x01010101u, s[0]);
+        } else if (B == 2) {
+            s[0] = __dp4a(w, 0x00010001u, s[0]);
+            s[1 % B] = __dp4a(w, 0x01000100u, s[1 % B]);
+        } else if (B == 3) {
+            const uint32_t m0 = ph == 0 ? 0x01000001u : (ph == 1 ? 0x00010000u : 0x00000100u);
+            const uint32_t m1 = ph == 0 ? 0x00000100u : (ph == 1 ? 0x01000001u : 0x00010000u);
+            const uint32_t m2 = ph == 0 ? 0x00010000u : (ph == 1 ? 0x00000100u : 0x01000001u);
+            s[0] = __dp4a(w, m0, s[0]);
+            s[1 % B] = __dp4a(w, m1, s[1 % B]);
+            s[2 % B] = __dp4a(w, m2, s[2 % B]);
+        } else {
+#pragma unroll
+            for (int b = 0; b < B; ++b) s[b] = __dp4a(w, 1u << (8 * b), s[b]);
+        }
     };
-    for (int j0 = 0; j0 < fh; j0 += 256) {  // each 16-bit lane holds at most 256 x 255
-        const int j1 = min(fh, j0 + 256);
-        uint32_t a02 = 0, b02 = 0, a1 = 0, b1 = 0;
-        int j = j0;
-        for (; j + 2 <= j1; j += 2) {
-            uint32_t hi = wp[j + 1];
-            const uint32_t w0 = __funnelshift_r(lo, hi, sh);
-            lo = hi;
-            hi = wp[j + 2];
-            const uint32_t w1 = __funnelshift_r(lo, hi, sh);
-            lo = hi;
-            pix(w0, a02, a1);
-            pix(w1, b02, b1);
+    // unmasked groups [g0, g1): two accumulator sets halve the dp4a chains
+    auto run = [&](int g0, int g1) {
+        if (g0 >= g1) return;
+        int k = g0 * G;
+        uint32_t lo = wp[k];
+        int g = g0;
+        for (; g + 2 <= g1; g += 2, k += 2 * G) {
+#pragma unroll
+            for (int j = 0; j < G; ++j) {
+                const uint32_t hi = wp[k + j + 1];
+                acc(sa, __funnelshift_r(lo, hi, sh), j);
+                lo = hi;
+            }
+#pragma unroll
+            for (int j = 0; j < G; ++j) {
+                const uint32_t hi = wp[k + G + j + 1];
+                acc(sb, __funnelshift_r(lo, hi, sh), j);
+                lo = hi;
+            }
         }
-        if (j < j1) {
-            const uint32_t hi = wp[j + 1];
-            const uint32_t w0 = __funnelshift_r(lo, hi, sh);
-            lo = hi;
-            pix(w0, a02, a1);
+        if (g < g1) {
+#pragma unroll
+            for (int j = 0; j < G; ++j) {
+                const uint32_t hi = wp[k + j + 1];
+                acc(sa, __funnelshift_r(lo, hi, sh), j);
+                lo = hi;
+            }
         }
-        s0 += (a02 & 0xFFFFu) + (b02 & 0xFFFFu);
-        s2 += (a02 >> 16) + (b02 >> 16);
-        s1 += a1 + b1;
+    };
+    run(q0, Kg - 1);
+    {
+        const int k = (Kg - 1) * G;
+        uint32_t lo = wp[k];
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+            const uint32_t hi = wp[k + j + 1];
+            const int valid = nbytes - 4 * (k + j);
+            const uint32_t m = valid >= 4 ? 0xFFFFFFFFu : (valid <= 0 ? 0u : ((1u << (8 * valid)) - 1u));
+            acc(sb, __funnelshift_r(lo, hi, sh) & m, j);
+            lo = hi;
+        }
     }
+    run(0, q0);
+#pragma unroll
+    for (int b = 0; b < B; ++b) sums[b] = sa[b] + sb[b];
+}
+
+// Premultiplied box sums of fh 4-band pixels (Premultiply<U8> applied to each
+// source pixel before the sum, as the separate Premultiply op would), from a
+// 4-byte aligned box, pixels in the order q0 .. fh-1, 0 .. q0-1 (bank spread).
+// premultiply_u8(c, a) = (t + (t >> 8)) >> 8 with t = c a + 128 equals
+// (c (257 a) + 32896) >> 16 for every c, a in 0..255 (t < 65536).
+__device__ __forceinline__ void box_sums_premul4_rot(const uint8_t* p, int fh, int q0, uint32_t (&sums)[4]) {
+    const uint32_t* wp = reinterpret_cast<const uint32_t*>(p);
+    uint32_t s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    auto pix = [&](uint32_t w) {
+        const uint32_t a = w >> 24;
+        const uint32_t a257 = a * 257u;
+        s0 += (__byte_perm(w, 0u, 0x4440) * a257 + 32896u) >> 16;
+        s1 += (__byte_perm(w, 0u, 0x4441) * a257 + 32896u) >> 16;
+        s2 += (__byte_perm(w, 0u, 0x4442) * a257 + 32896u) >> 16;
+        s3 += a;
+    };
+    for (int j = q0; j < fh; ++j) pix(wp[j]);
+    for (int j = 0; j < q0; ++j) pix(wp[j]);
     sums[0] = s0;
     sums[1] = s1;
     sums[2] = s2;
@@ -548,115 +509,135 @@ __device__ __forceinline__ void box_sums_premul2_u8(const uint8_t* p, int fh, ui
     sums[1] = s1;
 }
 
-// Box sums of one output pixel from the staged span (inside or clamped box,
-// premultiplied or not).
-template <int B>
-__device__ __forceinline__ void ws_box(const ShrinkArgs& a, const uint8_t* span, int64_t s_lo, int64_t fcol,
-                                       bool inside, bool premul, uint32_t (&sums)[B]) {
-    const int fh = int(a.fh);
-    const uint8_t* box = span + (fcol - s_lo) * B;
-    if (!inside) {
-        box_sums_clamped_pm_u8<B>(span, fcol, fh, s_lo, a.in.w, premul, sums);
-    } else if (premul) {
-        if constexpr (B == 4) box_sums_premul4_u8(box, fh, sums);
-        else if constexpr (B == 2) box_sums_premul2_u8(box, fh, sums);
-        else box_sums_u8<B>(box, fh, sums);
-    } else {
-        box_sums_u8<B>(box, fh, sums);
-    }
+// Start group of this lane's box walk: lanes whose boxes start in the same
+// bank start (lane >> rot_shift) groups apart.
+__device__ __forceinline__ int ws_rot_group(const ShrinkArgs& a, int B) {
+    const int G = B == 3 ? 3 : 1;
+    const int K = (int(a.fh) * B + 3) >> 2;
+    const int Kg = (K + G - 1) / G;
+    const int r = (threadIdx.x & 31) >> a.rot_shift;
+    return (B == 4 && a.premul_in) ? (r % int(a.fh)) : (r % Kg);
 }
 
-// Consumers: output rows [oy0, oy1) of column chunk `c`, whose (oy1 - oy0) * fv
-// source row segments arrive in ring order starting at (slot, ph).  Thread x
-// owns output pixels c.lx0 + x + kCThreads * j, j < P (P pixels per thread
-// share the per-row wait, release and addressing).  Returns false once `stop`
-// is raised.
-template <int B, int P>
+// Consumers: output rows [oy0, oy1) of column chunk `c`, whose source rows
+// arrive slot_rows at a time in ring order starting at (slot, ph).  Thread x
+// owns output pixel c.lx0 + x.  Returns false once `stop` is raised.
+template <int B>
 __device__ bool ws_consume(const ShrinkArgs& a, int32_t oy0, int32_t oy1, const ShrinkChunk& c, WsRing* ring,
                            const uint8_t* bufs, uint32_t stage_bytes, int S, int& slot, uint32_t& ph,
                            volatile int32_t* stop) {
-    const int32_t fh = int32_t(a.fh), fv = int32_t(a.fv);
+    const int32_t fh = int32_t(a.fh), fv = int32_t(a.fv), R = a.slot_rows;
+    const uint32_t cap = a.row_cap;
     const int x = threadIdx.x, lane = x & 31;
-    bool mine[P], inside[P];
-    int64_t fcol[P];
-#pragma unroll
-    for (int j = 0; j < P; ++j) {
-        const int px = x + kCThreads * j;
-        mine[j] = px < c.ncols;
-        fcol[j] = (a.out.x0 + c.lx0 + px) * (int64_t)fh - a.in.x0;
-        inside[j] = fcol[j] >= 0 && fcol[j] + fh <= a.in.w;
-    }
-    const bool any = mine[0];
+    const bool mine = x < c.ncols;
+    const int64_t fcol = (a.out.x0 + c.lx0 + x) * (int64_t)fh - a.in.x0;
+    const bool inside = fcol >= 0 && fcol + fh <= a.in.w;
+    const int32_t off = inside ? int32_t(fcol - c.s_lo) * B : 0;
     const bool premul = a.premul_in != 0;
-    const uint32_t hhalf = uint32_t(fh) / 2;
-    const bool hmult = a.hmode == 3;
+    const int q0 = ws_rot_group(a, B);
     for (int32_t oy = oy0; oy < oy1; ++oy) {
-        uint32_t vacc[P][B];
+        uint32_t vacc[B];
 #pragma unroll
-        for (int j = 0; j < P; ++j)
-#pragma unroll
-            for (int b = 0; b < B; ++b) vacc[j][b] = 0;
-        for (int32_t k = 0; k < fv; ++k) {
+        for (int b = 0; b < B; ++b) vacc[b] = 0;
+        for (int32_t k0 = 0; k0 < fv; k0 += R) {
+            const int32_t rr = min(R, fv - k0);
             bool live = *stop == 0;
             if (live && !mbar_wait(&ring->full[slot], ph)) {
                 *stop = 1;
                 live = false;
             }
-            if (live && any) {
-                const uint8_t* span = bufs + (size_t)slot * stage_bytes + ring->lead[slot];
-#pragma unroll
-                for (int j = 0; j < P; ++j) {
-                    if (!mine[j]) continue;
+            if (live && mine) {
+                const uint8_t* sb = bufs + (size_t)slot * stage_bytes;
+                const int32_t* leads = ring->lead[slot];
+                for (int32_t r = 0; r < rr; ++r) {
+                    const uint8_t* span = sb + r * cap + leads[r];
                     uint32_t sums[B];
-                    ws_box<B>(a, span, c.s_lo, fcol[j], inside[j], premul, sums);
-                    if (hmult) {
-#pragma unroll
-                        for (int b = 0; b < B; ++b) vacc[j][b] += round_mult_u8(sums[b], hhalf, a.hmult);
+                    if (!inside) {
+                        box_sums_clamped_pm_u8<B>(span, fcol, fh, c.s_lo, a.in.w, premul, sums);
+                    } else if (premul && B == 4) {
+                        box_sums_premul4_rot(span + off, fh, q0, *reinterpret_cast<uint32_t(*)[4]>(sums));
+                    } else if (premul && B == 2) {
+                        box_sums_premul2_u8(span + off, fh, *reinterpret_cast<uint32_t(*)[2]>(sums));
                     } else {
-#pragma unroll
-                        for (int b = 0; b < B; ++b) vacc[j][b] += round_mode_u8(sums[b], a.hmode, uint32_t(fh), a.hmult);
+                        box_sums_rot_u8<B>(span + off, fh, q0, sums);
                     }
+#pragma unroll
+                    for (int b = 0; b < B; ++b) vacc[b] += round_box(sums[b], a.hmul, a.hadd);
                 }
             }
             __syncwarp();
             if (live && lane == 0) mbar_arrive(&ring->empty[slot]);
             if (++slot == S) { slot = 0; ph ^= 1u; }
         }
-        if (*stop == 0) {
+        if (*stop == 0 && mine) {
+            uint32_t o[B];
 #pragma unroll
-            for (int j = 0; j < P; ++j) {
-                if (!mine[j]) continue;
-                uint8_t o[B];
+            for (int b = 0; b < B; ++b) o[b] = round_box(vacc[b], a.vmul, a.vadd);
+            if (a.unpremul_out) {
 #pragma unroll
-                for (int b = 0; b < B; ++b) o[b] = (uint8_t)round_mode_u8(vacc[j][b], a.vmode, uint32_t(fv), a.vmult);
-                if (a.unpremul_out) {
+                for (int b = 0; b < B - 1; ++b) o[b] = unpremultiply_u8(o[b], o[B - 1]);
+            }
+            uint8_t* dst = a.out.data + (int64_t)oy * a.out.pitch + (int64_t)(c.lx0 + x) * B;
+            if (B == 4 && (reinterpret_cast<uintptr_t>(dst) & 3) == 0) {
+                *reinterpret_cast<uint32_t*>(dst) = o[0] | (o[1 % B] << 8) | (o[2 % B] << 16) | (o[3 % B] << 24);
+            } else {
 #pragma unroll
-                    for (int b = 0; b < B - 1; ++b) o[b] = (uint8_t)unpremultiply_u8(o[b], o[B - 1]);
-                }
-                uint8_t* dst = a.out.data + (int64_t)oy * a.out.pitch + (int64_t)(c.lx0 + x + kCThreads * j) * B;
-#pragma unroll
-                for (int b = 0; b < B; ++b) dst[b] = o[b];
+                for (int b = 0; b < B; ++b) dst[b] = uint8_t(o[b]);
             }
         }
     }
     return *stop == 0;
 }
 
-// Producer: issue the source rows of output rows [oy0, oy1) of chunk `c`.
-// Returns false if a slot never came free.
+// Producer: issue the source rows of output rows [oy0, oy1) of chunk `c`,
+// slot_rows per slot.  Per row the 16-byte aligned cover of its segment goes
+// by one bulk copy into the row's region of the slot; bytes whose cover would
+// pass the end of the buffer go by plain loads first.  Returns false if a slot
+// never came free.
 template <int B>
 __device__ bool ws_produce(const ShrinkArgs& a, const uint8_t* in_data, int32_t oy0, int32_t oy1,
                            const ShrinkChunk& c, WsRing* ring, uint8_t* bufs, uint32_t stage_bytes, int S,
                            int& slot, uint32_t& ph, int64_t& issued) {
-    const int32_t fv = int32_t(a.fv);
+    const int32_t fv = int32_t(a.fv), R = a.slot_rows;
+    const uint32_t cap = a.row_cap;
     const int64_t n = (c.s_hi - c.s_lo) * B;
+    const int64_t total = a.in.total_bytes;
     for (int32_t oy = oy0; oy < oy1; ++oy) {
-        for (int32_t k = 0; k < fv; ++k) {
+        for (int32_t k0 = 0; k0 < fv; k0 += R) {
+            const int32_t rr = min(R, fv - k0);
             if (!mbar_wait(&ring->empty[slot], ph ^ 1u)) return false;
-            int64_t ly = (a.out.y0 + oy) * (int64_t)fv + k - a.in.y0;
-            ly = ly < 0 ? 0 : (ly >= a.in.h ? a.in.h - 1 : ly);
-            ws_issue_row(in_data, a.in.total_bytes, ly * a.in.pitch + c.s_lo * B, n, bufs + (size_t)slot * stage_bytes,
-                         &ring->full[slot], &ring->lead[slot]);
+            uint8_t* dst = bufs + (size_t)slot * stage_bytes;
+            const int64_t ly0 = (a.out.y0 + oy) * (int64_t)fv + k0 - a.in.y0;
+            uint32_t tx = 0;
+            for (int32_t r = 0; r < rr; ++r) {
+                int64_t ly = ly0 + r;
+                ly = ly < 0 ? 0 : (ly >= a.in.h ? a.in.h - 1 : ly);
+                const int64_t s0 = ly * a.in.pitch + c.s_lo * B, e0 = s0 + n;
+                const int64_t as = s0 & ~int64_t(15);
+                int64_t ae = (e0 + 15) & ~int64_t(15);
+                if (ae > total) {
+                    const int64_t ab = e0 & ~int64_t(15);
+                    uint8_t* d = dst + (size_t)r * cap;
+                    for (int64_t q = ab > as ? ab : as; q < e0; ++q) d[q - as] = in_data[q];
+                    ae = ab > as ? ab : as;
+                }
+                ring->lead[slot][r] = int32_t(s0 - as);
+                tx += uint32_t(ae - as);
+            }
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(&ring->full[slot], tx);
+            for (int32_t r = 0; r < rr; ++r) {
+                int64_t ly = ly0 + r;
+                ly = ly < 0 ? 0 : (ly >= a.in.h ? a.in.h - 1 : ly);
+                const int64_t s0 = ly * a.in.pitch + c.s_lo * B, e0 = s0 + n;
+                const int64_t as = s0 & ~int64_t(15);
+                int64_t ae = (e0 + 15) & ~int64_t(15);
+                if (ae > total) {
+                    const int64_t ab = e0 & ~int64_t(15);
+                    ae = ab > as ? ab : as;
+                }
+                if (ae > as) bulk_load(dst + (size_t)r * cap, in_data + as, uint32_t(ae - as), &ring->full[slot]);
+            }
             ++issued;
             if (++slot == S) { slot = 0; ph ^= 1u; }
         }
@@ -665,11 +646,11 @@ __device__ bool ws_produce(const ShrinkArgs& a, const uint8_t* in_data, int32_t 
 }
 
 // Standalone ShrinkH+ShrinkV (u8, B bands, source 16-byte aligned).  Items are
-// (output row, column chunk); the chunks partition the output columns and
-// block b owns items b, b + G, ...  The host picks the chunk count, ring depth
-// and blocks per SM (makespan model over the resident grid).
-template <int B, int P>
-__global__ void __launch_bounds__(kWsThreads, 5) shrink_hv_u8_ws(ShrinkArgs a) {
+// (band of output rows, column chunk); the chunks partition the output columns and
+// block b owns items b, b + G, ...  The host picks the chunk count, ring depth,
+// rows per slot and blocks per SM.
+template <int B>
+__global__ void __launch_bounds__(kWsThreads, 4) shrink_hv_u8_ws(ShrinkArgs a) {
     extern __shared__ __align__(128) uint8_t smem_ws[];
     WsRing* ring = reinterpret_cast<WsRing*>(smem_ws);
     volatile int32_t* stop = reinterpret_cast<volatile int32_t*>(smem_ws + sizeof(WsRing));
@@ -708,7 +689,7 @@ __global__ void __launch_bounds__(kWsThreads, 5) shrink_hv_u8_ws(ShrinkArgs a) {
         const int32_t band = item / chunks;
         const ShrinkChunk c = shrink_chunk(a, item - band * chunks);
         const int32_t oy0 = band * rpi, oy1 = min(a.out.h, oy0 + rpi);
-        if (!ws_consume<B, P>(a, oy0, oy1, c, ring, bufs, a.stage_bytes, S, slot, ph, stop)) {
+        if (!ws_consume<B>(a, oy0, oy1, c, ring, bufs, a.stage_bytes, S, slot, ph, stop)) {
             if (threadIdx.x == 0 && a.err) atomicExch(a.err, VIPRS_ERR_TIMEOUT);
             break;
         }
