@@ -208,7 +208,11 @@ def test_affine_adjoint_identity(geom, extend, bands):
     gd, _ = _affine_grad_raw(xt, gy, bm, bt, extend, bg, premul, det=True)
     gd2, _ = _affine_grad_raw(xt, gy, bm, bt, extend, bg, premul, det=True)
     assert torch.equal(gd, gd2), "deterministic scatter differs between runs"
-    assert normwise(host(gd), host(gx)) <= 1e-6
+    # the deterministic (2^-32 fixed-point) scatter satisfies the identity on its own
+    assert identity_err(lhs, dot(x, host(gd)), host(y) - host(y0), host(gy)) <= RTOL_IDENTITY
+    # f32 atomics add a pixel's (up to 16) contributions in a varying order:
+    # agreement within a few f32 ulps of the largest gradient
+    assert normwise(host(gd), host(gx)) <= 1e-5
 
 
 def _affine_fd_case(bands, seed):
@@ -354,7 +358,8 @@ def test_mapim_adjoint_identity(kernel, extend_copy, bands):
     assert identity_err(lhs, dot(src, host(ga)), host(y) - host(y0), host(gy)) <= RTOL_IDENTITY
     gd, gd2 = grad(True), grad(True)
     assert torch.equal(gd, gd2), "deterministic scatter differs between runs"
-    assert normwise(host(gd), host(ga)) <= 1e-6
+    assert identity_err(lhs, dot(src, host(gd)), host(y) - host(y0), host(gy)) <= RTOL_IDENTITY
+    assert normwise(host(gd), host(ga)) <= 1e-5
 
 
 @pytest.mark.parametrize("kernel", ["nearest", "bilinear", "bicubic", "lanczos3"])
@@ -389,7 +394,8 @@ def test_mapim_grad_smooth_field(kernel, extend_copy, bands):
     assert identity_err(lhs, dot(src, host(ga)), host(y) - host(y0), host(gy)) <= RTOL_IDENTITY
     gd, gd2 = grad(True), grad(True)
     assert torch.equal(gd, gd2), "deterministic scatter differs between runs"
-    assert normwise(host(gd), host(ga)) <= 1e-6
+    assert identity_err(lhs, dot(src, host(gd)), host(y) - host(y0), host(gy)) <= RTOL_IDENTITY
+    assert normwise(host(gd), host(ga)) <= 1e-5
 
 
 @pytest.mark.parametrize("kernel", ["bilinear", "bicubic", "quadratic", "lanczos2", "lanczos3"])

@@ -55,20 +55,25 @@ struct BatchArgs {
     int32_t* err = nullptr;       // first error (timeout) seen by any block
     const uint64_t* srcs = nullptr;  // device array: source pointer of each image
     const uint64_t* dsts = nullptr;  // device array: destination pointer of each image
-    uint32_t ring_stage_bytes = 0;   // bytes of one shrink ring slot
-    int32_t ring_slots = 0;          // slots of the shrink ring
+    uint32_t ring_stage_bytes = 0;   // bytes of one stage buffer of a shrink warp
+    int32_t ring_slots = 0;          // unused by the warp shrink
     uint32_t work_bytes = 0;         // shared memory of the other item kinds
     uint32_t smem_bytes = 0;         // control block + stage copy + ring + work
 };
 
 namespace launch {
-// Launch the persistent kernel on `grid` blocks: the shrink-ring variant
-// (`ring`) or the variant for the other item kinds.
+// Launch the persistent kernel on `grid` blocks: the shrink variant
+// (`ring`: independent warps, each with its own stage buffers of
+// a.ring_stage_bytes) or the variant for the other item kinds.
 cudaError_t batch(const BatchArgs& a, int grid, bool ring, cudaStream_t s);
 // Largest resident block count per SM for `smem` bytes of shared memory.
 int batch_blocks_per_sm(size_t smem, bool ring);
-// Shared memory ahead of the ring: control block and the item's stage copy.
+// Shared memory of the other item kinds' variant ahead of its work region:
+// control block and the queued stage copies.
 size_t batch_ctl_bytes();
+// Shared memory of a shrink launch whose warps have stage buffers of
+// `stage_bytes` (a stage descriptor and the buffers per warp).
+size_t batch_warp_smem_bytes(uint32_t stage_bytes);
 }  // namespace launch
 
 }  // namespace viprs

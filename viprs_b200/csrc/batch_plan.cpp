@@ -17,6 +17,7 @@
 
 #include "batch_launch.hpp"
 #include "chain.hpp"
+#include "shrink_warp.hpp"
 #include "viprs_b200.h"
 
 using namespace viprs;
@@ -36,12 +37,11 @@ struct viprs_batch {
     std::vector<uint32_t> w, h, bands;
     std::vector<viprs_plan*> plans;
     // knobs (autotuned)
-    uint32_t ring_target = 8192;  // source bytes per shrink row segment
-    int32_t ring_slots_knob = 0;  // ring slots per block (0: ring_total / slot size)
+    uint32_t ring_target = 2048;  // bytes of one shrink warp's stage buffer (source row segment)
+    int32_t ring_slots_knob = 0;  // kept for the configuration API; the warp shrink ignores it
     int32_t blocks_per_sm = 0;    // cap of the shrink launches (0 = occupancy maximum)
     uint32_t reduce_smem_budget = 40 * 1024;  // shared memory of one fused-reduce tile
-    int64_t item_bytes = 256 * 1024;          // source bytes per shrink work item
-    uint32_t ring_total = 56 * 1024;          // shrink ring bytes per block (auto slots)
+    int64_t item_bytes = 48 * 1024;           // source bytes per shrink work item
     // device work list
     std::vector<BatchStage> stages;
     std::vector<WorkItem> items;
@@ -52,7 +52,6 @@ struct viprs_batch {
     int32_t* d_ctrl = nullptr;  // [0] error, [1 + k] cursor of launch k
     size_t counters_cap = 0, stages_cap = 0, items_cap = 0;
     uint32_t ring_stage_bytes = 0;
-    size_t edge_bytes = 0;
     // captured graph
     cudaGraphExec_t graph = nullptr;
     const uint64_t* graph_srcs = nullptr;
@@ -107,28 +106,11 @@ int plan_stages(viprs_batch* b, int image, std::vector<std::vector<BatchStage>>*
             int32_t lo, hi;
             launch::shrink_prepare(&bs.sh, &lo, &hi);
             bs.lo = lo; bs.hi = hi;
-            // column chunks partition the output columns (clamped boxes at the
-            // edges, as in the standalone kernel); one consumer thread per column
-            const int64_t per_col = int64_t(bs.sh.fh) * p->bands;
-            // at most one column per consumer thread and `ring_target` source
-            // bytes per row segment; balanced chunk widths
-            const int64_t cap = std::max<int64_t>(1, std::min<int64_t>(256, b->ring_target / std::max<int64_t>(per_col, 1)));
-            const int64_t nch = (outp.w + cap - 1) / cap;
-            bs.chunk_cols = int32_t(std::max<int64_t>(1, (outp.w + nch - 1) / nch));
-            bs.sh.nxf = bs.chunk_cols;
-            bs.n_chunks = (outp.w + bs.chunk_cols - 1) / bs.chunk_cols;
-            // output rows per item: about `item_bytes` of source per item
-            const int64_t row_src = int64_t(bs.chunk_cols) * per_col * bs.sh.fv;
-            bs.rows_per_item = int32_t(std::max<int64_t>(1, std::min<int64_t>(outp.h, b->item_bytes / std::max<int64_t>(row_src, 1))));
-            bs.n_items = ((outp.h + bs.rows_per_item - 1) / bs.rows_per_item) * bs.n_chunks;
-            // ring slots of about `ring_target` bytes: several source rows per
-            // slot when the chunk's rows are short
-            b->ring_stage_bytes =
-                std::max(b->ring_stage_bytes, launch::shrink_ring_setup(&bs.sh, bs.chunk_cols, b->ring_target));
-            // the plain-load routine (unaligned sources) stages fv x fh source
-            // pixels of at least one output column in the work region
-            const int64_t edge = int64_t(bs.sh.fv) * per_col + p->bands + 64;
-            b->edge_bytes = std::max<size_t>(b->edge_bytes, size_t(edge + 64));
+            // independent warps: pixels per warp, stage buffers of at most
+            // `ring_target` bytes, about `item_bytes` of source per item
+            if (!launch::shrink_warp_setup(&bs.sh, b->ring_target, b->item_bytes)) return VIPRS_ERR_INVALID_ARGUMENT;
+            bs.n_items = int32_t(launch::shrink_warp_items(bs.sh));
+            b->ring_stage_bytes = std::max(b->ring_stage_bytes, bs.sh.row_cap);
             break;
         }
         case StageType::Reduce2D: {
@@ -209,16 +191,12 @@ size_t reduce2d_need(const Reduce2DArgs& a) { return launch::reduce2d_smem_bytes
 // order in the stream is the whole dependency structure: no item waits.
 int build_list(viprs_batch* b) {
     b->ring_stage_bytes = 0;
-    b->edge_bytes = 0;
     std::vector<std::vector<BatchStage>> per(size_t(b->n));
     for (int i = 0; i < b->n; ++i) {
         const int st = plan_stages(b, i, &per);
         if (st) return st;
     }
     b->ring_stage_bytes = std::max<uint32_t>(b->ring_stage_bytes, 256);
-    const int32_t ring_slots = b->ring_slots_knob > 0
-        ? std::min(b->ring_slots_knob, 16)
-        : int32_t(std::min<int64_t>(16, std::max<int64_t>(3, int64_t(b->ring_total) / b->ring_stage_bytes)));
 
     // flatten the stages; levels
     b->stages.clear();
@@ -259,8 +237,8 @@ int build_list(viprs_batch* b) {
                     const BatchStage& s = b->stages[size_t(g)];
                     if ((s.type == kBatchShrink) != ring) continue;
                     for (int32_t k = 0; k < s.n_items; ++k) b->items.push_back(WorkItem{g, k});
-                    if (s.type == kBatchShrink) work = std::max(work, b->edge_bytes);
-                    else if (s.type == kBatchReduce2D) work = std::max(work, reduce2d_need(s.r2));
+                    if (s.type == kBatchShrink) continue;
+                    if (s.type == kBatchReduce2D) work = std::max(work, reduce2d_need(s.r2));
                     else if (s.type == kBatchReduceH || s.type == kBatchReduceV)
                         work = std::max(work, size_t(65 * s.rd.taps * 2 + 15) / 16 * 16 + 256);
                     else work = std::max<size_t>(work, 1024);
@@ -270,8 +248,8 @@ int build_list(viprs_batch* b) {
             if (l.count == 0) continue;
             if (int(b->launches.size()) >= kMaxLaunches) return VIPRS_ERR_UNSUPPORTED_FORMAT;
             l.work_bytes = uint32_t((std::max<size_t>(work, 256) + 127) / 128 * 128);
-            l.ring_slots = ring ? ring_slots : 0;
-            l.smem = ctl + size_t(l.ring_slots) * b->ring_stage_bytes + l.work_bytes;
+            l.ring_slots = 0;
+            l.smem = ring ? launch::batch_warp_smem_bytes(b->ring_stage_bytes) : ctl + l.work_bytes;
             if (l.smem > 220 * 1024) return VIPRS_ERR_INVALID_ARGUMENT;
             int per_sm = launch::batch_blocks_per_sm(l.smem, ring);
             if (per_sm <= 0) return VIPRS_ERR_INVALID_ARGUMENT;
@@ -433,7 +411,7 @@ int32_t viprs_batch_launch_count(const viprs_batch* b, int32_t* batched, int32_t
 
 int32_t viprs_batch_set_config(viprs_batch* b, uint32_t ring_bytes, int32_t ring_slots, int32_t blocks_per_sm) {
     if (!b) return VIPRS_ERR_NULL_POINTER;
-    if (ring_bytes < 256 || ring_bytes > 32768 || ring_slots < 0 || ring_slots > 16 || blocks_per_sm < 0)
+    if (ring_bytes < 1024 || ring_bytes > 32768 || ring_slots < 0 || ring_slots > 16 || blocks_per_sm < 0)
         return VIPRS_ERR_INVALID_ARGUMENT;
     b->ring_target = ring_bytes;
     b->ring_slots_knob = ring_slots;
@@ -454,8 +432,8 @@ int32_t viprs_batch_autotune(viprs_batch* b, const uint64_t* d_srcs, const uint6
                              int32_t repeats, float* best_ms) {
     if (!b || !d_srcs || !d_dsts) return VIPRS_ERR_NULL_POINTER;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const uint32_t rings[] = {8192, 12288, 16384, 24576};
-    const int32_t lags[] = {0, 3, 4, 6};  // ring slots (0: from the ring budget)
+    const uint32_t rings[] = {1536, 2048, 3072, 4096};  // warp stage buffer bytes
+    const int32_t lags[] = {0};
     const int32_t caps[] = {0, 2, 3};
     float best = 1e30f;
     uint32_t br = b->ring_target;

@@ -45,14 +45,12 @@ struct ShrinkArgs {
     uint64_t hmult = 0, vmult = 0;
     // the same roundings as one 32-bit multiply-add: round(s) = (s * mul + add) >> 24
     uint32_t hmul = 0, hadd = 0, vmul = 0, vadd = 0;
-    // bulk-copy pipeline (u8, ShrinkH then ShrinkV): column chunks of nxf
-    // outputs, output rows per item, ring slots of stage_bytes holding
-    // slot_rows source row segments of row_cap bytes each
-    int32_t chunks = 0, nxf = 0, stages = 0, rows_per_item = 1;
-    uint32_t stage_bytes = 0;
-    int32_t slot_rows = 1;
+    // warp shrink (u8, ShrinkH then ShrinkV; shrink_warp.cuh): nxf output
+    // pixels per warp, rows_per_item output rows per work item, stage buffers
+    // of row_cap bytes, box walks rotated by (lane >> rot_shift) groups
+    int32_t nxf = 0, rows_per_item = 1;
     uint32_t row_cap = 0;
-    int32_t rot_shift = 5;     // box word order rotated by (lane >> rot_shift) groups
+    int32_t rot_shift = 5;
     int32_t* err = nullptr;    // device error word (timeout), may be null
 };
 
@@ -116,9 +114,7 @@ struct Reduce2DArgs {
 // segment sits at its plane offset mod 16 within the slot (the 16-byte aligned
 // cover is copied), with 32 bytes of slack after it for the box sums'
 // over-read.
-VIPRS_HD inline uint32_t ws_slot_bytes(int64_t n) { return uint32_t((n + 15 + 32 + 127) / 128 * 128); }
-// Most source rows one ring slot holds.
-constexpr int32_t kMaxSlotRows = 32;
+
 
 // Shared-memory layout of one fused-reduce tile (byte offsets, 16-aligned):
 // both coefficient tables, the tile's start/phase tables, one offset per
@@ -178,12 +174,6 @@ size_t shrink2d_smem_bytes(const ShrinkArgs& a, int32_t* nx);
 // Set the u8 rounding constants of `a` and return its interior output columns
 // [lo, hi) (source boxes inside the plane, aligned spans inside the buffer).
 void shrink_prepare(ShrinkArgs* a, int32_t* lo, int32_t* hi);
-// Ring geometry of a u8 ShrinkH+ShrinkV stage whose column chunks are
-// `chunk_cols` wide: row regions of row_cap bytes, as many source rows per
-// ring slot as fit `slot_target` bytes (at least 1, at most fv and
-// kMaxSlotRows), and the lanes' rotation of their box walk.  Returns the
-// slot size in bytes.
-uint32_t shrink_ring_setup(ShrinkArgs* a, int64_t chunk_cols, uint32_t slot_target);
 }  // namespace launch
 
 }  // namespace viprs

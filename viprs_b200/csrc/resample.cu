@@ -17,9 +17,11 @@
 // the (L2-resident) shrunk plane with coefficient tables in shared memory.
 #include <algorithm>
 #include <cstdio>
-#include <numeric>
+#include <mutex>
+#include <vector>
 
-#include "resample_dev.cuh"
+#include "shrink_warp.cuh"
+#include "shrink_warp.hpp"
 
 namespace viprs {
 namespace launch {
@@ -110,25 +112,6 @@ static void shrink_round_all(ShrinkArgs* a) {
     round_consts32(a->fv, a->vmode, &a->vmul, &a->vadd);
 }
 
-uint32_t shrink_ring_setup(ShrinkArgs* a, int64_t chunk_cols, uint32_t slot_target) {
-    const int64_t per_col = int64_t(a->fh) * a->bands;
-    a->row_cap = ws_slot_bytes(chunk_cols * per_col);
-    int64_t r = int64_t(slot_target) / a->row_cap;
-    r = std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(r, int64_t(a->fv)), int64_t(kMaxSlotRows)));
-    a->slot_rows = int32_t(r);
-    // boxes a multiple of 4 bytes long start in the same bank for lanes
-    // 32 / g apart (g = gcd(box words, 32)): start those lanes' walks at
-    // different words
-    int shift = 5;
-    if (per_col % 4 == 0) {
-        int64_t g = std::gcd<int64_t>(per_col / 4, 32);
-        shift = 0;
-        while ((int64_t(32) >> shift) > g) ++shift;
-    }
-    a->rot_shift = shift;
-    return uint32_t(r * a->row_cap);
-}
-
 // Interior output columns [lo, hi): their source span lies inside the plane
 // and its 16-byte aligned cover lies inside the buffer for every row.
 static void interior_columns(const ShrinkArgs& a, int32_t* lo, int32_t* hi) {
@@ -148,6 +131,104 @@ static void interior_columns(const ShrinkArgs& a, int32_t* lo, int32_t* hi) {
     *hi = int32_t(std::max(l, h));
 }
 
+// Bank-conflict cost of a warp's box walk in shared memory for lane rotation
+// `shift`: lanes read word base + ((q0 + t) % Kg) * G + j at step t, with
+// q0 = (lane >> shift) % Kg; the cost is the sum over steps of the most
+// distinct words any bank serves (the wavefronts of that load).
+static int64_t walk_cost(int B, int fh, int pw, bool premul4, int shift) {
+    const int lp = 32 / pw;
+    const int G = (B == 3 && !premul4) ? 3 : 1;
+    int64_t cost = 0;
+    const int leads = premul4 ? 1 : 4;
+    for (int o = 0; o < leads; ++o) {
+        int base[32], kg[32], q0[32], steps = 0;
+        for (int l = 0; l < 32; ++l) {
+            const int pix = l % pw, part = l / pw;
+            const int j0 = part * fh / lp, j1 = (part + 1) * fh / lp, npix = j1 - j0;
+            const int start = o + (pix * fh + j0) * B;
+            base[l] = start / 4;
+            if (premul4) kg[l] = std::max(npix, 1);
+            else kg[l] = std::max(1, (((npix * B + 3) >> 2) + G - 1) / G);
+            q0[l] = (l >> shift) % kg[l];
+            steps = std::max(steps, kg[l]);
+        }
+        for (int t = 0; t < steps; ++t)
+            for (int j = 0; j < G; ++j) {
+                int64_t words[32];
+                int n = 0;
+                for (int l = 0; l < 32; ++l) {
+                    if (t >= kg[l]) continue;
+                    words[n++] = base[l] + int64_t((q0[l] + t) % kg[l]) * G + j;
+                }
+                int worst = 0;
+                for (int b = 0; b < 32; ++b) {
+                    int distinct = 0;
+                    for (int i = 0; i < n; ++i) {
+                        if (((words[i] % 32) + 32) % 32 != b) continue;
+                        bool seen = false;
+                        for (int q = 0; q < i; ++q) seen |= words[q] == words[i];
+                        distinct += seen ? 0 : 1;
+                    }
+                    worst = std::max(worst, distinct);
+                }
+                cost += worst;
+            }
+    }
+    return cost;
+}
+
+// Resident blocks per SM of a warp-shrink kernel with `smem` bytes of shared
+// memory; the kernel's shared-memory limit is raised once per (bands, size)
+// and the answer cached, so that launches make no driver queries.
+static int warp_blocks_per_sm(void (*kern)(ShrinkArgs), int bands, size_t smem) {
+    struct Entry { int bands; size_t smem; int bps; };
+    static std::vector<Entry> cache;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    bool raised = false;
+    for (const Entry& e : cache) {
+        if (e.bands == bands && e.smem == smem) return e.bps;
+        raised |= e.bands == bands;
+    }
+    // one limit for every size this kernel is launched with (a lower limit
+    // set later would refuse the larger launches)
+    if (!raised) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    int bps = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, kWarpBlockThreads, smem);
+    bps = std::max(1, bps);
+    cache.push_back(Entry{bands, smem, bps});
+    return bps;
+}
+
+static uint32_t warp_stage_bytes(int64_t seg_bytes) { return uint32_t((15 + seg_bytes + 32 + 15) / 16 * 16); }
+
+bool shrink_warp_setup(ShrinkArgs* a, uint32_t stage_budget, int64_t item_bytes) {
+    const int64_t s = int64_t(a->fh) * a->bands;
+    int pw = 32;
+    const int64_t w = std::max<int64_t>(a->out.w, 1);
+    while (pw > 8 && pw / 2 >= w) pw /= 2;  // narrow outputs: spare lanes split the boxes
+    while (pw > 8 && warp_stage_bytes(pw * s) > stage_budget) pw /= 2;
+    if (warp_stage_bytes(pw * s) > stage_budget) return false;
+    a->nxf = pw;
+    a->row_cap = warp_stage_bytes(pw * s);
+    const int64_t per_row = std::max<int64_t>(1, pw * s * int64_t(a->fv));
+    a->rows_per_item = int32_t(std::max<int64_t>(1, std::min<int64_t>(a->out.h, item_bytes / per_row)));
+    const bool premul4 = a->premul_in && a->bands == 4;
+    int best = 5;
+    int64_t best_cost = walk_cost(a->bands, int(a->fh), pw, premul4, 5);
+    for (int sh = 0; sh < 5; ++sh) {
+        const int64_t c = walk_cost(a->bands, int(a->fh), pw, premul4, sh);
+        if (c < best_cost) { best_cost = c; best = sh; }
+    }
+    a->rot_shift = best;
+    return true;
+}
+
+int64_t shrink_warp_items(const ShrinkArgs& a) {
+    const int64_t groups = (a.out.w + a.nxf - 1) / a.nxf;
+    return ((a.out.h + a.rows_per_item - 1) / a.rows_per_item) * groups;
+}
+
 void shrink_prepare(ShrinkArgs* a, int32_t* lo, int32_t* hi) {
     shrink_round_all(a);
     interior_columns(*a, lo, hi);
@@ -156,38 +237,19 @@ void shrink_prepare(ShrinkArgs* a, int32_t* lo, int32_t* hi) {
 cudaError_t shrink2d(ShrinkArgs a, cudaStream_t s) {
     if (a.out.w <= 0 || a.out.h <= 0) return cudaSuccess;
     shrink_round_all(&a);
-    if (a.fmt == kU8 && a.hv_order && (reinterpret_cast<uintptr_t>(a.in.data) & 15) == 0 && a.bands <= 4 &&
-        int64_t(a.fh) * a.bands <= 8192) {
-        // One consumer thread per output column of a chunk: the fewest chunks
-        // (widest row segments, least per-row overhead), three ring slots of
-        // about 16 KB (several source rows each for narrow images), and as many
-        // blocks per SM as fit.
-        const int64_t per_col = int64_t(a.fh) * a.bands;
-        const int64_t chunks = std::max<int64_t>(1, (a.out.w + dev::kCThreads - 1) / dev::kCThreads);
-        const int64_t nxf = (a.out.w + chunks - 1) / chunks;
-        const int stages = 3;
+    if (a.fmt == kU8 && a.hv_order && (reinterpret_cast<uintptr_t>(a.in.data) & 15) == 0 && a.bands <= 4) {
+        // independent warps, each streaming its own source rows (shrink_warp.cuh)
         ShrinkArgs f = a;
-        const uint32_t stage_bytes = shrink_ring_setup(&f, nxf, 16384);
-        void (*kern)(ShrinkArgs) = a.bands == 1 ? dev::shrink_hv_u8_ws<1>
-                                  : a.bands == 2 ? dev::shrink_hv_u8_ws<2>
-                                  : a.bands == 3 ? dev::shrink_hv_u8_ws<3> : dev::shrink_hv_u8_ws<4>;
-        const size_t ctl = (sizeof(dev::WsRing) + 4 + 127) / 128 * 128;
-        const size_t smem = ctl + size_t(stages) * stage_bytes;
-        if (smem <= 200 * 1024 && int64_t(a.out.h) * chunks < (int64_t(1) << 30)) {
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-            int bps = 0;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, dev::kWsThreads, smem);
-            bps = std::max(1, bps);
-            f.chunks = int32_t(chunks);
-            f.nxf = int32_t(nxf);
-            f.stages = stages;
-            f.stage_bytes = stage_bytes;
-            const int64_t resident = int64_t(bps) * sm_count();
-            const int64_t rpi = 1;
-            f.rows_per_item = 1;
-            const int64_t items = ((a.out.h + rpi - 1) / rpi) * chunks;
-            const int64_t grid = std::min<int64_t>(items, resident);
-            kern<<<(unsigned)grid, dev::kWsThreads, smem, s>>>(f);
+        if (shrink_warp_setup(&f, 2048, 48 * 1024)) {
+            const size_t smem = size_t(kWarpBlockThreads / 32) * kWarpStagesHost * f.row_cap;
+            void (*kern)(ShrinkArgs) = a.bands == 1 ? dev::shrink_warp_kernel<1>
+                                      : a.bands == 2 ? dev::shrink_warp_kernel<2>
+                                      : a.bands == 3 ? dev::shrink_warp_kernel<3> : dev::shrink_warp_kernel<4>;
+            const int bps = warp_blocks_per_sm(kern, a.bands, smem);
+            // one warp per item up to the resident grid; warps then stride over the items
+            const int64_t items = shrink_warp_items(f);
+            const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((items + 7) / 8, int64_t(bps) * sm_count()));
+            kern<<<(unsigned)grid, kWarpBlockThreads, smem, s>>>(f);
             return cudaGetLastError();
         }
     }

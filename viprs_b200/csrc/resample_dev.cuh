@@ -322,44 +322,14 @@ __device__ __forceinline__ ShrinkChunk shrink_chunk(const ShrinkArgs& a, int32_t
     return k;
 }
 
-// ---------------------------------------------------------------- warp-specialised shrink ring
+// ---------------------------------------------------------------- u8 box sums
 //
-// ShrinkH then ShrinkV over u8, streaming source row segments through a ring
-// of shared-memory slots.  A producer warp (thread kCThreads, one elected
-// thread) fills a slot with `slot_rows` consecutive source rows of the current
-// column chunk, one TMA bulk copy (`cp.async.bulk`, no multicast) per row, all
-// completing on the slot's `full` mbarrier; eight consumer warps (threads
-// 0..255) each own one output pixel of the chunk and add its box of every row
-// in the slot.  Slots hand over through mbarriers only -- `full` (the copies'
-// transaction bytes) and `empty` (one arrival per consumer warp) -- so there
-// is no block-wide barrier and the ring runs across item boundaries.  Several
-// rows per slot keep enough bytes in flight for narrow images and pay one
-// wait per slot.  Every wait is bounded; a consumer that gives up stops
-// waiting (and raises `stop`), the producer stops issuing, and before it
-// exits the producer waits (bounded) for the copies it still has in flight.
+// Helpers of the u8 ShrinkH+ShrinkV kernels (shrink_warp.cuh): box sums of
+// one output pixel from a staged source row segment, and the rounding.
 
+// Threads of the blocks that run whole-block routines (reduce tiles and rows)
+// plus the producer warp of the persistent batch kernel.
 constexpr int kWsThreads = kCThreads + 32;
-constexpr int kConsumerWarps = kCThreads / 32;
-constexpr int kMaxRing = 16;
-
-struct WsRing {
-    uint64_t full[kMaxRing];
-    uint64_t empty[kMaxRing];
-    int32_t lead[kMaxRing][kMaxSlotRows];  // offset of each row's first byte within its row region
-};
-
-__device__ __forceinline__ void ws_ring_init(WsRing* r, int S) {
-    for (int i = 0; i < S; ++i) {
-        mbar_init(&r->full[i], 1);
-        mbar_init(&r->empty[i], kConsumerWarps);
-    }
-}
-
-// Producer: wait (bounded) for the copies of the last min(issued, S) issues.
-__device__ __forceinline__ void ws_drain(WsRing* r, int S, int64_t issued) {
-    const int64_t first = issued > S ? issued - S : 0;
-    for (int64_t i = first; i < issued; ++i) mbar_wait(&r->full[int(i % S)], uint32_t((i / S) & 1));
-}
 
 // 32-bit rounding of a box sum: (s * mul + add) >> 24 reproduces every u8
 // rounding rule of ShrinkH / ShrinkV (shrinkh.rs:323-397, shrinkv.rs:191-339)
@@ -507,193 +477,6 @@ __device__ __forceinline__ void box_sums_premul2_u8(const uint8_t* p, int fh, ui
     }
     sums[0] = s0;
     sums[1] = s1;
-}
-
-// Start group of this lane's box walk: lanes whose boxes start in the same
-// bank start (lane >> rot_shift) groups apart.
-__device__ __forceinline__ int ws_rot_group(const ShrinkArgs& a, int B) {
-    const int G = B == 3 ? 3 : 1;
-    const int K = (int(a.fh) * B + 3) >> 2;
-    const int Kg = (K + G - 1) / G;
-    const int r = (threadIdx.x & 31) >> a.rot_shift;
-    return (B == 4 && a.premul_in) ? (r % int(a.fh)) : (r % Kg);
-}
-
-// Consumers: output rows [oy0, oy1) of column chunk `c`, whose source rows
-// arrive slot_rows at a time in ring order starting at (slot, ph).  Thread x
-// owns output pixel c.lx0 + x.  Returns false once `stop` is raised.
-template <int B>
-__device__ bool ws_consume(const ShrinkArgs& a, int32_t oy0, int32_t oy1, const ShrinkChunk& c, WsRing* ring,
-                           const uint8_t* bufs, uint32_t stage_bytes, int S, int& slot, uint32_t& ph,
-                           volatile int32_t* stop) {
-    const int32_t fh = int32_t(a.fh), fv = int32_t(a.fv), R = a.slot_rows;
-    const uint32_t cap = a.row_cap;
-    const int x = threadIdx.x, lane = x & 31;
-    const bool mine = x < c.ncols;
-    const int64_t fcol = (a.out.x0 + c.lx0 + x) * (int64_t)fh - a.in.x0;
-    const bool inside = fcol >= 0 && fcol + fh <= a.in.w;
-    const int32_t off = inside ? int32_t(fcol - c.s_lo) * B : 0;
-    const bool premul = a.premul_in != 0;
-    const int q0 = ws_rot_group(a, B);
-    for (int32_t oy = oy0; oy < oy1; ++oy) {
-        uint32_t vacc[B];
-#pragma unroll
-        for (int b = 0; b < B; ++b) vacc[b] = 0;
-        for (int32_t k0 = 0; k0 < fv; k0 += R) {
-            const int32_t rr = min(R, fv - k0);
-            bool live = *stop == 0;
-            if (live && !mbar_wait(&ring->full[slot], ph)) {
-                *stop = 1;
-                live = false;
-            }
-            if (live && mine) {
-                const uint8_t* sb = bufs + (size_t)slot * stage_bytes;
-                const int32_t* leads = ring->lead[slot];
-                for (int32_t r = 0; r < rr; ++r) {
-                    const uint8_t* span = sb + r * cap + leads[r];
-                    uint32_t sums[B];
-                    if (!inside) {
-                        box_sums_clamped_pm_u8<B>(span, fcol, fh, c.s_lo, a.in.w, premul, sums);
-                    } else if (premul && B == 4) {
-                        box_sums_premul4_rot(span + off, fh, q0, *reinterpret_cast<uint32_t(*)[4]>(sums));
-                    } else if (premul && B == 2) {
-                        box_sums_premul2_u8(span + off, fh, *reinterpret_cast<uint32_t(*)[2]>(sums));
-                    } else {
-                        box_sums_rot_u8<B>(span + off, fh, q0, sums);
-                    }
-#pragma unroll
-                    for (int b = 0; b < B; ++b) vacc[b] += round_box(sums[b], a.hmul, a.hadd);
-                }
-            }
-            __syncwarp();
-            if (live && lane == 0) mbar_arrive(&ring->empty[slot]);
-            if (++slot == S) { slot = 0; ph ^= 1u; }
-        }
-        if (*stop == 0 && mine) {
-            uint32_t o[B];
-#pragma unroll
-            for (int b = 0; b < B; ++b) o[b] = round_box(vacc[b], a.vmul, a.vadd);
-            if (a.unpremul_out) {
-#pragma unroll
-                for (int b = 0; b < B - 1; ++b) o[b] = unpremultiply_u8(o[b], o[B - 1]);
-            }
-            uint8_t* dst = a.out.data + (int64_t)oy * a.out.pitch + (int64_t)(c.lx0 + x) * B;
-            if (B == 4 && (reinterpret_cast<uintptr_t>(dst) & 3) == 0) {
-                *reinterpret_cast<uint32_t*>(dst) = o[0] | (o[1 % B] << 8) | (o[2 % B] << 16) | (o[3 % B] << 24);
-            } else {
-#pragma unroll
-                for (int b = 0; b < B; ++b) dst[b] = uint8_t(o[b]);
-            }
-        }
-    }
-    return *stop == 0;
-}
-
-// Producer: issue the source rows of output rows [oy0, oy1) of chunk `c`,
-// slot_rows per slot.  Per row the 16-byte aligned cover of its segment goes
-// by one bulk copy into the row's region of the slot; bytes whose cover would
-// pass the end of the buffer go by plain loads first.  Returns false if a slot
-// never came free.
-template <int B>
-__device__ bool ws_produce(const ShrinkArgs& a, const uint8_t* in_data, int32_t oy0, int32_t oy1,
-                           const ShrinkChunk& c, WsRing* ring, uint8_t* bufs, uint32_t stage_bytes, int S,
-                           int& slot, uint32_t& ph, int64_t& issued) {
-    const int32_t fv = int32_t(a.fv), R = a.slot_rows;
-    const uint32_t cap = a.row_cap;
-    const int64_t n = (c.s_hi - c.s_lo) * B;
-    const int64_t total = a.in.total_bytes;
-    for (int32_t oy = oy0; oy < oy1; ++oy) {
-        for (int32_t k0 = 0; k0 < fv; k0 += R) {
-            const int32_t rr = min(R, fv - k0);
-            if (!mbar_wait(&ring->empty[slot], ph ^ 1u)) return false;
-            uint8_t* dst = bufs + (size_t)slot * stage_bytes;
-            const int64_t ly0 = (a.out.y0 + oy) * (int64_t)fv + k0 - a.in.y0;
-            uint32_t tx = 0;
-            for (int32_t r = 0; r < rr; ++r) {
-                int64_t ly = ly0 + r;
-                ly = ly < 0 ? 0 : (ly >= a.in.h ? a.in.h - 1 : ly);
-                const int64_t s0 = ly * a.in.pitch + c.s_lo * B, e0 = s0 + n;
-                const int64_t as = s0 & ~int64_t(15);
-                int64_t ae = (e0 + 15) & ~int64_t(15);
-                if (ae > total) {
-                    const int64_t ab = e0 & ~int64_t(15);
-                    uint8_t* d = dst + (size_t)r * cap;
-                    for (int64_t q = ab > as ? ab : as; q < e0; ++q) d[q - as] = in_data[q];
-                    ae = ab > as ? ab : as;
-                }
-                ring->lead[slot][r] = int32_t(s0 - as);
-                tx += uint32_t(ae - as);
-            }
-            fence_proxy_async_smem();
-            mbar_arrive_expect_tx(&ring->full[slot], tx);
-            for (int32_t r = 0; r < rr; ++r) {
-                int64_t ly = ly0 + r;
-                ly = ly < 0 ? 0 : (ly >= a.in.h ? a.in.h - 1 : ly);
-                const int64_t s0 = ly * a.in.pitch + c.s_lo * B, e0 = s0 + n;
-                const int64_t as = s0 & ~int64_t(15);
-                int64_t ae = (e0 + 15) & ~int64_t(15);
-                if (ae > total) {
-                    const int64_t ab = e0 & ~int64_t(15);
-                    ae = ab > as ? ab : as;
-                }
-                if (ae > as) bulk_load(dst + (size_t)r * cap, in_data + as, uint32_t(ae - as), &ring->full[slot]);
-            }
-            ++issued;
-            if (++slot == S) { slot = 0; ph ^= 1u; }
-        }
-    }
-    return true;
-}
-
-// Standalone ShrinkH+ShrinkV (u8, B bands, source 16-byte aligned).  Items are
-// (band of output rows, column chunk); the chunks partition the output columns and
-// block b owns items b, b + G, ...  The host picks the chunk count, ring depth,
-// rows per slot and blocks per SM.
-template <int B>
-__global__ void __launch_bounds__(kWsThreads, 4) shrink_hv_u8_ws(ShrinkArgs a) {
-    extern __shared__ __align__(128) uint8_t smem_ws[];
-    WsRing* ring = reinterpret_cast<WsRing*>(smem_ws);
-    volatile int32_t* stop = reinterpret_cast<volatile int32_t*>(smem_ws + sizeof(WsRing));
-    uint8_t* bufs = smem_ws + (sizeof(WsRing) + 4 + 127) / 128 * 128;  // stop flag after the ring
-    const int S = a.stages;
-    const int32_t chunks = a.chunks, G = gridDim.x, rpi = a.rows_per_item;
-    const int32_t n_items = ((a.out.h + rpi - 1) / rpi) * chunks;
-    if (threadIdx.x == 0) {
-        ws_ring_init(ring, S);
-        *stop = 0;
-        mbar_fence_init();
-    }
-    __syncthreads();
-    if (threadIdx.x >= kCThreads) {
-        if (threadIdx.x == kCThreads) {
-            int slot = 0;
-            uint32_t ph = 0;
-            int64_t issued = 0;
-            for (int32_t item = blockIdx.x; item < n_items && *stop == 0; item += G) {
-                const int32_t band = item / chunks;
-                const ShrinkChunk c = shrink_chunk(a, item - band * chunks);
-                const int32_t oy0 = band * rpi, oy1 = min(a.out.h, oy0 + rpi);
-                if (!ws_produce<B>(a, a.in.data, oy0, oy1, c, ring, bufs, a.stage_bytes, S, slot, ph, issued)) {
-                    *stop = 1;
-                    if (a.err) atomicExch(a.err, VIPRS_ERR_TIMEOUT);
-                    break;
-                }
-            }
-            ws_drain(ring, S, issued);
-        }
-        return;
-    }
-    int slot = 0;
-    uint32_t ph = 0;
-    for (int32_t item = blockIdx.x; item < n_items; item += G) {
-        const int32_t band = item / chunks;
-        const ShrinkChunk c = shrink_chunk(a, item - band * chunks);
-        const int32_t oy0 = band * rpi, oy1 = min(a.out.h, oy0 + rpi);
-        if (!ws_consume<B>(a, oy0, oy1, c, ring, bufs, a.stage_bytes, S, slot, ph, stop)) {
-            if (threadIdx.x == 0 && a.err) atomicExch(a.err, VIPRS_ERR_TIMEOUT);
-            break;
-        }
-    }
 }
 
 // ---------------------------------------------------------------- reduce
