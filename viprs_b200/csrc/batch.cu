@@ -10,8 +10,8 @@
 //   pixel    (output row)                                       copy / premultiply / unpremultiply
 //
 // Shrink items run in batch_warp_kernel: every warp claims items on its own
-// and streams its source rows through its own stage buffers (shrink_warp.cuh),
-// so warps never wait for each other.  The other item kinds run in
+// and streams its source rows through its own stage buffers by TMA bulk
+// copies (shrink_warp.cuh), so warps never wait for each other.  The other item kinds run in
 // batch_kernel: a producer warp (threads kCThreads..) claims items one ahead
 // and copies each item's stage descriptor into a queue slot in shared memory
 // (pointers resolved for this launch); the eight consumer warps run the items
@@ -193,14 +193,17 @@ constexpr uint32_t kWarpDesc = (sizeof(ShrinkArgs) + 127) / 128 * 128;
 
 // Shrink items by independent warps: each warp claims items (atomic cursor),
 // copies the item's stage descriptor into its own shared memory, resolves the
-// image pointers for this launch and runs the item with its own stage buffers.
+// image pointers for this launch and runs the item with its own stage
+// buffers.  A warp's shared memory: barriers, descriptor, stage buffers.
 __global__ void __launch_bounds__(256, 4) batch_warp_kernel(BatchArgs g) {
     extern __shared__ __align__(128) uint8_t smem_w[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint8_t* mine = smem_w + size_t(warp) * (kWarpDesc + size_t(kWarpStages) * g.ring_stage_bytes);
-    ShrinkArgs* d = reinterpret_cast<ShrinkArgs*>(mine);
-    uint8_t* wbuf = mine + kWarpDesc;
-    for (;;) {
+    uint8_t* mine = smem_w + size_t(warp) * (kWarpBars + kWarpDesc + size_t(kWarpStages) * g.ring_stage_bytes);
+    WarpPipe p;
+    warp_pipe_init(p, mine);
+    ShrinkArgs* d = reinterpret_cast<ShrinkArgs*>(mine + kWarpBars);
+    uint8_t* wbuf = mine + kWarpBars + kWarpDesc;
+    while (p.ok) {
         int32_t idx = 0;
         if (lane == 0) idx = atomicAdd(g.cursor, 1);
         idx = __shfl_sync(0xffffffffu, idx, 0);
@@ -214,13 +217,14 @@ __global__ void __launch_bounds__(256, 4) batch_warp_kernel(BatchArgs g) {
         if (lane == 0) {
             if (st->in_src) d->in.data = reinterpret_cast<const uint8_t*>(g.srcs[st->image]);
             if (st->out_dst) d->out.data = reinterpret_cast<uint8_t*>(g.dsts[st->image]);
+            d->err = g.err;
         }
         __syncwarp();
         switch (d->bands) {
-        case 1: shrink_warp_index<1>(*d, it.index, wbuf); break;
-        case 2: shrink_warp_index<2>(*d, it.index, wbuf); break;
-        case 3: shrink_warp_index<3>(*d, it.index, wbuf); break;
-        default: shrink_warp_index<4>(*d, it.index, wbuf); break;
+        case 1: shrink_warp_index<1>(*d, it.index, wbuf, p); break;
+        case 2: shrink_warp_index<2>(*d, it.index, wbuf, p); break;
+        case 3: shrink_warp_index<3>(*d, it.index, wbuf, p); break;
+        default: shrink_warp_index<4>(*d, it.index, wbuf, p); break;
         }
         __syncwarp();
     }
@@ -235,7 +239,7 @@ size_t batch_ctl_bytes() {
 }
 
 size_t batch_warp_smem_bytes(uint32_t stage_bytes) {
-    return size_t(8) * (dev::kWarpDesc + size_t(dev::kWarpStages) * stage_bytes);
+    return size_t(8) * (dev::kWarpBars + dev::kWarpDesc + size_t(dev::kWarpStages) * stage_bytes);
 }
 
 int batch_blocks_per_sm(size_t smem, bool ring) {

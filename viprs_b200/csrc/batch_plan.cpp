@@ -108,7 +108,7 @@ int plan_stages(viprs_batch* b, int image, std::vector<std::vector<BatchStage>>*
             bs.lo = lo; bs.hi = hi;
             // independent warps: pixels per warp, stage buffers of at most
             // `ring_target` bytes, about `item_bytes` of source per item
-            if (!launch::shrink_warp_setup(&bs.sh, b->ring_target, b->item_bytes)) return VIPRS_ERR_INVALID_ARGUMENT;
+            if (!launch::shrink_warp_setup(&bs.sh, b->ring_target, b->item_bytes, 0)) return VIPRS_ERR_INVALID_ARGUMENT;
             bs.n_items = int32_t(launch::shrink_warp_items(bs.sh));
             b->ring_stage_bytes = std::max(b->ring_stage_bytes, bs.sh.row_cap);
             break;

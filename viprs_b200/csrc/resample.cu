@@ -202,7 +202,7 @@ static int warp_blocks_per_sm(void (*kern)(ShrinkArgs), int bands, size_t smem) 
 
 static uint32_t warp_stage_bytes(int64_t seg_bytes) { return uint32_t((15 + seg_bytes + 32 + 15) / 16 * 16); }
 
-bool shrink_warp_setup(ShrinkArgs* a, uint32_t stage_budget, int64_t item_bytes) {
+bool shrink_warp_setup(ShrinkArgs* a, uint32_t stage_budget, int64_t item_bytes, int64_t min_items) {
     const int64_t s = int64_t(a->fh) * a->bands;
     int pw = 32;
     const int64_t w = std::max<int64_t>(a->out.w, 1);
@@ -212,15 +212,29 @@ bool shrink_warp_setup(ShrinkArgs* a, uint32_t stage_budget, int64_t item_bytes)
     a->nxf = pw;
     a->row_cap = warp_stage_bytes(pw * s);
     const int64_t per_row = std::max<int64_t>(1, pw * s * int64_t(a->fv));
-    a->rows_per_item = int32_t(std::max<int64_t>(1, std::min<int64_t>(a->out.h, item_bytes / per_row)));
-    const bool premul4 = a->premul_in && a->bands == 4;
-    int best = 5;
-    int64_t best_cost = walk_cost(a->bands, int(a->fh), pw, premul4, 5);
-    for (int sh = 0; sh < 5; ++sh) {
-        const int64_t c = walk_cost(a->bands, int(a->fh), pw, premul4, sh);
-        if (c < best_cost) { best_cost = c; best = sh; }
+    int64_t rows = std::max<int64_t>(1, std::min<int64_t>(a->out.h, item_bytes / per_row));
+    const int64_t groups = (a->out.w + pw - 1) / pw;
+    if (min_items > 0) rows = std::max<int64_t>(1, std::min<int64_t>(rows, groups * a->out.h / min_items));
+    a->rows_per_item = int32_t(rows);
+    // only the premultiplied 4-band walk is rotated (uniform trip counts);
+    // its best rotation per (fh, pw) is cached
+    a->rot_shift = 5;
+    if (a->premul_in && a->bands == 4) {
+        struct Entry { uint32_t fh; int pw; int shift; };
+        static std::vector<Entry> cache;
+        static std::mutex mu;
+        std::lock_guard<std::mutex> lock(mu);
+        for (const Entry& e : cache)
+            if (e.fh == a->fh && e.pw == pw) { a->rot_shift = e.shift; return true; }
+        int best = 5;
+        int64_t best_cost = walk_cost(4, int(a->fh), pw, true, 5);
+        for (int sh = 0; sh < 5; ++sh) {
+            const int64_t c = walk_cost(4, int(a->fh), pw, true, sh);
+            if (c < best_cost) { best_cost = c; best = sh; }
+        }
+        cache.push_back(Entry{a->fh, pw, best});
+        a->rot_shift = best;
     }
-    a->rot_shift = best;
     return true;
 }
 
@@ -240,8 +254,9 @@ cudaError_t shrink2d(ShrinkArgs a, cudaStream_t s) {
     if (a.fmt == kU8 && a.hv_order && (reinterpret_cast<uintptr_t>(a.in.data) & 15) == 0 && a.bands <= 4) {
         // independent warps, each streaming its own source rows (shrink_warp.cuh)
         ShrinkArgs f = a;
-        if (shrink_warp_setup(&f, 2048, 48 * 1024)) {
-            const size_t smem = size_t(kWarpBlockThreads / 32) * kWarpStagesHost * f.row_cap;
+        // items small enough that every resident warp gets several
+        if (shrink_warp_setup(&f, 2048, 48 * 1024, int64_t(sm_count()) * 24 * 4)) {
+            const size_t smem = size_t(kWarpBlockThreads / 32) * (dev::kWarpBars + kWarpStagesHost * size_t(f.row_cap));
             void (*kern)(ShrinkArgs) = a.bands == 1 ? dev::shrink_warp_kernel<1>
                                       : a.bands == 2 ? dev::shrink_warp_kernel<2>
                                       : a.bands == 3 ? dev::shrink_warp_kernel<3> : dev::shrink_warp_kernel<4>;

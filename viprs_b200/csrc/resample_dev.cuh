@@ -342,13 +342,11 @@ __device__ __forceinline__ uint32_t round_box(uint32_t s, uint32_t mul, uint32_t
 // memory at any byte alignment: words are realigned with a funnel shift and
 // the bands are summed four bytes at a time with dp4a masks.  Words go in
 // groups of G (3 for 3 bands: the band pattern repeats every 12 bytes, else
-// 1), starting at group q0 and wrapping around: lanes start at different
-// groups so that a warp's reads spread over the shared-memory banks even when
-// the lanes' boxes lie a multiple of 128 bytes apart.  The last group is
-// masked to the box and may read up to 16 bytes past it (row regions carry
-// 32 bytes of slack).
+// 1); two accumulator sets halve the dp4a chains.  The last group is masked
+// to the box and may read up to 16 bytes past it (stage buffers carry 32
+// bytes of slack).
 template <int B>
-__device__ __forceinline__ void box_sums_rot_u8(const uint8_t* p, int fh, int q0, uint32_t (&sums)[B]) {
+__device__ __forceinline__ void box_sums_u8(const uint8_t* p, int fh, uint32_t (&sums)[B]) {
     constexpr int G = B == 3 ? 3 : 1;
     const int o = int(reinterpret_cast<uintptr_t>(p) & 3);
     const uint32_t* wp = reinterpret_cast<const uint32_t*>(p - o);
@@ -407,7 +405,7 @@ __device__ __forceinline__ void box_sums_rot_u8(const uint8_t* p, int fh, int q0
             }
         }
     };
-    run(q0, Kg - 1);
+    run(0, Kg - 1);
     {
         const int k = (Kg - 1) * G;
         uint32_t lo = wp[k];
@@ -420,29 +418,32 @@ __device__ __forceinline__ void box_sums_rot_u8(const uint8_t* p, int fh, int q0
             lo = hi;
         }
     }
-    run(0, q0);
 #pragma unroll
     for (int b = 0; b < B; ++b) sums[b] = sa[b] + sb[b];
 }
 
 // Premultiplied box sums of fh 4-band pixels (Premultiply<U8> applied to each
 // source pixel before the sum, as the separate Premultiply op would), from a
-// 4-byte aligned box, pixels in the order q0 .. fh-1, 0 .. q0-1 (bank spread).
+// 4-byte aligned box.  Every lane walks fh pixels starting at pixel q0 and
+// wrapping around (the same trip count for every lane, so the warp does not
+// diverge), which spreads the lanes' reads over the shared-memory banks when
+// their boxes lie a multiple of 128 bytes apart.
 // premultiply_u8(c, a) = (t + (t >> 8)) >> 8 with t = c a + 128 equals
 // (c (257 a) + 32896) >> 16 for every c, a in 0..255 (t < 65536).
 __device__ __forceinline__ void box_sums_premul4_rot(const uint8_t* p, int fh, int q0, uint32_t (&sums)[4]) {
     const uint32_t* wp = reinterpret_cast<const uint32_t*>(p);
     uint32_t s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-    auto pix = [&](uint32_t w) {
+    int j = q0;
+    for (int t = 0; t < fh; ++t) {
+        const uint32_t w = wp[j];
+        j = j + 1 == fh ? 0 : j + 1;
         const uint32_t a = w >> 24;
         const uint32_t a257 = a * 257u;
         s0 += (__byte_perm(w, 0u, 0x4440) * a257 + 32896u) >> 16;
         s1 += (__byte_perm(w, 0u, 0x4441) * a257 + 32896u) >> 16;
         s2 += (__byte_perm(w, 0u, 0x4442) * a257 + 32896u) >> 16;
         s3 += a;
-    };
-    for (int j = q0; j < fh; ++j) pix(wp[j]);
-    for (int j = 0; j < q0; ++j) pix(wp[j]);
+    }
     sums[0] = s0;
     sums[1] = s1;
     sums[2] = s2;

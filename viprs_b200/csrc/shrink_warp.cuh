@@ -4,22 +4,27 @@
 // A warp owns `pw` consecutive output pixels (32, 16 or 8: 32 / pw lanes
 // share one pixel's box) of a band of output rows.  It streams the source row
 // segment its boxes cover through a private kWarpStages-deep buffer in shared
-// memory with cp.async (16-byte copies, L1 bypassed), so that the next rows
-// are in flight while it sums the current one; nothing is shared with other
-// warps -- no producer warp, no block barrier, no mbarrier -- and warps pick
-// their work independently.  Per source row each lane sums its part of its
-// pixel's box (dp4a over realigned words, or premultiplied 4-band pixels),
-// the parts are combined with shuffles and rounded as ShrinkH rounds; per
-// output row the rounded sums are rounded as ShrinkV rounds, unpremultiplied
-// when the chain ends there, and stored.  Boxes that leave the plane (the
-// reduce halo beyond the image) read clamped columns from the staged segment.
+// memory: lane 0 issues one TMA bulk copy (`cp.async.bulk`, no multicast) per
+// source row, completing on the stage's mbarrier in the warp's own shared
+// memory, so that the next rows are in flight while the warp sums the current
+// one; rows further ahead are pulled into L2 by bulk prefetches, so that the
+// stage copies wait for L2 rather than DRAM.  Nothing is shared with other warps -- no producer warp, no block
+// barrier -- and warps pick their work independently.  Per source row each
+// lane sums its part of its pixel's box (dp4a over realigned words, or
+// premultiplied 4-band pixels), the parts are combined with shuffles and
+// rounded as ShrinkH rounds; per output row the rounded sums are rounded as
+// ShrinkV rounds, unpremultiplied when the chain ends there, and stored.
+// Boxes that leave the plane (the reduce halo beyond the image) read clamped
+// columns from the staged segment.
 //
 // ShrinkArgs fields used here: nxf = pw, rows_per_item = output rows per
 // work item, row_cap = bytes of one stage buffer (source segment + 16-byte
 // alignment + 32 bytes of over-read slack), rot_shift = lane rotation of the
-// box walk (chosen on the host to spread shared-memory banks).  cp.async
-// completes by itself (no flag to spin on), so the warp never waits on
-// another warp or thread.
+// premultiplied 4-band walk (chosen on the host to spread shared-memory
+// banks).  Every wait on
+// a stage is bounded: a wait that gives up records VIPRS_ERR_TIMEOUT in
+// a.err, waits (bounded) for the warp's copies still in flight and makes the
+// warp stop.
 #pragma once
 
 #include "resample_dev.cuh"
@@ -27,32 +32,72 @@
 namespace viprs {
 namespace dev {
 
-constexpr int kWarpStages = 4;  // source rows in flight per warp
+constexpr int kWarpStages = 4;    // source rows in flight to shared memory per warp
+constexpr int kWarpPrefetch = 12;  // rows ahead of the consumed one pulled into L2
+// Shared memory ahead of a warp's stage buffers: its kWarpStages mbarriers.
+constexpr uint32_t kWarpBars = 128;
 
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+// A warp's copy pipeline: the stage mbarriers and the number of rows issued
+// and consumed so far (row n uses stage n % kWarpStages, phase parity
+// (n / kWarpStages) & 1), kept across the warp's work items.
+struct WarpPipe {
+    uint64_t* bars;
+    uint32_t issued = 0, consumed = 0;
+    bool ok = true;
+};
+
+// Lane 0: initialise the pipe's barriers (one arrival each: lane 0's
+// arrive.expect_tx).
+__device__ __forceinline__ void warp_pipe_init(WarpPipe& p, uint8_t* warp_smem) {
+    p.bars = reinterpret_cast<uint64_t*>(warp_smem);
+    if ((threadIdx.x & 31) == 0) {
+        for (int s = 0; s < kWarpStages; ++s) mbar_init(&p.bars[s], 1);
+        mbar_fence_init();
+    }
+    __syncwarp();
 }
 
-// Groups of the dp4a box walk for `npix` pixels of B bands (G words per
-// group: 3 for 3 bands, else 1), or pixels for the premultiplied 4-band walk.
-__device__ __forceinline__ int warp_walk_groups(int npix, int B, bool premul4) {
-    if (premul4) return npix > 0 ? npix : 1;
-    const int G = B == 3 ? 3 : 1;
-    const int K = (npix * B + 3) >> 2;
-    const int Kg = (K + G - 1) / G;
-    return Kg > 0 ? Kg : 1;
+// Box sums of a pixel whose box leaves the plane (the reduce halo): the
+// columns beyond the plane read its edge columns, so the sum is the box over
+// the part inside the plane plus each edge pixel times the columns clamped
+// onto it (premultiplied when `premul`).  `row` holds plane columns from c_lo.
+template <int B>
+__device__ __forceinline__ void box_sums_edge(const uint8_t* row, int64_t fcol, int32_t fh, int64_t c_lo, int64_t w,
+                                              bool premul, uint32_t (&sums)[B]) {
+    const int64_t ca = fcol < 0 ? 0 : (fcol > w ? w : fcol);
+    const int64_t cb = fcol + fh > w ? w : (fcol + fh < 0 ? 0 : fcol + fh);
+    const int32_t n_in = cb > ca ? int32_t(cb - ca) : 0;
+    const int32_t left = int32_t((fcol < 0 ? (fcol + fh < 0 ? fh : -fcol) : 0));
+    const int32_t right = fh - n_in - left;
+#pragma unroll
+    for (int b = 0; b < B; ++b) sums[b] = 0;
+    if (n_in > 0) {
+        const uint8_t* p = row + (ca - c_lo) * B;
+        if (premul && B == 4) box_sums_premul4_rot(p, n_in, 0, *reinterpret_cast<uint32_t(*)[4]>(sums));
+        else if (premul && B == 2) box_sums_premul2_u8(p, n_in, *reinterpret_cast<uint32_t(*)[2]>(sums));
+        else box_sums_u8<B>(p, n_in, sums);
+    }
+    auto add_px = [&](int64_t c, int32_t times) {
+        if (times <= 0) return;
+        const uint8_t* px = row + (c - c_lo) * B;
+        const uint32_t al = px[B - 1];
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            const uint32_t v = (premul && b != B - 1 && B >= 2) ? premultiply_u8(px[b], al) : uint32_t(px[b]);
+            sums[b] += v * uint32_t(times);
+        }
+    };
+    add_px(0, left);
+    add_px(w - 1, right);
 }
 
 // One work item: output columns [x0, x0 + pw) (local to a.out) of output rows
 // [oy0, oy1).  `wbuf`: this warp's kWarpStages * a.row_cap bytes of shared
-// memory (16-byte aligned).  Every lane of the warp calls it.
+// memory (16-byte aligned).  Every lane of the warp calls it; on a timeout it
+// clears p.ok.
 template <int B>
-__device__ void shrink_warp_item(const ShrinkArgs& a, int32_t x0, int32_t oy0, int32_t oy1, uint8_t* wbuf) {
+__device__ void shrink_warp_item(const ShrinkArgs& a, int32_t x0, int32_t oy0, int32_t oy1, uint8_t* wbuf,
+                                 WarpPipe& p) {
     constexpr int D = kWarpStages;
     const int lane = threadIdx.x & 31;
     const int pw = a.nxf, lp = 32 / pw;
@@ -69,80 +114,102 @@ __device__ void shrink_warp_item(const ShrinkArgs& a, int32_t x0, int32_t oy0, i
     c_hi = c_hi <= c_lo ? c_lo + 1 : (c_hi > a.in.w ? a.in.w : c_hi);
     const int64_t seg_bytes = (c_hi - c_lo) * B;
     const uint32_t rb = a.row_cap;
-    const uint32_t sbase = smem_u32(wbuf);
     // this lane's part of its pixel's box: pixels [j0, j1)
     const int32_t j0 = part * fh / lp, j1 = (part + 1) * fh / lp;
     const int32_t npix = j1 - j0;
     const int32_t off = inside ? int32_t(fcol + j0 - c_lo) * B : 0;
     const bool premul = a.premul_in != 0;
     const bool premul4 = premul && B == 4;
-    const int q0 = (lane >> a.rot_shift) % warp_walk_groups(npix, B, premul4);
+    // lane rotation of the premultiplied walk (the dp4a walk is not rotated:
+    // its split loops would diverge)
+    const int q0 = premul4 ? (lane >> a.rot_shift) % (npix > 0 ? npix : 1) : 0;
     const int32_t T = (oy1 - oy0) * fv;
     const int64_t total = a.in.total_bytes;
-
-    // source row of flattened row index (oy, k) and its first byte
-    auto row_start = [&](int32_t oy, int32_t k) -> int64_t {
-        int64_t ly = (a.out.y0 + oy) * (int64_t)fv + k - a.in.y0;
-        ly = ly < 0 ? 0 : (ly >= a.in.h ? a.in.h - 1 : ly);
+    // flattened row i of the item is plane row ly0 + i (clamped to the plane)
+    const int64_t ly0 = (a.out.y0 + oy0) * (int64_t)fv - a.in.y0;
+    const int64_t hmax = a.in.h - 1;
+    auto row_start = [&](int32_t i) -> int64_t {
+        int64_t ly = ly0 + i;
+        ly = ly < 0 ? 0 : (ly > hmax ? hmax : ly);
         return ly * a.in.pitch + c_lo * B;
     };
-    // A 16-byte aligned plane streams each row segment's aligned cover with
-    // cp.async (a copy passing the end of the buffer takes only the bytes
-    // inside it); any other plane copies the segment byte by byte.
+    // A 16-byte aligned plane streams each row segment's aligned cover by one
+    // bulk copy; bytes whose cover would pass the end of the buffer go by
+    // plain loads first.  Any other plane is copied byte by byte by the whole
+    // warp (the stage's barrier then completes with no transaction bytes).
     const bool al16 = (reinterpret_cast<uintptr_t>(a.in.data) & 15) == 0;
-    auto lead_of = [&](int64_t s0) -> uint32_t { return al16 ? uint32_t(s0 & 15) : 0u; };
-    // copy row (oy, k) into stage buffer `stage`
-    auto issue = [&](int32_t oy, int32_t k, int stage) {
-        const int64_t s0 = row_start(oy, k);
+    // copy row i into the next stage; rows kWarpPrefetch ahead of it are
+    // pulled into L2 first, so that the copy finds its bytes there
+    auto issue = [&](int32_t i) {
+        const int stage = int(p.issued % kWarpStages);
+        uint8_t* dst = wbuf + uint32_t(stage) * rb;
+        const int64_t s0 = row_start(i);
         if (!al16) {
-            uint8_t* d = wbuf + uint32_t(stage) * rb;
-            for (int32_t v = lane; v < int32_t(seg_bytes); v += 32) d[v] = a.in.data[s0 + v];
-            return;
+            for (int32_t v = lane; v < int32_t(seg_bytes); v += 32) dst[v] = a.in.data[s0 + v];
+            __syncwarp();
+            if (lane == 0) mbar_arrive_expect_tx(&p.bars[stage], 0);
+        } else if (lane == 0) {
+            const int64_t e0 = s0 + seg_bytes;
+            const int64_t as = s0 & ~int64_t(15);
+            int64_t ae = (e0 + 15) & ~int64_t(15);
+            if (ae > total) {
+                const int64_t ab = e0 & ~int64_t(15);
+                for (int64_t q = ab > as ? ab : as; q < e0; ++q) dst[q - as] = a.in.data[q];
+                ae = ab > as ? ab : as;
+            }
+            // this stage's earlier reads (generic proxy) before the copy's writes
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(&p.bars[stage], uint32_t(ae - as));
+            if (ae > as) bulk_load(dst, a.in.data + as, uint32_t(ae - as), &p.bars[stage]);
+            if (i + kWarpPrefetch < T) {
+                const int64_t f0 = row_start(i + kWarpPrefetch) & ~int64_t(15);
+                int64_t fe = (f0 + seg_bytes + 31) & ~int64_t(15);
+                fe = fe > (total & ~int64_t(15)) ? (total & ~int64_t(15)) : fe;
+                if (fe > f0) bulk_prefetch_l2(a.in.data + f0, uint32_t(fe - f0));
+            }
         }
-        const int64_t as = s0 & ~int64_t(15);
-        const int32_t nv = int32_t((((s0 + seg_bytes + 15) & ~int64_t(15)) - as) >> 4);
-        const uint32_t dst = sbase + uint32_t(stage) * rb;
-        for (int32_t v = lane; v < nv; v += 32) {
-            const int64_t g = as + 16 * int64_t(v);
-            const int64_t left = total - g;
-            if (left > 0) cp_async16(dst + 16u * uint32_t(v), a.in.data + g, left >= 16 ? 16u : uint32_t(left));
-        }
+        ++p.issued;
+    };
+    // wait (bounded) for the oldest issued row; false on a timeout
+    auto arrive = [&]() -> bool {
+        const int stage = int(p.consumed % kWarpStages);
+        const bool got = mbar_wait(&p.bars[stage], (p.consumed / kWarpStages) & 1u);
+        return __all_sync(0xffffffffu, got);
     };
 
-    // prologue: rows 0 .. D-2 in flight
-    int32_t ioy = oy0, ik = 0;  // next row to issue
-    for (int s = 0; s < D - 1; ++s) {
-        if (s < T) {
-            issue(ioy, ik, s);
-            if (++ik == fv) { ik = 0; ++ioy; }
+    // prologue: the first kWarpPrefetch rows to L2, rows 0 .. D-2 in flight
+    if (al16 && lane == 0) {
+        for (int32_t i = D - 1; i < kWarpPrefetch && i < T; ++i) {
+            const int64_t f0 = row_start(i) & ~int64_t(15);
+            int64_t fe = (f0 + seg_bytes + 31) & ~int64_t(15);
+            fe = fe > (total & ~int64_t(15)) ? (total & ~int64_t(15)) : fe;
+            if (fe > f0) bulk_prefetch_l2(a.in.data + f0, uint32_t(fe - f0));
         }
-        cp_async_commit();
     }
+    for (int32_t i = 0; i < D - 1 && i < T; ++i) issue(i);
     uint32_t vacc[B];
 #pragma unroll
     for (int b = 0; b < B; ++b) vacc[b] = 0;
-    int32_t coy = oy0, ck = 0;  // row being consumed
+    int32_t coy = oy0, ck = 0;  // output row and source row within it being consumed
     for (int32_t i = 0; i < T; ++i) {
-        if (i + D - 1 < T) {
-            issue(ioy, ik, (i + D - 1) % D);
-            if (++ik == fv) { ik = 0; ++ioy; }
+        if (i + D - 1 < T) issue(i + D - 1);
+        if (!arrive()) {
+            p.ok = false;
+            break;
         }
-        cp_async_commit();
-        cp_async_wait<D - 1>();
-        __syncwarp();
-        const uint8_t* row = wbuf + uint32_t(i % D) * rb + lead_of(row_start(coy, ck));
+        const uint8_t* row = wbuf + uint32_t(p.consumed % kWarpStages) * rb + (al16 ? uint32_t(row_start(i) & 15) : 0u);
         uint32_t sums[B];
 #pragma unroll
         for (int b = 0; b < B; ++b) sums[b] = 0;
         if (mine) {
             if (!inside) {
-                if (part == 0) box_sums_clamped_pm_u8<B>(row, fcol, fh, c_lo, a.in.w, premul, sums);
+                if (part == 0) box_sums_edge<B>(row, fcol, fh, c_lo, a.in.w, premul, sums);
             } else if (premul4) {
                 box_sums_premul4_rot(row + off, npix, q0, *reinterpret_cast<uint32_t(*)[4]>(sums));
             } else if (premul && B == 2) {
                 box_sums_premul2_u8(row + off, npix, *reinterpret_cast<uint32_t(*)[2]>(sums));
             } else if (npix > 0) {
-                box_sums_rot_u8<B>(row + off, npix, q0, sums);
+                box_sums_u8<B>(row + off, npix, sums);
             }
         }
         // the parts of a pixel's box sit pw lanes apart
@@ -174,10 +241,18 @@ __device__ void shrink_warp_item(const ShrinkArgs& a, int32_t x0, int32_t oy0, i
             ck = 0;
             ++coy;
         }
+        ++p.consumed;
+        __syncwarp();  // every lane is done with the stage before it is refilled
+    }
+    if (!p.ok) {
+        // record the timeout, then let the copies still in flight land (bounded)
+        if (lane == 0 && a.err) atomicExch(a.err, VIPRS_ERR_TIMEOUT);
+        while (p.consumed < p.issued) {
+            mbar_wait(&p.bars[p.consumed % kWarpStages], (p.consumed / kWarpStages) & 1u);
+            ++p.consumed;
+        }
         __syncwarp();
     }
-    cp_async_wait<0>();
-    __syncwarp();
 }
 
 // Work items of one shrink stage: bands of a.rows_per_item output rows x
@@ -188,24 +263,28 @@ __device__ __forceinline__ int32_t warp_items(const ShrinkArgs& a) {
 }
 
 template <int B>
-__device__ __forceinline__ void shrink_warp_index(const ShrinkArgs& a, int32_t item, uint8_t* wbuf) {
+__device__ __forceinline__ void shrink_warp_index(const ShrinkArgs& a, int32_t item, uint8_t* wbuf, WarpPipe& p) {
     const int32_t groups = (a.out.w + a.nxf - 1) / a.nxf;
     const int32_t band = item / groups, g = item - band * groups;
     const int32_t oy0 = band * a.rows_per_item, oy1 = min(a.out.h, oy0 + a.rows_per_item);
-    shrink_warp_item<B>(a, g * a.nxf, oy0, oy1, wbuf);
+    shrink_warp_item<B>(a, g * a.nxf, oy0, oy1, wbuf, p);
 }
 
 // Standalone ShrinkH+ShrinkV (u8, B <= 4 bands): warp w of the grid takes
-// items w, w + (warps in the grid), ...
+// items w, w + (warps in the grid), ...  Each warp's shared memory: its
+// barriers (kWarpBars bytes), then kWarpStages buffers of a.row_cap bytes.
 template <int B>
 __global__ void __launch_bounds__(256) shrink_warp_kernel(ShrinkArgs a) {
     extern __shared__ __align__(128) uint8_t smem_sw[];
     const int warp = threadIdx.x >> 5;
-    uint8_t* wbuf = smem_sw + size_t(warp) * kWarpStages * a.row_cap;
+    uint8_t* mine = smem_sw + size_t(warp) * (kWarpBars + size_t(kWarpStages) * a.row_cap);
+    WarpPipe p;
+    warp_pipe_init(p, mine);
+    uint8_t* wbuf = mine + kWarpBars;
     const int32_t n = warp_items(a);
     const int32_t stride = int32_t(gridDim.x) * (blockDim.x >> 5);
-    for (int32_t item = int32_t(blockIdx.x) * (blockDim.x >> 5) + warp; item < n; item += stride)
-        shrink_warp_index<B>(a, item, wbuf);
+    for (int32_t item = int32_t(blockIdx.x) * (blockDim.x >> 5) + warp; item < n && p.ok; item += stride)
+        shrink_warp_index<B>(a, item, wbuf, p);
 }
 
 }  // namespace dev

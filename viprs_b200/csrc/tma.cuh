@@ -103,5 +103,12 @@ __device__ __forceinline__ void bulk_load(void* dst_smem, const void* src_gmem, 
         : "memory");
 }
 
+// Bulk prefetch of global [src, src + bytes) into L2 (`bytes` a multiple of
+// 16, src 16-byte aligned): a hint that completes nothing and writes no
+// shared memory.
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 }  // namespace dev
 }  // namespace viprs
