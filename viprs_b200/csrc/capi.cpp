@@ -182,6 +182,7 @@ bool add_reduce2d_stage(viprs_plan* p, const ReduceKernel& first, const ReduceKe
     a.out.w = int32_t(outr.w);
     a.out.h = int32_t(outr.h);
     const Region& ir = p->planes[size_t(in_plane)].r;
+    a.in.pitch = p->planes[size_t(in_plane)].pitch;
     if (!launch::reduce2d_configure(&a, sh.data(), sv.data(), ir.x, ir.y, ir.w, ir.h, 2 * 148, 64 * 1024))
         return false;
     if (launch::reduce2d_smem_bytes(a) == 0) return false;

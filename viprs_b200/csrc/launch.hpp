@@ -102,6 +102,11 @@ struct Reduce2DArgs {
     int32_t span_max = 0;     // largest mid rows (hfirst) or columns (vfirst) one tile reads
     int32_t in_rows_max = 0;  // largest source rows one tile stages in shared memory
     int32_t in_cols_max = 0;  // largest source columns one tile stages
+    // f32: the row-strip kernel (reduce_strip.cuh) instead of tiles: tile_w
+    // output columns per strip, tile_h output rows per block, in_cols_max the
+    // widest source / mid column span of a strip, span_max the rows of its
+    // ring, in_rows_max the source rows in flight per block
+    int32_t strip = 0;
 };
 
 #if defined(__CUDACC__)

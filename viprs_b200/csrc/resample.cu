@@ -18,8 +18,10 @@
 #include <algorithm>
 #include <cstdio>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
+#include "reduce_strip.cuh"
 #include "shrink_warp.cuh"
 #include "shrink_warp.hpp"
 
@@ -313,14 +315,120 @@ static cudaError_t reduce_any(const ReduceArgs& a, cudaStream_t s) {
 cudaError_t reduce_h(const ReduceArgs& a, cudaStream_t s) { return reduce_any<true>(a, s); }
 cudaError_t reduce_v(const ReduceArgs& a, cudaStream_t s) { return reduce_any<false>(a, s); }
 
+// Strip-kernel launch parameters of a configured f32 stage (strip_configure
+// stores the staged-row slots in in_rows_max).
+static dev::StripArgs strip_args(const Reduce2DArgs& a) {
+    dev::StripArgs sa;
+    sa.r = a;
+    sa.tw = a.tile_w;
+    sa.seg = a.tile_h;
+    sa.cs_max = a.in_cols_max;
+    sa.ring = a.span_max;
+    sa.slots = a.in_rows_max;
+    // V first reads whole kStripUnit values per warp unit from a staged row
+    const int64_t vals = int64_t(a.in_cols_max) * a.bands;
+    const int64_t units = (vals + dev::kStripUnit - 1) / dev::kStripUnit * dev::kStripUnit;
+    sa.stage_bytes = a.hfirst ? dev::strip_align16(vals * 4 + 32) : dev::strip_align16((units + 4) * 4);
+    return sa;
+}
+
 size_t reduce2d_smem_bytes(const Reduce2DArgs& a) {
+    if (a.strip) {
+        const dev::StripLayout L = dev::strip_layout(strip_args(a));
+        return L.total <= 200 * 1024 ? size_t(L.total) : 0;
+    }
     if (a.tile_w <= 0 || a.tile_h <= 0 || a.span_max <= 0 || a.in_rows_max <= 0 || a.in_cols_max <= 0) return 0;
     const Reduce2DLayout L = reduce2d_layout(a);
     return L.total <= 200 * 1024 ? size_t(L.total) : 0;
 }
 
+// f32 stages with 1, 3 or 4 bands and a source pitch that is a multiple of 16
+// bytes run as row strips (reduce_strip.cuh): the widest strip whose block
+// fits 110 KB of shared memory (two blocks per SM) with staged rows (a power of
+// two) for twice the span of one group of output rows, else for that span plus
+// one batch, and rows per block for about four waves of blocks.
+static bool strip_configure(Reduce2DArgs* a, const int32_t* sh, const int32_t* sv, int64_t in_x0, int64_t in_w) {
+    if (a->fmt != kF32 || a->premul_in || a->unpremul_out) return false;
+    if (a->bands != 1 && a->bands != 3 && a->bands != 4) return false;
+    if (a->mode_h == kReduceFixed || a->mode_v == kReduceFixed) return false;
+    if (a->in.pitch <= 0 || a->in.pitch % 16 != 0) return false;
+    const int64_t ow = a->out.w, oh = a->out.h;
+    if (ow <= 0 || oh <= 0) return false;
+    // every block's taps must reach the mid plane (the kernel's row and column
+    // sequences are its intersection with the mid plane)
+    if (a->hfirst && (sv[oh - 1] > a->my0 + a->mh - 1 || int64_t(sv[0]) + a->taps_v - 1 < a->my0)) return false;
+    if (!a->hfirst && (sh[ow - 1] > a->mx0 + a->mw - 1 || int64_t(sh[0]) + a->taps_h - 1 < a->mx0)) return false;
+    const int G = dev::kStripGroup, B = dev::kStripBatch;
+    // span: the most rows one group of output rows reaches (groups start at
+    // multiples of G: blocks cover multiples of G rows)
+    int64_t span = 1;
+    for (int64_t y = 0; y < oh; y += G) {
+        const int64_t yb = std::min(oh, y + G) - 1;
+        int64_t v0 = sv[y], v1 = int64_t(sv[yb]) + a->taps_v - 1;
+        if (a->hfirst) {
+            v0 = std::max<int64_t>(v0, a->my0);
+            v1 = std::min<int64_t>(v1, int64_t(a->my0) + a->mh - 1);
+        }
+        span = std::max(span, v1 - v0 + 1);
+    }
+    // staged rows: a power of two, the group's span plus at least one batch in flight
+    int64_t min_slots = B;
+    while (min_slots < span + B) min_slots *= 2;
+    if (min_slots > dev::kStripMaxSlots) return false;
+    int64_t ring = 1;  // H first: mid ring rows, a power of two
+    while (ring < span) ring *= 2;
+    const int tws[3] = {a->bands == 1 ? 128 : 32, a->bands == 1 ? 64 : 16, a->bands == 1 ? 32 : 8};
+    const int64_t budget = 110 * 1024;
+    for (int pass = 0; pass < 2; ++pass) {
+        // first the most slots (a batch or more beyond one group), then the fewest
+        const int64_t want = pass == 0 ? std::min<int64_t>(dev::kStripMaxSlots, 2 * min_slots) : min_slots;
+        for (int tw : tws) {
+            int64_t cs = 1;
+            for (int64_t x = 0; x < ow; x += tw) {
+                const int64_t xb = std::min(ow, x + tw) - 1;
+                const int64_t h0 = sh[x], h1 = int64_t(sh[xb]) + a->taps_h - 1;
+                if (a->hfirst) {
+                    const int64_t c0 = std::min(std::max(h0 - in_x0, int64_t(0)), in_w - 1);
+                    const int64_t c1 = std::min(std::max(h1 - in_x0, int64_t(0)), in_w - 1);
+                    cs = std::max(cs, c1 - c0 + 1);
+                } else {
+                    const int64_t lo = std::max<int64_t>(h0, a->mx0);
+                    const int64_t hi = std::min<int64_t>(h1, int64_t(a->mx0) + a->mw - 1);
+                    cs = std::max(cs, hi - lo + 1);
+                }
+            }
+            Reduce2DArgs c = *a;
+            c.strip = 1;
+            c.tile_w = tw;
+            c.tile_h = 1024;  // the table size of the largest band: fixed below
+            c.in_cols_max = int32_t(cs);
+            c.span_max = int32_t(ring);
+            int64_t slots = 0;
+            for (int64_t p = dev::kStripMaxSlots; p >= want; p /= 2) {
+                c.in_rows_max = int32_t(p);
+                if (dev::strip_layout(strip_args(c)).total <= budget) { slots = p; break; }
+            }
+            if (slots == 0) continue;
+            c.in_rows_max = int32_t(slots);
+            const int64_t total = dev::strip_layout(strip_args(c)).total;
+            const int64_t per_sm = std::max<int64_t>(1, std::min<int64_t>(8, (228 * 1024) / (total + 1024)));
+            const int64_t strips = (ow + tw - 1) / tw;
+            const int64_t min_blocks = 4 * per_sm * 148;
+            const int64_t bands_rows = std::max<int64_t>(1, (min_blocks + strips - 1) / strips);
+            int64_t seg = (oh + bands_rows - 1) / bands_rows;
+            seg = std::max<int64_t>(G, (seg + G - 1) / G * G);
+            c.tile_h = int32_t(std::min<int64_t>(seg, 1024));
+            *a = c;
+            return true;
+        }
+    }
+    return false;
+}
+
 bool reduce2d_configure(Reduce2DArgs* a, const int32_t* sh, const int32_t* sv, int64_t in_x0, int64_t in_y0,
                         int64_t in_w, int64_t in_h, int64_t min_tiles, size_t smem_budget) {
+    a->strip = 0;
+    if (strip_configure(a, sh, sv, in_x0, in_w)) return true;
     static const int32_t kShapes[][2] = {{128, 32}, {64, 64}, {64, 32}, {32, 64}, {32, 32}, {64, 16}, {32, 16},
                                          {16, 32}, {16, 16}, {32, 8}, {16, 8}, {8, 8}, {8, 4}, {4, 4},
                                          {4, 2}, {2, 2}, {2, 1}, {1, 1}};
@@ -397,11 +505,32 @@ static cudaError_t r2d(const Reduce2DArgs& a, size_t smem, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template <int MH, int MV>
+static cudaError_t strip_launch(const Reduce2DArgs& a, size_t smem, cudaStream_t s) {
+    const dev::StripArgs sa = strip_args(a);
+    auto pick = [&](auto hf) {
+        constexpr bool HF = decltype(hf)::value;
+        return a.bands == 1 ? dev::reduce_strip_kernel<1, MH, MV, HF>
+             : a.bands == 3 ? dev::reduce_strip_kernel<3, MH, MV, HF> : dev::reduce_strip_kernel<4, MH, MV, HF>;
+    };
+    auto k = a.hfirst ? pick(std::true_type{}) : pick(std::false_type{});
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    dim3 grid((unsigned)((a.out.w + a.tile_w - 1) / a.tile_w), (unsigned)((a.out.h + a.tile_h - 1) / a.tile_h));
+    k<<<grid, dev::kStripThreads, smem, s>>>(sa);
+    return cudaGetLastError();
+}
+
 cudaError_t reduce2d(const Reduce2DArgs& a, cudaStream_t s) {
     if (a.out.w <= 0 || a.out.h <= 0) return cudaSuccess;
     if (a.unpremul_out && (256 % a.bands) != 0) return cudaErrorInvalidValue;
     const size_t smem = reduce2d_smem_bytes(a);
     if (smem == 0) return cudaErrorInvalidValue;
+    if (a.strip) {
+        if (a.mode_h == kReduceF64Fma && a.mode_v == kReduceF64Fma) return strip_launch<kReduceF64Fma, kReduceF64Fma>(a, smem, s);
+        if (a.mode_h == kReduceF64Fma) return strip_launch<kReduceF64Fma, kReduceF32Simd>(a, smem, s);
+        if (a.mode_v == kReduceF64Fma) return strip_launch<kReduceF32Simd, kReduceF64Fma>(a, smem, s);
+        return strip_launch<kReduceF32Simd, kReduceF32Simd>(a, smem, s);
+    }
     switch (a.fmt) {
     case kU8:
         if (a.mode_h == kReduceFixed) return r2d<uint8_t, kReduceFixed, kReduceFixed>(a, smem, s);
