@@ -86,6 +86,11 @@ typedef struct {
 const char *viprs_status_string(int32_t status);
 /* Last CUDA error code seen by this thread (0 if none). */
 int32_t viprs_last_cuda_error(void);
+/* Host evaluation of the sine the device Lanczos2/3 weights use (rounded to
+   nearest, |x| <= 2^20; kernel.rs:133-214 calls the platform sin): out[i] =
+   sin(x[i]) for i < n.  Returns VIPRS_OK, or INVALID_ARGUMENT for NULL
+   pointers with n > 0. */
+int32_t viprs_sin_rn(const double *x, double *out, int64_t n);
 /* ReduceConfig::output_len (crates/viprs-core/src/resample.rs:92-98). */
 uint32_t viprs_reduce_output_len(double factor, uint32_t input_len);
 /* Number of filter taps and the 65 x taps fixed-point table of ReduceKernel

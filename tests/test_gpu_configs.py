@@ -111,6 +111,29 @@ def test_mapim_bicubic_4096_forward(oracle):
     assert max_rel_err(host(out), exp) <= 1e-5
 
 
+@pytest.mark.parametrize("kernel", ["lanczos2", "lanczos3"])
+def test_affine_lanczos_u8_rotated_2048_bit_exact(oracle, kernel):
+    """u8 Lanczos weights take their sines rounded to nearest on the device:
+    a rotated 2048^2 x 4 image matches viprs's glibc-sin weights bit for bit."""
+    rng = np.random.default_rng(0x5EED0006)
+    img = rng.integers(0, 256, (2048, 2048, 4), dtype=np.uint8)
+    img[::7, :, 3] = 0
+    th, sc = 0.4137, 0.83
+    m = [sc * np.cos(th), -sc * np.sin(th), sc * np.sin(th), sc * np.cos(th)]
+    got = api.affine(torch.from_numpy(img).cuda(), m, 301.25, -417.5, 2048, 2048, kernel)
+    exp = oracle.affine(img, m, 301.25, -417.5, 2048, 2048, kernel, threads=THREADS)
+    assert np.array_equal(host(got), exp)
+
+
+def test_mapim_lanczos3_u8_2048_bit_exact(oracle):
+    rng = np.random.default_rng(0x5EED0007)
+    src = rng.integers(0, 256, (2048, 2048, 3), dtype=np.uint8)
+    index = synth.displacement_index(2048, 0x5EED0007)
+    got = api.mapim(torch.from_numpy(src).cuda(), index, "lanczos3")
+    exp = oracle.mapim(src, host(index), "lanczos3", threads=THREADS)
+    assert np.array_equal(host(got), exp)
+
+
 def _ddot(a, b):
     return float((a.double() * b.double()).sum())
 

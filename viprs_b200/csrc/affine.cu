@@ -5,9 +5,12 @@
 // coordinate and weight arithmetic is f64 in viprs's operation order (these
 // TUs are compiled with --fmad=false; fma() appears exactly where viprs calls
 // mul_add), so u8 and
-// f32 outputs reproduce viprs bit for bit except for kernels that evaluate
-// sin() on the device (Lanczos2/3, Nohalo), whose weights can differ from
-// glibc's by an ulp.
+// f32 outputs reproduce viprs bit for bit.  The Lanczos2/3 weights take their
+// sines from sin_rn.cuh (rounded to nearest); glibc's sin, which viprs calls,
+// differs from it by one ulp on about 0.13% of the arguments (glibc's own
+// rounding error, up to about 0.51 ulp), which moves a weight by one ulp and
+// an u8 output only when its weighted sum lies within about 1e-16 of a
+// rounding boundary.
 //
 //   Affine::process_region ........ affine/core.rs:1593-1632 (incremental walk
 //                                   from each scheduler tile's origin)

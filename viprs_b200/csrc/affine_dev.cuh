@@ -4,6 +4,7 @@
 
 #include "affine_launch.hpp"
 #include "common.cuh"
+#include "sin_rn.cuh"
 
 namespace viprs {
 namespace dev {
@@ -20,7 +21,8 @@ __device__ __forceinline__ double bicubic_w(double x) {
     return 0.0;
 }
 
-// InterpolationKernel::interpolate (kernel.rs:133-214)
+// InterpolationKernel::interpolate (kernel.rs:133-214); the Lanczos sines are
+// rounded to nearest (sin_rn.cuh), as the platform sin viprs calls rounds them
 __device__ __forceinline__ double kernel_w(int k, double x) {
     const double eps = 2.220446049250313e-16;
     const double pi = 3.141592653589793;
@@ -36,13 +38,13 @@ __device__ __forceinline__ double kernel_w(int k, double x) {
     case 8: {
         x = fabs(x);
         if (x < eps) return 1.0;
-        if (x < 2.0) { const double p = pi * x; return 2.0 * sin(p) * sin(p / 2.0) / (p * p); }
+        if (x < 2.0) { const double p = pi * x; return 2.0 * sinrn::sin_rn(p) * sinrn::sin_rn(p / 2.0) / (p * p); }
         return 0.0;
     }
     case 9: {
         x = fabs(x);
         if (x < eps) return 1.0;
-        if (x < 3.0) { const double p = pi * x; return 3.0 * sin(p) * sin(p / 3.0) / (p * p); }
+        if (x < 3.0) { const double p = pi * x; return 3.0 * sinrn::sin_rn(p) * sinrn::sin_rn(p / 3.0) / (p * p); }
         return 0.0;
     }
     default: return 0.0;

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "chain.hpp"
+#include "sin_rn.cuh"
 #include "viprs_b200.h"
 
 using namespace viprs;
@@ -688,6 +689,12 @@ const char* viprs_status_string(int32_t status) {
 }
 
 int32_t viprs_last_cuda_error(void) { return g_last_cuda_error; }
+
+int32_t viprs_sin_rn(const double* x, double* out, int64_t n) {
+    if (n > 0 && (!x || !out)) return VIPRS_ERR_INVALID_ARGUMENT;
+    for (int64_t i = 0; i < n; ++i) out[i] = sinrn::sin_rn(x[i]);
+    return VIPRS_OK;
+}
 
 uint32_t viprs_reduce_output_len(double factor, uint32_t input_len) {
     return reduce_output_len(factor, input_len);
