@@ -439,6 +439,35 @@ def other_reduce_1024(stream, steps):
     return r
 
 
+def other_reduce_1024_batch(stream, steps, n=256):
+    """The reduce_h(4)+reduce_v(4) workload of the 1024x768x3 case on n images
+    at once: one persistent launch over the batch's work list (ChainBatch), and
+    the same n images as n per-image plan launches."""
+    import torch
+
+    from viprs_b200 import api, synth
+    imgs = [synth.smooth_u8(768, 1024, 3, 0x5EED0000 + i) for i in range(n)]
+    builder = api.PipelineBuilder(1024, 768, 3, torch.uint8).reduce_h(4.0).reduce_v(4.0)
+    batch = api.ChainBatch([(768, 1024, 3)] * n, builder)
+    outs = batch.alloc_outputs()
+    ms = timed(lambda: batch.run(imgs, outs, graph=True), steps, 3, stream)
+    plan = builder.build()
+    pouts = [torch.empty(plan.out_shape, dtype=torch.uint8, device="cuda") for _ in range(n)]
+
+    def per_image():
+        for i in range(n):
+            plan(imgs[i], pouts[i])
+    pms = timed(per_image, steps, 3, stream)
+    b = n * (1024 * 768 * 3 + 256 * 192 * 3)
+    peak, kind = measured_hbm_peak()
+    gbs = b / (ms / 1e3) / 1e9
+    return {"workload": f"{n} x reduce_h(4)+reduce_v(4) Lanczos3 1024x768x3 u8, one persistent launch (ChainBatch)",
+            "images": n, "mpix_per_s": round(n * 0.786432 / (ms / 1e3), 1), "ms": round(ms, 4),
+            "algorithmic_bytes": b, "gbs": round(gbs, 1), "frac": round(gbs / peak, 4), "peak_kind": kind,
+            "per_image_ms": round(pms, 4), "batched_vs_per_image": round(pms / ms, 2),
+            "launches": batch.launches()[0], "per_image_launches": n * plan.launches}
+
+
 def other_resize_f32(stream, steps):
     import torch
 
@@ -549,6 +578,7 @@ def other_mapim_grad(stream, steps):
 
 
 OTHERS = (("thumbnail_8192", other_thumbnail_8192), ("reduce_1024x768", other_reduce_1024),
+          ("reduce_1024x768_x256", other_reduce_1024_batch),
           ("resize_f32_6000x4000", other_resize_f32), ("reduce_affine_fwd_bwd", other_reduce_affine_grad),
           ("mapim_fwd_bwd", other_mapim_grad))
 

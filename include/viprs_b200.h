@@ -240,6 +240,11 @@ int32_t viprs_thumbnail_batch_create(int32_t n_images, const uint32_t *widths,
                                      int32_t target, uint32_t target_width,
                                      uint32_t target_height, int32_t kernel, int32_t crop,
                                      viprs_batch **out_batch);
+/* The same node chain (as viprs_chain_plan_create) on every image of the batch
+   (u8 images): e.g. reduce_h + reduce_v over many photos of uneven size. */
+int32_t viprs_chain_batch_create(int32_t n_images, const uint32_t *widths, const uint32_t *heights,
+                                 const uint32_t *bands, const viprs_node *nodes, int32_t n_nodes,
+                                 int32_t demand_override, viprs_batch **out_batch);
 int32_t viprs_batch_output_size(const viprs_batch *batch, int32_t index, uint32_t *width,
                                 uint32_t *height);
 /* Work items, stages and the largest persistent grid of the current configuration. */

@@ -36,6 +36,36 @@ def host(t):
     return t.cpu().numpy()
 
 
+def test_chain_batch_reduce_uneven(oracle):
+    """ChainBatch: one reduce_h(4)+reduce_v(4) chain on u8 images of uneven
+    size and band count in one persistent launch, bit-exact per image."""
+    rng = np.random.default_rng(0x5EED0008)
+    shapes = [(768, 1024, 3), (501, 777, 1), (1200, 333, 4), (64, 2048, 3), (97, 89, 1), (768, 1024, 3)]
+    imgs = [torch.from_numpy(rng.integers(0, 256, s, dtype=np.uint8)).cuda() for s in shapes]
+    builder = api.PipelineBuilder(1024, 768, 3, torch.uint8).reduce_h(4.0).reduce_v(4.0)
+    batch = api.ChainBatch(shapes, builder)
+    outs = batch.run(imgs, graph=False)
+    outs_g = batch.run(imgs, graph=True)
+    for img, out, og in zip(imgs, outs, outs_g):
+        exp = run_chain(host(img), [("reduce_h", dict(factor=4.0, kernel="lanczos3")),
+                                    ("reduce_v", dict(factor=4.0, kernel="lanczos3"))], threads=THREADS)
+        assert np.array_equal(host(out), exp)
+        assert np.array_equal(host(og), exp)
+
+
+def test_chain_batch_reduce_1024x768_x256(oracle):
+    """The batched 1024x768x3 workload of the benchmark (256 images)."""
+    n = 256
+    imgs = [synth.smooth_u8(768, 1024, 3, 0x5EED0000 + i) for i in range(n)]
+    builder = api.PipelineBuilder(1024, 768, 3, torch.uint8).reduce_h(4.0).reduce_v(4.0)
+    batch = api.ChainBatch([(768, 1024, 3)] * n, builder)
+    outs = batch.run(imgs, graph=True)
+    for i in (0, 1, 137, 255):
+        exp = run_chain(host(imgs[i]), [("reduce_h", dict(factor=4.0, kernel="lanczos3")),
+                                        ("reduce_v", dict(factor=4.0, kernel="lanczos3"))], threads=THREADS)
+        assert np.array_equal(host(outs[i]), exp)
+
+
 def test_reduce_1024x768x3_quarter(oracle):
     img = synth.smooth_u8(768, 1024, 3, 0x5EED0000)
     plan = api.PipelineBuilder(1024, 768, 3, torch.uint8).reduce_h(4.0).reduce_v(4.0).build()

@@ -80,6 +80,7 @@ SIGNATURES = {
     "viprs_plan_execute_host": (_I, [_P, _P, _P, _P]),
     "viprs_plan_destroy": (None, [_P]),
     "viprs_thumbnail_batch_create": (_I, [_I, _P, _P, _P, _I, _U, _U, _I, _I, ctypes.POINTER(_P)]),
+    "viprs_chain_batch_create": (_I, [_I, _P, _P, _P, _P, _I, _I, ctypes.POINTER(_P)]),
     "viprs_batch_output_size": (_I, [_P, _I, ctypes.POINTER(_U), ctypes.POINTER(_U)]),
     "viprs_batch_work_items": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "viprs_batch_launch_count": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I)]),

@@ -414,6 +414,11 @@ class ThumbnailBatch:
         h = ctypes.c_void_p()
         N.check(L.viprs_thumbnail_batch_create(n, ws, hs, bs, t, target_width, target_height, _kernel(kernel),
                                                int(crop), ctypes.byref(h)), "thumbnail_batch_create")
+        self._init(h, shapes)
+
+    def _init(self, h, shapes):
+        L = N.lib()
+        n = len(shapes)
         self._h = h
         self.shapes = [tuple(int(v) for v in s) for s in shapes]
         self.out_shapes = []
@@ -510,3 +515,22 @@ class ThumbnailBatch:
             self.close()
         except Exception:
             pass
+
+
+class ChainBatch(ThumbnailBatch):
+    """One builder chain (a PipelineBuilder's nodes, e.g. reduce_h + reduce_v)
+    on every u8 image of a batch of uneven size, with ThumbnailBatch's
+    execution paths."""
+
+    def __init__(self, shapes, builder):
+        if builder._composite is not None:
+            raise ValueError("thumbnail/resize batches are ThumbnailBatch")
+        n = len(shapes)
+        hs = (ctypes.c_uint32 * n)(*[int(s[0]) for s in shapes])
+        ws = (ctypes.c_uint32 * n)(*[int(s[1]) for s in shapes])
+        bs = (ctypes.c_uint32 * n)(*[int(s[2]) for s in shapes])
+        arr = (N.Node * max(1, len(builder.nodes)))(*builder.nodes)
+        h = ctypes.c_void_p()
+        N.check(N.lib().viprs_chain_batch_create(n, ws, hs, bs, arr, len(builder.nodes), builder.demand_override,
+                                                 ctypes.byref(h)), "chain_batch_create")
+        self._init(h, shapes)

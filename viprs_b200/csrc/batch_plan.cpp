@@ -299,17 +299,11 @@ int launch_batch(viprs_batch* b, const uint64_t* d_srcs, const uint64_t* d_dsts,
     return VIPRS_OK;
 }
 
-}  // namespace
-
-extern "C" {
-
-int32_t viprs_thumbnail_batch_create(int32_t n, const uint32_t* widths, const uint32_t* heights,
-                                     const uint32_t* bands, int32_t target, uint32_t tw, uint32_t th,
-                                     int32_t kernel, int32_t crop, viprs_batch** out) {
-    if (!out || !widths || !heights || !bands) return VIPRS_ERR_NULL_POINTER;
-    *out = nullptr;
-    if (n <= 0 || target < 0 || target > 3) return VIPRS_ERR_INVALID_ARGUMENT;
-    if (kernel < 0 || kernel > 9) return VIPRS_ERR_INVALID_KERNEL;
+// A batch of one u8 chain plan per image (`chain_of(i, &chain)` builds image
+// i's chain), its control words and work list.
+template <typename ChainOf>
+int32_t batch_create(int32_t n, const uint32_t* widths, const uint32_t* heights, const uint32_t* bands,
+                     viprs_batch** out, ChainOf chain_of) {
     std::unique_ptr<viprs_batch> b(new (std::nothrow) viprs_batch());
     if (!b) return VIPRS_ERR_OUT_OF_MEMORY;
     b->n = n;
@@ -320,8 +314,7 @@ int32_t viprs_thumbnail_batch_create(int32_t n, const uint32_t* widths, const ui
     int st = VIPRS_OK;
     for (int i = 0; i < n && st == VIPRS_OK; ++i) {
         Chain c;
-        st = builder_thumbnail_chain(widths[i], heights[i], bands[i], ThumbTarget(target), tw, th, Kernel(kernel),
-                                     crop != 0, &c);
+        st = chain_of(i, &c);
         if (st == VIPRS_OK) st = create_chain_plan(widths[i], heights[i], bands[i], VIPRS_U8, c, &b->plans[size_t(i)]);
     }
     if (st == VIPRS_OK) {
@@ -335,6 +328,38 @@ int32_t viprs_thumbnail_batch_create(int32_t n, const uint32_t* widths, const ui
     }
     *out = b.release();
     return VIPRS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t viprs_thumbnail_batch_create(int32_t n, const uint32_t* widths, const uint32_t* heights,
+                                     const uint32_t* bands, int32_t target, uint32_t tw, uint32_t th,
+                                     int32_t kernel, int32_t crop, viprs_batch** out) {
+    if (!out || !widths || !heights || !bands) return VIPRS_ERR_NULL_POINTER;
+    *out = nullptr;
+    if (n <= 0 || target < 0 || target > 3) return VIPRS_ERR_INVALID_ARGUMENT;
+    if (kernel < 0 || kernel > 9) return VIPRS_ERR_INVALID_KERNEL;
+    return batch_create(n, widths, heights, bands, out, [&](int i, Chain* c) {
+        return builder_thumbnail_chain(widths[i], heights[i], bands[i], ThumbTarget(target), tw, th, Kernel(kernel),
+                                       crop != 0, c);
+    });
+}
+
+int32_t viprs_chain_batch_create(int32_t n, const uint32_t* widths, const uint32_t* heights, const uint32_t* bands,
+                                 const viprs_node* nodes, int32_t n_nodes, int32_t demand_override,
+                                 viprs_batch** out) {
+    if (!out || !widths || !heights || !bands) return VIPRS_ERR_NULL_POINTER;
+    *out = nullptr;
+    if (n <= 0) return VIPRS_ERR_INVALID_ARGUMENT;
+    Chain chain;
+    const int32_t st = nodes_to_chain(nodes, n_nodes, demand_override, &chain);
+    if (st) return st;
+    return batch_create(n, widths, heights, bands, out, [&](int, Chain* c) {
+        *c = chain;
+        return int(VIPRS_OK);
+    });
 }
 
 int32_t viprs_batch_output_size(const viprs_batch* b, int32_t i, uint32_t* w, uint32_t* h) {

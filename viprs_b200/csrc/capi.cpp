@@ -624,6 +624,44 @@ int create_chain_plan_a(uint32_t w, uint32_t h, uint32_t bands, int32_t format, 
 }  // namespace
 
 namespace viprs {
+int32_t nodes_to_chain(const viprs_node* nodes, int32_t n_nodes, int32_t demand_override, Chain* out) {
+    if (n_nodes < 0 || (n_nodes > 0 && !nodes) || !out) return VIPRS_ERR_NULL_POINTER;
+    Chain c;
+    c.demand_override = demand_override < 0 ? -1 : demand_override;
+    if (demand_override > 5) return VIPRS_ERR_INVALID_ARGUMENT;
+    for (int32_t i = 0; i < n_nodes; ++i) {
+        const viprs_node& v = nodes[i];
+        PlanNode n;
+        switch (v.kind) {
+        case VIPRS_NODE_PREMULTIPLY: n.kind = NodeKind::Premultiply; break;
+        case VIPRS_NODE_UNPREMULTIPLY: n.kind = NodeKind::Unpremultiply; break;
+        case VIPRS_NODE_SHRINKH: n.kind = NodeKind::ShrinkH; break;
+        case VIPRS_NODE_SHRINKV: n.kind = NodeKind::ShrinkV; break;
+        case VIPRS_NODE_SHRINK: n.kind = NodeKind::Shrink; break;
+        case VIPRS_NODE_REDUCEH: n.kind = NodeKind::ReduceH; break;
+        case VIPRS_NODE_REDUCEV: n.kind = NodeKind::ReduceV; break;
+        case VIPRS_NODE_REDUCE: n.kind = NodeKind::Reduce; break;
+        case VIPRS_NODE_AFFINE: n.kind = NodeKind::Affine; break;
+        case VIPRS_NODE_EXTRACT_AREA: n.kind = NodeKind::ExtractArea; break;
+        default: return VIPRS_ERR_INVALID_ARGUMENT;
+        }
+        if (v.kernel < 0 || v.kernel > 9) return VIPRS_ERR_INVALID_KERNEL;
+        if (v.extend < 0 || v.extend > 5) return VIPRS_ERR_INVALID_ARGUMENT;
+        if (v.demand_hint < 0 || v.demand_hint > 5) return VIPRS_ERR_INVALID_ARGUMENT;
+        n.ufactor = v.factor_u; n.vufactor = v.vfactor_u; n.ceil = v.ceil_mode != 0;
+        n.factor = v.factor; n.vfactor = v.vfactor; n.kernel = Kernel(v.kernel);
+        std::memcpy(n.m, v.matrix, sizeof(n.m));
+        n.tx = v.tx; n.ty = v.ty; n.out_w = v.out_width; n.out_h = v.out_height;
+        n.extend = Extend(v.extend); n.background = v.background; n.premultiplied = v.premultiplied != 0;
+        n.ex = v.area_x; n.ey = v.area_y;
+        if (n.kind == NodeKind::ExtractArea) { n.ew = v.area_width; n.eh = v.area_height; }
+        n.demand = Demand(v.demand_hint);
+        c.nodes.push_back(n);
+    }
+    *out = c;
+    return VIPRS_OK;
+}
+
 int create_chain_plan(uint32_t w, uint32_t h, uint32_t bands, int32_t format, const Chain& chain, viprs_plan** out) {
     return create_chain_plan_a(w, h, bands, format, chain, out);
 }
@@ -824,39 +862,9 @@ int32_t viprs_forward_affine_to_backward(const double f[4], double tx, double ty
 
 int32_t viprs_chain_plan_create(uint32_t w, uint32_t h, uint32_t bands, int32_t format, const viprs_node* nodes,
                                 int32_t n_nodes, int32_t demand_override, viprs_plan** out) {
-    if (n_nodes < 0 || (n_nodes > 0 && !nodes)) return VIPRS_ERR_NULL_POINTER;
     Chain c;
-    c.demand_override = demand_override < 0 ? -1 : demand_override;
-    if (demand_override > 5) return VIPRS_ERR_INVALID_ARGUMENT;
-    for (int32_t i = 0; i < n_nodes; ++i) {
-        const viprs_node& v = nodes[i];
-        PlanNode n;
-        switch (v.kind) {
-        case VIPRS_NODE_PREMULTIPLY: n.kind = NodeKind::Premultiply; break;
-        case VIPRS_NODE_UNPREMULTIPLY: n.kind = NodeKind::Unpremultiply; break;
-        case VIPRS_NODE_SHRINKH: n.kind = NodeKind::ShrinkH; break;
-        case VIPRS_NODE_SHRINKV: n.kind = NodeKind::ShrinkV; break;
-        case VIPRS_NODE_SHRINK: n.kind = NodeKind::Shrink; break;
-        case VIPRS_NODE_REDUCEH: n.kind = NodeKind::ReduceH; break;
-        case VIPRS_NODE_REDUCEV: n.kind = NodeKind::ReduceV; break;
-        case VIPRS_NODE_REDUCE: n.kind = NodeKind::Reduce; break;
-        case VIPRS_NODE_AFFINE: n.kind = NodeKind::Affine; break;
-        case VIPRS_NODE_EXTRACT_AREA: n.kind = NodeKind::ExtractArea; break;
-        default: return VIPRS_ERR_INVALID_ARGUMENT;
-        }
-        if (v.kernel < 0 || v.kernel > 9) return VIPRS_ERR_INVALID_KERNEL;
-        if (v.extend < 0 || v.extend > 5) return VIPRS_ERR_INVALID_ARGUMENT;
-        if (v.demand_hint < 0 || v.demand_hint > 5) return VIPRS_ERR_INVALID_ARGUMENT;
-        n.ufactor = v.factor_u; n.vufactor = v.vfactor_u; n.ceil = v.ceil_mode != 0;
-        n.factor = v.factor; n.vfactor = v.vfactor; n.kernel = Kernel(v.kernel);
-        std::memcpy(n.m, v.matrix, sizeof(n.m));
-        n.tx = v.tx; n.ty = v.ty; n.out_w = v.out_width; n.out_h = v.out_height;
-        n.extend = Extend(v.extend); n.background = v.background; n.premultiplied = v.premultiplied != 0;
-        n.ex = v.area_x; n.ey = v.area_y;
-        if (n.kind == NodeKind::ExtractArea) { n.ew = v.area_width; n.eh = v.area_height; }
-        n.demand = Demand(v.demand_hint);
-        c.nodes.push_back(n);
-    }
+    const int32_t st = nodes_to_chain(nodes, n_nodes, demand_override, &c);
+    if (st) return st;
     return create_chain_plan_a(w, h, bands, format, c, out);
 }
 

@@ -63,6 +63,9 @@ namespace viprs {
 
 // Build a plan for `chain` on an image of (w, h, bands, format) and allocate
 // its tables and workspace (cudaMalloc); status 0 on success.
+// The builder chain of a C-ABI node list (PipelineBuilder node by node).
+int32_t nodes_to_chain(const viprs_node* nodes, int32_t n_nodes, int32_t demand_override, Chain* out);
+
 int create_chain_plan(uint32_t w, uint32_t h, uint32_t bands, int32_t format, const Chain& chain,
                       viprs_plan** out);
 // Enqueue stages [first, first + count) (count < 0: all) on `s`.
