@@ -210,6 +210,10 @@ int32_t viprs_chain_plan_create(uint32_t width, uint32_t height, uint32_t bands,
                                 const viprs_node *nodes, int32_t n_nodes, int32_t demand_override,
                                 viprs_plan **out_plan);
 int32_t viprs_plan_output_size(const viprs_plan *plan, uint32_t *width, uint32_t *height);
+/* Synchronise `stream`, then return and clear the plan's device error word:
+   VIPRS_OK, or VIPRS_ERR_TIMEOUT when a kernel's bounded wait for its bulk
+   copies gave up since the last call (its output is then incomplete). */
+int32_t viprs_plan_status(viprs_plan *plan, void *stream);
 int32_t viprs_plan_workspace_bytes(const viprs_plan *plan, uint64_t *bytes);
 /* Number of kernel launches one execution enqueues. */
 int32_t viprs_plan_launch_count(const viprs_plan *plan, int32_t *launches);

@@ -297,3 +297,14 @@ def test_plan_reuse_and_launch_count():
     b = to_host(plan(to_dev(img)))
     assert np.array_equal(a, b)
     assert 1 <= plan.launches <= 4
+    plan.status()  # no bounded wait of the warp shrink gave up
+
+
+def test_strip_plan_status_clean(oracle):
+    # the f32 strip kernel's waits report into the plan's error word
+    rng = np.random.default_rng(2)
+    img = rng.random((900, 1300, 4), dtype=np.float32)
+    plan = api.resize_plan(1300, 900, 4, torch.float32, 0.37)
+    out = to_host(plan(to_dev(img)))
+    plan.status()
+    assert_same(out, oracle.resize(img, 0.37, 0.37, "lanczos3"), np.float32)

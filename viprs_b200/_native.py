@@ -54,6 +54,7 @@ SIGNATURES = {
     "viprs_status_string": (ctypes.c_char_p, [_I]),
     "viprs_last_cuda_error": (_I, []),
     "viprs_sin_rn": (_I, [_P, _P, ctypes.c_int64]),
+    "viprs_plan_status": (_I, [_P, _P]),
     "viprs_reduce_output_len": (_U, [_D, _U]),
     "viprs_reduce_kernel_table": (_I, [_D, _I, ctypes.POINTER(_I), _P]),
     "viprs_reduceh": (_I, [_IMG, _IMG, _D, _I, _P]),

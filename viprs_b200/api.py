@@ -229,6 +229,11 @@ class Plan:
                 "plan_execute_host")
         return host_dst
 
+    def status(self):
+        """Synchronise the current stream; raise ViprsError if a kernel of an
+        earlier execution gave up a bounded wait (its output is incomplete)."""
+        N.check(N.lib().viprs_plan_status(self._h, _stream()), "plan_status")
+
     def close(self):
         if self._h:
             N.lib().viprs_plan_destroy(self._h)

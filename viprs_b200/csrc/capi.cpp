@@ -443,6 +443,8 @@ int alloc_plan(viprs_plan* p, cudaStream_t stream, bool stream_ordered) {
     cudaGetDevice(&p->device);
     p->stream_ordered_alloc = stream_ordered;
     p->alloc_stream = stream;
+    static const int32_t zero[4] = {0, 0, 0, 0};
+    p->err_off = push_table(p->host_tables, zero, sizeof(zero));
     const size_t tb = std::max<size_t>(p->host_tables.size(), 16);
     cudaError_t e;
     if (stream_ordered) {
@@ -456,6 +458,7 @@ int alloc_plan(viprs_plan* p, cudaStream_t stream, bool stream_ordered) {
         if (e == cudaSuccess && !p->host_tables.empty())
             e = cudaMemcpy(p->d_tables, p->host_tables.data(), p->host_tables.size(), cudaMemcpyHostToDevice);
     }
+    if (e == cudaSuccess) p->d_err = reinterpret_cast<int32_t*>(p->d_tables + p->err_off);
     return cuda_status(e);
 }
 
@@ -506,7 +509,7 @@ int execute_a(viprs_plan* p, const void* src, void* dst, cudaStream_t s, int fir
         cudaError_t e = cudaSuccess;
         switch (st.type) {
         case StageType::Shrink: {
-            ShrinkArgs a = st.sh; a.in = ia; a.out = oa;
+            ShrinkArgs a = st.sh; a.in = ia; a.out = oa; a.err = p->d_err;
             e = launch::shrink2d(a, s);
             break;
         }
@@ -527,6 +530,7 @@ int execute_a(viprs_plan* p, const void* src, void* dst, cudaStream_t s, int fir
             a.phases_v = p->d_tables + st.phases2_off;
             a.coeffs_h = p->d_tables + st.coeffs_off;
             a.coeffs_v = p->d_tables + st.coeffs2_off;
+            a.err = p->d_err;
             e = launch::reduce2d(a, s);
             break;
         }
@@ -885,6 +889,20 @@ int32_t viprs_resize_plan_create(uint32_t w, uint32_t h, uint32_t bands, int32_t
     int st = builder_resize_chain(w, h, bands, hscale, vscale, Kernel(kernel), &c);
     if (st) return st;
     return create_chain_plan_a(w, h, bands, format, c, out);
+}
+
+int32_t viprs_plan_status(viprs_plan* p, void* stream) {
+    if (!p) return VIPRS_ERR_NULL_POINTER;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_status(e);
+    int32_t h = 0;
+    if (p->d_err) {
+        e = cudaMemcpy(&h, p->d_err, sizeof(h), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess && h != 0) e = cudaMemset(p->d_err, 0, sizeof(h));
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    return h;
 }
 
 int32_t viprs_plan_output_size(const viprs_plan* p, uint32_t* w, uint32_t* h) {

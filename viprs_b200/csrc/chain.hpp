@@ -56,6 +56,10 @@ struct viprs_plan {
     // execute_host staging
     uint8_t* d_in = nullptr;
     uint8_t* d_out = nullptr;
+    // device error word inside d_tables (a bounded wait that gave up records
+    // VIPRS_ERR_TIMEOUT there); read and cleared by viprs_plan_status
+    size_t err_off = 0;
+    int32_t* d_err = nullptr;
 };
 
 

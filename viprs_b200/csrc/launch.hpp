@@ -107,6 +107,7 @@ struct Reduce2DArgs {
     // widest source / mid column span of a strip, span_max the rows of its
     // ring, in_rows_max the source rows in flight per block
     int32_t strip = 0;
+    int32_t* err = nullptr;   // device error word (a bounded wait that gave up), may be null
 };
 
 #if defined(__CUDACC__)

@@ -325,6 +325,7 @@ static dev::StripArgs strip_args(const Reduce2DArgs& a) {
     sa.cs_max = a.in_cols_max;
     sa.ring = a.span_max;
     sa.slots = a.in_rows_max;
+    sa.err = a.err;
     // V first reads whole kStripUnit values per warp unit from a staged row
     const int64_t vals = int64_t(a.in_cols_max) * a.bands;
     const int64_t units = (vals + dev::kStripUnit - 1) / dev::kStripUnit * dev::kStripUnit;

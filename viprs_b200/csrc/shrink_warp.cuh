@@ -157,8 +157,7 @@ __device__ void shrink_warp_item(const ShrinkArgs& a, int32_t x0, int32_t oy0, i
                 for (int64_t q = ab > as ? ab : as; q < e0; ++q) dst[q - as] = a.in.data[q];
                 ae = ab > as ? ab : as;
             }
-            // this stage's earlier reads (generic proxy) before the copy's writes
-            fence_proxy_async_smem();
+            if (ae != ((e0 + 15) & ~int64_t(15))) fence_proxy_async_smem();  // plain stores above
             mbar_arrive_expect_tx(&p.bars[stage], uint32_t(ae - as));
             if (ae > as) bulk_load(dst, a.in.data + as, uint32_t(ae - as), &p.bars[stage]);
             if (i + kWarpPrefetch < T) {
