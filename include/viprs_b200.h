@@ -266,13 +266,16 @@ int32_t viprs_batch_execute_graph(viprs_batch *batch, const uint64_t *d_srcs,
 /* Plain per-image path: h_srcs / h_dsts are HOST arrays of device pointers. */
 int32_t viprs_batch_execute_per_image(viprs_batch *batch, const uint64_t *h_srcs,
                                       const uint64_t *h_dsts, void *stream);
-/* Autotuner: times candidate shrink row-segment sizes, ring depths and blocks
-   per SM on the given images and keeps the fastest. */
+/* Autotuner: times candidate warp-shrink stage budgets (1536, 2048, 3072,
+   4096 bytes) x blocks per SM (occupancy maximum, 2, 3) on the given images
+   and keeps the fastest. */
 int32_t viprs_batch_autotune(viprs_batch *batch, const uint64_t *d_srcs, const uint64_t *d_dsts,
                              void *stream, int32_t repeats, float *best_ms);
-/* ring_bytes: source bytes per shrink row segment (256..32768); ring_slots:
-   slots of each block's shrink ring (1..16, 0 = from a 56 KB budget);
-   blocks_per_sm: cap of the shrink launches (0 = occupancy maximum). */
+/* ring_bytes: the warp shrink's stage budget, the most source bytes one row
+   segment of a shrink item may take (1024..32768; each warp holds four such
+   stages); ring_slots: kept for the interface, 0..16, no effect on the warp
+   shrink; blocks_per_sm: cap of the persistent launches (0 = occupancy
+   maximum). */
 int32_t viprs_batch_set_config(viprs_batch *batch, uint32_t ring_bytes, int32_t ring_slots,
                                int32_t blocks_per_sm);
 int32_t viprs_batch_get_config(const viprs_batch *batch, uint32_t *ring_bytes,
@@ -296,9 +299,9 @@ void viprs_batch_destroy(viprs_batch *batch);
    device.  Work needing more than the array returns VIPRS_ERR_SCRATCH_LIMIT
    before touching the GPU.  The first call on each device (with that device
    current) looks up the array's device address and may load this library's
-   device code there: make it before any stream capture begins.  All calls on
-   a device share the array, so calls whose GPU work overlaps (different
-   streams or threads without ordering between them) race; order them. */
+   device code there.  All calls on a device share the array, so calls whose
+   GPU work overlaps (different streams or threads without ordering between
+   them) race; order them. */
 #define VIPRS_NOALLOC_SCRATCH_BYTES (4u << 20)
 int32_t viprs_reduce_noalloc(const viprs_image *in, const viprs_image *out, double hfactor,
                              double vfactor, int32_t kernel, void *stream);

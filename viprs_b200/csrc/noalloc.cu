@@ -14,9 +14,9 @@
 // The array (kScratchBytes = VIPRS_NOALLOC_SCRATCH_BYTES, 4 MiB) exists on
 // every GPU that loads this library, for as long as the process runs.  Its
 // device address is looked up once per device, on the first call made with
-// that device current (cudaGetSymbolAddress).  That first call may load this
-// library's device code on the device, so make it before any stream capture
-// begins.  Every call shares the array and it keeps the last call's contents:
+// that device current (cudaGetSymbolAddress); that first call may load this
+// library's device code on the device.  Every call shares the array and it
+// keeps the last call's contents:
 // calls whose GPU work overlaps (different streams, or different host threads
 // on one device, without ordering between them) race on it.  Nothing in it
 // needs to start at zero: each call's host-to-device copy rewrites the tables
