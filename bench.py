@@ -490,10 +490,15 @@ def other_reduce_affine_grad(stream, steps):
 
     from viprs_b200 import _native as N
     from viprs_b200 import api, synth
-    n = 16
+    n, S = 16, 4
     xs = [synth.uniform_f32(1024, 1024, 4, 0x5EED0004 + i) for i in range(n)]
     gys = [torch.randn((512, 512, 4), device="cuda") for _ in range(n)]
-    plan = api.PipelineBuilder(1024, 1024, 4, torch.float32).reduce_h(2.0).reduce_v(2.0).build()
+    # the 16 images run on S streams (one plan per stream: a plan's executions
+    # must not overlap), so that their small launches overlap on the GPU
+    plans = [api.PipelineBuilder(1024, 1024, 4, torch.float32).reduce_h(2.0).reduce_v(2.0).build()
+             for _ in range(S)]
+    plan = plans[0]
+    streams = [torch.cuda.Stream() for _ in range(S)]
     zs = [torch.empty(plan.out_shape, device="cuda") for _ in range(n)]
     ys = [torch.empty((512, 512, 4), device="cuda") for _ in range(n)]
     gzs = [torch.empty(plan.out_shape, device="cuda") for _ in range(n)]
@@ -505,22 +510,38 @@ def other_reduce_affine_grad(stream, steps):
         mats.append(((ctypes.c_double * 4)(*bm), btx, bty))
     L = N.lib()
 
-    def fwd():
+    def fan_out(work):
+        """work(k, i) for image i on stream k = i % S; every stream starts after
+        and ends before the current stream's position."""
+        main = torch.cuda.current_stream()
+        ev = main.record_event()
+        for k, st in enumerate(streams):
+            st.wait_event(ev)
+            with torch.cuda.stream(st):
+                for i in range(k, n, S):
+                    work(k, i)
+        for st in streams:
+            main.wait_stream(st)
+
+    def fwd_one(k, i):
+        plans[k](xs[i], zs[i])
+        m, btx, bty = mats[i]
+        N.check(L.viprs_affine_backward_matrix(api.image(zs[i]), api.image(ys[i]), m, btx, bty, 1, 2, 0.0, 0,
+                                               0, 0, api._stream()), "affine")
+
+    def bwd_one(k, i):
+        m, btx, bty = mats[i]
         sp = api._stream()
-        for i in range(n):
-            plan(xs[i], zs[i])
-            m, btx, bty = mats[i]
-            N.check(L.viprs_affine_backward_matrix(api.image(zs[i]), api.image(ys[i]), m, btx, bty, 1, 2, 0.0, 0,
-                                                   0, 0, sp), "affine")
+        N.check(L.viprs_affine_grad(api.image(zs[i]), api.image(gys[i]), api.image(gzs[i]), m, btx, bty, 1, 2,
+                                    0.0, 0, 0, 0, 0, ctypes.c_void_p(gms[i].data_ptr()), sp), "affine_grad")
+        N.check(L.viprs_reduce_hv_adjoint(api.image(gzs[i]), api.image(gxs[i]), 2.0, 2.0, 9, sp),
+                "reduce_hv_adjoint")
+
+    def fwd():
+        fan_out(fwd_one)
 
     def bwd():
-        sp = api._stream()
-        for i in range(n):
-            m, btx, bty = mats[i]
-            N.check(L.viprs_affine_grad(api.image(zs[i]), api.image(gys[i]), api.image(gzs[i]), m, btx, bty, 1, 2,
-                                        0.0, 0, 0, 0, 0, ctypes.c_void_p(gms[i].data_ptr()), sp), "affine_grad")
-            N.check(L.viprs_reduce_hv_adjoint(api.image(gzs[i]), api.image(gxs[i]), 2.0, 2.0, 9, sp),
-                    "reduce_hv_adjoint")
+        fan_out(bwd_one)
 
     fwd_ms = timed(fwd, steps, 3, stream)
     bwd_ms = timed(bwd, steps, 3, stream)
@@ -530,7 +551,7 @@ def other_reduce_affine_grad(stream, steps):
     peak, _ = measured_hbm_peak()
     gbs = alg / ((fwd_ms + bwd_ms) / 1e3) / 1e9
     r = {"workload": "16 x 1024^2x4 f32: reduce_h(2)+reduce_v(2) L3 -> affine(s R(theta), t) bilinear 512^2, "
-                     "fwd + bwd (image and matrix gradients, f32-atomic scatter)",
+                     "fwd + bwd (image and matrix gradients, f32-atomic scatter), images over 4 streams",
          "fwd_ms": round(fwd_ms, 4), "bwd_ms": round(bwd_ms, 4), "algorithmic_bytes_fwd_bwd": alg,
          "gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}
     if g_fwd is not None and g_bwd is not None:
