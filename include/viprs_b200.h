@@ -199,6 +199,15 @@ int32_t viprs_thumbnail_plan_create(uint32_t width, uint32_t height, uint32_t ba
                                     int32_t format, int32_t target, uint32_t target_width,
                                     uint32_t target_height, int32_t kernel, int32_t crop,
                                     viprs_plan **out_plan);
+/* Thumbnail::into_pipeline_nodes / into_pipeline_nodes_without_shrink_hint
+   (thumbnail.rs:204-524), host only: the planned nodes (kind 9 = the Zoom
+   upscale), the output size and the shrink-on-load hint (0 = none).  Returns
+   SIZE_MISMATCH, with *n_nodes set, when `capacity` nodes do not suffice. */
+int32_t viprs_thumbnail_plan_nodes(int32_t target, uint32_t target_width, uint32_t target_height,
+                                   int32_t kernel, int32_t crop, uint32_t width, uint32_t height,
+                                   uint32_t bands, int32_t allow_shrink_hint, viprs_node *nodes,
+                                   int32_t capacity, int32_t *n_nodes, uint32_t *out_width,
+                                   uint32_t *out_height, uint32_t *shrink_factor);
 /* PipelineBuilder::resize(Resize::new(hscale, vscale, kernel)) (builder/resample.rs:637-711). */
 int32_t viprs_resize_plan_create(uint32_t width, uint32_t height, uint32_t bands, int32_t format,
                                  double hscale, double vscale, int32_t kernel,

@@ -71,3 +71,132 @@ def test_unpremultiply_integer_formula_equals_f64_formula():
     ci, ai = c.astype(np.int64), a.astype(np.int64)
     got = np.where(ai == 0, 0, np.minimum(255, (510 * ci + ai) // np.maximum(2 * ai, 1)))
     assert np.array_equal(ref.astype(np.int64), got)
+
+
+# ---------------------------------------------------------------- thumbnail planner
+# The product planner (plan.cpp) pinned directly to the reference's own planner
+# tests (thumbnail.rs:531-683), through viprs_thumbnail_plan_nodes (host only),
+# and to the same tests' properties on the CPU restatement.
+
+K_PREMUL, K_SHRINKH, K_SHRINKV, K_REDUCEH, K_REDUCEV, K_AFFINE, K_EXTRACT, K_UNPREMUL = 1, 2, 3, 4, 5, 6, 7, 8
+
+
+def product_plan(w, h, bands, target, tw, th, kernel="lanczos3", crop=False, hint=True):
+    from viprs_b200 import _native as N
+    from viprs_b200 import api
+    nodes = (N.Node * 32)()
+    n, ow, oh, sf = ctypes.c_int32(), ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+    st = N.lib().viprs_thumbnail_plan_nodes(api.TARGETS[target], tw, th, api.KERNELS[kernel], int(crop), w, h,
+                                            bands, int(hint), nodes, 32, ctypes.byref(n), ctypes.byref(ow),
+                                            ctypes.byref(oh), ctypes.byref(sf))
+    assert st == 0
+    return [nodes[i] for i in range(n.value)], (ow.value, oh.value), sf.value
+
+
+def test_product_plan_4000x3000_width99():
+    # thumbnail.rs:531-550
+    nodes, size, sf = product_plan(4000, 3000, 3, "width", 99, 0, hint=True)
+    assert sf == 16 and size == (99, 74)
+    assert [n.kind for n in nodes] == [K_SHRINKH, K_SHRINKV, K_REDUCEH, K_REDUCEV]
+    assert nodes[0].factor_u == 2 and nodes[1].factor_u == 2
+
+
+def test_product_plan_crop_adds_centre_extract():
+    # thumbnail.rs:552-575
+    nodes, size, sf = product_plan(400, 200, 3, "fitbox", 120, 120, crop=True, hint=True)
+    assert sf == 0 and size == (120, 120)
+    assert any(n.kind == K_EXTRACT and n.area_width == 120 and n.area_height == 120 for n in nodes)
+
+
+def test_product_plan_2048_to_400_integer_shrink_no_affine():
+    # thumbnail.rs:587-603
+    nodes, _, _ = product_plan(2048, 2048, 3, "width", 400, 0, hint=False)
+    assert nodes[0].kind == K_SHRINKH and nodes[0].factor_u == 4
+    assert nodes[1].kind == K_SHRINKV and nodes[1].factor_u == 4
+    assert not any(n.kind == K_AFFINE for n in nodes)
+
+
+def _after_reduce(nodes, w):
+    """Width after the integer shrink and the reduce of a planned chain, as
+    thumbnail.rs:605-626 computes it: round(after_shrink / residual), >= 1."""
+    f = next((n.factor_u for n in nodes if n.kind == K_SHRINKH), 1)
+    after_shrink = w // f
+    r = next((n.factor for n in nodes if n.kind == K_REDUCEH), 1.0)
+    return max(1, int(np.floor(after_shrink / r + 0.5))) if r > 1.0 + 1e-9 else after_shrink
+
+
+def test_product_plan_never_undershoots_requested_width():
+    # thumbnail.rs:605-626, over every target width 1 .. 2048 of a 2048 image
+    for tw in range(1, 2049):
+        nodes, _, _ = product_plan(2048, 2048, 3, "width", tw, 0, hint=False)
+        assert _after_reduce(nodes, 2048) >= tw, tw
+
+
+def test_product_plan_rgba_wraps_alpha():
+    # thumbnail.rs:628-645
+    nodes, _, _ = product_plan(37, 19, 4, "width", 11, 0, hint=False)
+    assert nodes[0].kind == K_PREMUL and nodes[-1].kind == K_UNPREMUL
+
+
+def test_product_plan_lanczos_affine_tail_is_bicubic():
+    # thumbnail.rs:647-661
+    from viprs_b200 import api
+    nodes, _, _ = product_plan(1, 2048, 3, "height", 0, 400, hint=False)
+    assert any(n.kind == K_AFFINE and n.kernel == api.KERNELS["bicubic"] and n.out_width == 1 and n.out_height == 400
+               for n in nodes)
+
+
+def test_product_plan_force_exact_same_size_keeps_dimensions():
+    # thumbnail.rs:663-683 (property): ForceExact to the input size
+    rng = np.random.default_rng(7)
+    for _ in range(300):
+        w, h = (int(v) for v in rng.integers(1, 1025, 2))
+        bands = int(rng.choice([1, 3, 4]))
+        _, size, sf = product_plan(w, h, bands, "force_exact", w, h, hint=True)
+        assert sf == 0 and size == (w, h)
+
+
+@pytest.mark.parametrize("case", [(4000, 3000, 3, "width", 99, 0, True), (400, 200, 3, "fitbox", 120, 120, False),
+                                  (2048, 2048, 3, "width", 400, 0, False), (37, 19, 4, "width", 11, 0, False),
+                                  (1, 2048, 3, "height", 0, 400, False), (6000, 4000, 4, "fitbox", 256, 256, False),
+                                  (8192, 8192, 3, "width", 400, 0, False), (777, 1333, 1, "height", 0, 97, False)])
+def test_product_plan_equals_oracle_plan(oracle, case):
+    w, h, b, target, tw, th, hint = case
+    nodes, size, sf = product_plan(w, h, b, target, tw, th, hint=hint)
+    onodes, osize, osf = oracle.thumbnail_plan(w, h, b, target, tw, th, allow_shrink_hint=hint)
+    assert size == tuple(osize) and sf == (osf or 0)
+    assert [n.kind for n in nodes] == [ORACLE_KIND[n["kind"]] for n in onodes]
+    for n, o in zip(nodes, onodes):
+        if n.kind in (K_SHRINKH, K_SHRINKV):
+            assert n.factor_u == o["factor"]
+        elif n.kind in (K_REDUCEH, K_REDUCEV):
+            assert n.factor == o["factor"] and n.kernel == o["kernel"]
+        elif n.kind == K_AFFINE:
+            assert (n.out_width, n.out_height, n.kernel) == (o["out_w"], o["out_h"], o["kernel"])
+            assert list(n.matrix) == o["m"] and (n.tx, n.ty) == (o["tx"], o["ty"])
+        elif n.kind == K_EXTRACT:
+            assert (n.area_x, n.area_y, n.area_width, n.area_height) == (o["x"], o["y"], o["w"], o["h"])
+
+
+ORACLE_KIND = {"premultiply": K_PREMUL, "shrinkh": K_SHRINKH, "shrinkv": K_SHRINKV, "reduceh": K_REDUCEH,
+               "reducev": K_REDUCEV, "affine": K_AFFINE, "extract": K_EXTRACT, "unpremultiply": K_UNPREMUL}
+
+
+def test_oracle_plan_never_undershoots_requested_width(oracle):
+    # thumbnail.rs:605-626 on the CPU restatement's planner
+    class _N:
+        def __init__(self, n):
+            self.kind = ORACLE_KIND[n["kind"]]
+            self.factor_u = int(n.get("factor", 1)) if self.kind in (K_SHRINKH, K_SHRINKV) else 1
+            self.factor = float(n.get("factor", 1.0))
+    for tw in range(1, 2049, 7):
+        onodes, _, _ = oracle.thumbnail_plan(2048, 2048, 3, "width", tw, 0, allow_shrink_hint=False)
+        assert _after_reduce([_N(n) for n in onodes], 2048) >= tw, tw
+
+
+def test_oracle_plan_reference_cases(oracle):
+    # thumbnail.rs:628-661 on the CPU restatement's planner
+    nodes, _, _ = oracle.thumbnail_plan(37, 19, 4, "width", 11, 0, allow_shrink_hint=False)
+    assert nodes[0]["kind"] == "premultiply" and nodes[-1]["kind"] == "unpremultiply"
+    nodes, _, _ = oracle.thumbnail_plan(1, 2048, 3, "height", 0, 400, allow_shrink_hint=False)
+    assert any(n["kind"] == "affine" and n["kernel"] == 2 and (n["out_w"], n["out_h"]) == (1, 400) for n in nodes)

@@ -872,6 +872,37 @@ int32_t viprs_chain_plan_create(uint32_t w, uint32_t h, uint32_t bands, int32_t 
     return create_chain_plan_a(w, h, bands, format, c, out);
 }
 
+int32_t viprs_thumbnail_plan_nodes(int32_t target, uint32_t tw, uint32_t th, int32_t kernel, int32_t crop,
+                                   uint32_t w, uint32_t h, uint32_t bands, int32_t allow_shrink_hint,
+                                   viprs_node* nodes, int32_t capacity, int32_t* n_nodes, uint32_t* out_w,
+                                   uint32_t* out_h, uint32_t* shrink_factor) {
+    if (!n_nodes || !out_w || !out_h || !shrink_factor || (capacity > 0 && !nodes)) return VIPRS_ERR_NULL_POINTER;
+    if (target < 0 || target > 3 || capacity < 0) return VIPRS_ERR_INVALID_ARGUMENT;
+    if (kernel < 0 || kernel > 9) return VIPRS_ERR_INVALID_KERNEL;
+    const ThumbnailPlan plan =
+        thumbnail_plan(ThumbTarget(target), tw, th, Kernel(kernel), crop != 0, w, h, bands, allow_shrink_hint != 0);
+    *n_nodes = int32_t(plan.nodes.size());
+    *out_w = plan.output_width;
+    *out_h = plan.output_height;
+    *shrink_factor = plan.shrink_factor;
+    if (int64_t(plan.nodes.size()) > capacity) return VIPRS_ERR_SIZE_MISMATCH;
+    for (size_t i = 0; i < plan.nodes.size(); ++i) {
+        const PlanNode& n = plan.nodes[i];
+        viprs_node v;
+        std::memset(&v, 0, sizeof(v));
+        v.kind = int32_t(n.kind);
+        v.factor_u = n.ufactor; v.vfactor_u = n.vufactor; v.ceil_mode = n.ceil ? 1 : 0;
+        v.factor = n.factor; v.vfactor = n.vfactor; v.kernel = int32_t(n.kernel);
+        std::memcpy(v.matrix, n.m, sizeof(v.matrix));
+        v.tx = n.tx; v.ty = n.ty; v.out_width = n.out_w; v.out_height = n.out_h;
+        v.extend = int32_t(n.extend); v.background = n.background; v.premultiplied = n.premultiplied ? 1 : 0;
+        v.area_x = n.ex; v.area_y = n.ey; v.area_width = n.ew; v.area_height = n.eh;
+        v.demand_hint = int32_t(n.demand);
+        nodes[i] = v;
+    }
+    return VIPRS_OK;
+}
+
 int32_t viprs_thumbnail_plan_create(uint32_t w, uint32_t h, uint32_t bands, int32_t format, int32_t target,
                                     uint32_t tw, uint32_t th, int32_t kernel, int32_t crop, viprs_plan** out) {
     if (target < 0 || target > 3) return VIPRS_ERR_INVALID_ARGUMENT;
