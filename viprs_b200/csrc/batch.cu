@@ -195,7 +195,7 @@ constexpr uint32_t kWarpDesc = (sizeof(ShrinkArgs) + 127) / 128 * 128;
 // copies the item's stage descriptor into its own shared memory, resolves the
 // image pointers for this launch and runs the item with its own stage
 // buffers.  A warp's shared memory: barriers, descriptor, stage buffers.
-__global__ void __launch_bounds__(256, 4) batch_warp_kernel(BatchArgs g) {
+__global__ void __launch_bounds__(256, 3) batch_warp_kernel(BatchArgs g) {
     extern __shared__ __align__(128) uint8_t smem_w[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint8_t* mine = smem_w + size_t(warp) * (kWarpBars + kWarpDesc + size_t(kWarpStages) * g.ring_stage_bytes);

@@ -128,11 +128,28 @@ __device__ void shrink_warp_item(const ShrinkArgs& a, int32_t x0, int32_t oy0, i
     // flattened row i of the item is plane row ly0 + i (clamped to the plane)
     const int64_t ly0 = (a.out.y0 + oy0) * (int64_t)fv - a.in.y0;
     const int64_t hmax = a.in.h - 1;
-    auto row_start = [&](int32_t i) -> int64_t {
-        int64_t ly = ly0 + i;
-        ly = ly < 0 ? 0 : (ly > hmax ? hmax : ly);
-        return ly * a.in.pitch + c_lo * B;
+    // byte offset of flattened row i's segment, and the same advanced one row
+    // at a time (the rows of an item are consecutive, clamped at the plane's
+    // edges: the offset moves by a pitch only while the clamped row moves)
+    struct Cursor {
+        int64_t raw, off;
     };
+    auto cursor_at = [&](int32_t i) -> Cursor {
+        const int64_t ly = ly0 + i;
+        const int64_t c = ly < 0 ? 0 : (ly > hmax ? hmax : ly);
+        return Cursor{ly, c * a.in.pitch + c_lo * B};
+    };
+    auto step = [&](Cursor& c) {
+        ++c.raw;
+        if (uint64_t(c.raw - 1) < uint64_t(hmax)) c.off += a.in.pitch;
+    };
+    Cursor cur_issue = cursor_at(0);
+    // staged-row leads (segment offset mod 16), one byte per stage
+    uint32_t leads = 0;
+    // the row kWarpPrefetch below the one being issued is pulled into L2 (its
+    // offset is not clamped at the plane's edges: the prefetch is only a hint,
+    // kept inside the buffer below)
+    const int64_t pref_ahead = int64_t(kWarpPrefetch) * a.in.pitch;
     // A 16-byte aligned plane streams each row segment's aligned cover by one
     // bulk copy; bytes whose cover would pass the end of the buffer go by
     // plain loads first.  Any other plane is copied byte by byte by the whole
@@ -143,7 +160,9 @@ __device__ void shrink_warp_item(const ShrinkArgs& a, int32_t x0, int32_t oy0, i
     auto issue = [&](int32_t i) {
         const int stage = int(p.issued % kWarpStages);
         uint8_t* dst = wbuf + uint32_t(stage) * rb;
-        const int64_t s0 = row_start(i);
+        const int64_t s0 = cur_issue.off;
+        step(cur_issue);
+        leads = (leads & ~(0xFFu << (8 * stage))) | (uint32_t(s0 & 15) << (8 * stage));
         if (!al16) {
             for (int32_t v = lane; v < int32_t(seg_bytes); v += 32) dst[v] = a.in.data[s0 + v];
             __syncwarp();
@@ -161,7 +180,7 @@ __device__ void shrink_warp_item(const ShrinkArgs& a, int32_t x0, int32_t oy0, i
             mbar_arrive_expect_tx(&p.bars[stage], uint32_t(ae - as));
             if (ae > as) bulk_load(dst, a.in.data + as, uint32_t(ae - as), &p.bars[stage]);
             if (i + kWarpPrefetch < T) {
-                const int64_t f0 = row_start(i + kWarpPrefetch) & ~int64_t(15);
+                const int64_t f0 = (s0 + pref_ahead) & ~int64_t(15);
                 int64_t fe = (f0 + seg_bytes + 31) & ~int64_t(15);
                 fe = fe > (total & ~int64_t(15)) ? (total & ~int64_t(15)) : fe;
                 if (fe > f0) bulk_prefetch_l2(a.in.data + f0, uint32_t(fe - f0));
@@ -178,8 +197,9 @@ __device__ void shrink_warp_item(const ShrinkArgs& a, int32_t x0, int32_t oy0, i
 
     // prologue: the first kWarpPrefetch rows to L2, rows 0 .. D-2 in flight
     if (al16 && lane == 0) {
-        for (int32_t i = D - 1; i < kWarpPrefetch && i < T; ++i) {
-            const int64_t f0 = row_start(i) & ~int64_t(15);
+        Cursor c = cursor_at(D - 1);
+        for (int32_t i = D - 1; i < kWarpPrefetch && i < T; ++i, step(c)) {
+            const int64_t f0 = c.off & ~int64_t(15);
             int64_t fe = (f0 + seg_bytes + 31) & ~int64_t(15);
             fe = fe > (total & ~int64_t(15)) ? (total & ~int64_t(15)) : fe;
             if (fe > f0) bulk_prefetch_l2(a.in.data + f0, uint32_t(fe - f0));
@@ -196,7 +216,8 @@ __device__ void shrink_warp_item(const ShrinkArgs& a, int32_t x0, int32_t oy0, i
             p.ok = false;
             break;
         }
-        const uint8_t* row = wbuf + uint32_t(p.consumed % kWarpStages) * rb + (al16 ? uint32_t(row_start(i) & 15) : 0u);
+        const uint32_t cst = p.consumed % kWarpStages;
+        const uint8_t* row = wbuf + cst * rb + (al16 ? (leads >> (8 * cst)) & 0xFFu : 0u);
         uint32_t sums[B];
 #pragma unroll
         for (int b = 0; b < B; ++b) sums[b] = 0;
