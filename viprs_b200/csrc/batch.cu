@@ -221,10 +221,10 @@ __global__ void __launch_bounds__(256, 3) batch_warp_kernel(BatchArgs g) {
         }
         __syncwarp();
         switch (d->bands) {
-        case 1: shrink_warp_index<1>(*d, it.index, wbuf, p); break;
-        case 2: shrink_warp_index<2>(*d, it.index, wbuf, p); break;
-        case 3: shrink_warp_index<3>(*d, it.index, wbuf, p); break;
-        default: shrink_warp_index<4>(*d, it.index, wbuf, p); break;
+        case 1: shrink_warp_index<1, false>(*d, it.index, wbuf, p); break;
+        case 2: shrink_warp_index<2, false>(*d, it.index, wbuf, p); break;
+        case 3: shrink_warp_index<3, false>(*d, it.index, wbuf, p); break;
+        default: shrink_warp_index<4, false>(*d, it.index, wbuf, p); break;
         }
         __syncwarp();
     }

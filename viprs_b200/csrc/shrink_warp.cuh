@@ -95,7 +95,7 @@ __device__ __forceinline__ void box_sums_edge(const uint8_t* row, int64_t fcol, 
 // [oy0, oy1).  `wbuf`: this warp's kWarpStages * a.row_cap bytes of shared
 // memory (16-byte aligned).  Every lane of the warp calls it; on a timeout it
 // clears p.ok.
-template <int B>
+template <int B, bool PAIR>
 __device__ void shrink_warp_item(const ShrinkArgs& a, int32_t x0, int32_t oy0, int32_t oy1, uint8_t* wbuf,
                                  WarpPipe& p) {
     constexpr int D = kWarpStages;
@@ -155,19 +155,33 @@ __device__ void shrink_warp_item(const ShrinkArgs& a, int32_t x0, int32_t oy0, i
     // plain loads first.  Any other plane is copied byte by byte by the whole
     // warp (the stage's barrier then completes with no transaction bytes).
     const bool al16 = (reinterpret_cast<uintptr_t>(a.in.data) & 15) == 0;
-    // copy row i into the next stage; rows kWarpPrefetch ahead of it are
-    // pulled into L2 first, so that the copy finds its bytes there
-    auto issue = [&](int32_t i) {
-        const int stage = int(p.issued % kWarpStages);
-        uint8_t* dst = wbuf + uint32_t(stage) * rb;
-        const int64_t s0 = cur_issue.off;
+    // copy rows [first, first + n) of the item (n <= 2) into their
+    // stages: lanes 0 .. n-1 issue one bulk copy each, in parallel, and pull
+    // the row kWarpPrefetch below theirs into L2, so that its copy finds its
+    // bytes there
+    auto issue2 = [&](int32_t first, int n) {
+        const int64_t o0 = cur_issue.off;
         step(cur_issue);
-        leads = (leads & ~(0xFFu << (8 * stage))) | (uint32_t(s0 & 15) << (8 * stage));
+        const int64_t o1 = cur_issue.off;
+        if (n > 1) step(cur_issue);
+        // stages follow the warp's running count of issued rows (items chain
+        // on one pipe), exactly as the consumer's count of consumed rows does
+        const int st0 = int(p.issued % kWarpStages), st1 = int((p.issued + 1) % kWarpStages);
+        leads = (leads & ~(0xFFu << (8 * st0))) | (uint32_t(o0 & 15) << (8 * st0));
+        if (n > 1) leads = (leads & ~(0xFFu << (8 * st1))) | (uint32_t(o1 & 15) << (8 * st1));
         if (!al16) {
-            for (int32_t v = lane; v < int32_t(seg_bytes); v += 32) dst[v] = a.in.data[s0 + v];
-            __syncwarp();
-            if (lane == 0) mbar_arrive_expect_tx(&p.bars[stage], 0);
-        } else if (lane == 0) {
+            for (int k = 0; k < n; ++k) {
+                uint8_t* dst = wbuf + uint32_t(k == 0 ? st0 : st1) * rb;
+                const int64_t s0 = k == 0 ? o0 : o1;
+                for (int32_t v = lane; v < int32_t(seg_bytes); v += 32) dst[v] = a.in.data[s0 + v];
+                __syncwarp();
+                if (lane == 0) mbar_arrive_expect_tx(&p.bars[k == 0 ? st0 : st1], 0);
+            }
+        } else if (lane < n) {
+            const int stage = lane == 0 ? st0 : st1;
+            const int64_t s0 = lane == 0 ? o0 : o1;
+            const int32_t i = first + lane;
+            uint8_t* dst = wbuf + uint32_t(stage) * rb;
             const int64_t e0 = s0 + seg_bytes;
             const int64_t as = s0 & ~int64_t(15);
             int64_t ae = (e0 + 15) & ~int64_t(15);
@@ -186,7 +200,7 @@ __device__ void shrink_warp_item(const ShrinkArgs& a, int32_t x0, int32_t oy0, i
                 if (fe > f0) bulk_prefetch_l2(a.in.data + f0, uint32_t(fe - f0));
             }
         }
-        ++p.issued;
+        p.issued += uint32_t(n);
     };
     // wait (bounded) for the oldest issued row; false on a timeout
     auto arrive = [&]() -> bool {
@@ -195,23 +209,34 @@ __device__ void shrink_warp_item(const ShrinkArgs& a, int32_t x0, int32_t oy0, i
         return __all_sync(0xffffffffu, got);
     };
 
-    // prologue: the first kWarpPrefetch rows to L2, rows 0 .. D-2 in flight
+    // PAIR: rows are issued two at a time, when a pair of stages has been
+    // consumed (half the issue instructions per row, more registers); else one
+    // at a time, D - 1 rows ahead of the one being consumed.
+    // prologue: the rows up to kWarpPrefetch - 1 that no issue prefetches go
+    // to L2, then the first rows (D of them in pairs, D - 1 singly) in flight
+    static_assert(kWarpStages == 4, "rows are issued in pairs into two of four stages");
+    constexpr int kFirst = PAIR ? D : D - 1;
     if (al16 && lane == 0) {
-        Cursor c = cursor_at(D - 1);
-        for (int32_t i = D - 1; i < kWarpPrefetch && i < T; ++i, step(c)) {
+        Cursor c = cursor_at(kFirst);
+        for (int32_t i = kFirst; i < kWarpPrefetch && i < T; ++i, step(c)) {
             const int64_t f0 = c.off & ~int64_t(15);
             int64_t fe = (f0 + seg_bytes + 31) & ~int64_t(15);
             fe = fe > (total & ~int64_t(15)) ? (total & ~int64_t(15)) : fe;
             if (fe > f0) bulk_prefetch_l2(a.in.data + f0, uint32_t(fe - f0));
         }
     }
-    for (int32_t i = 0; i < D - 1 && i < T; ++i) issue(i);
+    if (PAIR) {
+        issue2(0, min(T, 2));
+        if (T > 2) issue2(2, min(T - 2, 2));
+    } else {
+        for (int32_t i = 0; i < D - 1 && i < T; ++i) issue2(i, 1);
+    }
     uint32_t vacc[B];
 #pragma unroll
     for (int b = 0; b < B; ++b) vacc[b] = 0;
     int32_t coy = oy0, ck = 0;  // output row and source row within it being consumed
     for (int32_t i = 0; i < T; ++i) {
-        if (i + D - 1 < T) issue(i + D - 1);
+        if (!PAIR && i + D - 1 < T) issue2(i + D - 1, 1);
         if (!arrive()) {
             p.ok = false;
             break;
@@ -263,6 +288,8 @@ __device__ void shrink_warp_item(const ShrinkArgs& a, int32_t x0, int32_t oy0, i
         }
         ++p.consumed;
         __syncwarp();  // every lane is done with the stage before it is refilled
+        // a pair of rows consumed: their two stages take rows i + 3 and i + 4
+        if (PAIR && (i & 1) && i + 3 < T) issue2(i + 3, min(T - (i + 3), 2));
     }
     if (!p.ok) {
         // record the timeout, then let the copies still in flight land (bounded)
@@ -282,12 +309,12 @@ __device__ __forceinline__ int32_t warp_items(const ShrinkArgs& a) {
     return ((a.out.h + a.rows_per_item - 1) / a.rows_per_item) * groups;
 }
 
-template <int B>
+template <int B, bool PAIR>
 __device__ __forceinline__ void shrink_warp_index(const ShrinkArgs& a, int32_t item, uint8_t* wbuf, WarpPipe& p) {
     const int32_t groups = (a.out.w + a.nxf - 1) / a.nxf;
     const int32_t band = item / groups, g = item - band * groups;
     const int32_t oy0 = band * a.rows_per_item, oy1 = min(a.out.h, oy0 + a.rows_per_item);
-    shrink_warp_item<B>(a, g * a.nxf, oy0, oy1, wbuf, p);
+    shrink_warp_item<B, PAIR>(a, g * a.nxf, oy0, oy1, wbuf, p);
 }
 
 // Standalone ShrinkH+ShrinkV (u8, B <= 4 bands): warp w of the grid takes
@@ -304,7 +331,7 @@ __global__ void __launch_bounds__(256) shrink_warp_kernel(ShrinkArgs a) {
     const int32_t n = warp_items(a);
     const int32_t stride = int32_t(gridDim.x) * (blockDim.x >> 5);
     for (int32_t item = int32_t(blockIdx.x) * (blockDim.x >> 5) + warp; item < n && p.ok; item += stride)
-        shrink_warp_index<B>(a, item, wbuf, p);
+        shrink_warp_index<B, true>(a, item, wbuf, p);
 }
 
 }  // namespace dev
