@@ -195,6 +195,7 @@ constexpr uint32_t kWarpDesc = (sizeof(ShrinkArgs) + 127) / 128 * 128;
 // copies the item's stage descriptor into its own shared memory, resolves the
 // image pointers for this launch and runs the item with its own stage
 // buffers.  A warp's shared memory: barriers, descriptor, stage buffers.
+template <int B>
 __global__ void __launch_bounds__(256, 3) batch_warp_kernel(BatchArgs g) {
     extern __shared__ __align__(128) uint8_t smem_w[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -220,12 +221,7 @@ __global__ void __launch_bounds__(256, 3) batch_warp_kernel(BatchArgs g) {
             d->err = g.err;
         }
         __syncwarp();
-        switch (d->bands) {
-        case 1: shrink_warp_index<1, false>(*d, it.index, wbuf, p); break;
-        case 2: shrink_warp_index<2, false>(*d, it.index, wbuf, p); break;
-        case 3: shrink_warp_index<3, false>(*d, it.index, wbuf, p); break;
-        default: shrink_warp_index<4, false>(*d, it.index, wbuf, p); break;
-        }
+        shrink_warp_index<B, false>(*d, it.index, wbuf, p);
         __syncwarp();
     }
 }
@@ -242,19 +238,31 @@ size_t batch_warp_smem_bytes(uint32_t stage_bytes) {
     return size_t(8) * (dev::kWarpBars + dev::kWarpDesc + size_t(dev::kWarpStages) * stage_bytes);
 }
 
-int batch_blocks_per_sm(size_t smem, bool ring) {
-    void (*k)(BatchArgs) = ring ? dev::batch_warp_kernel : dev::batch_kernel;
-    const int threads = ring ? 256 : dev::kWsThreads;
+// The persistent kernel of a launch: the tile variant (ring_bands 0) or the
+// warp shrink of images with ring_bands bands.
+static void (*batch_kernel_of(int ring_bands))(BatchArgs) {
+    switch (ring_bands) {
+    case 0: return dev::batch_kernel;
+    case 1: return dev::batch_warp_kernel<1>;
+    case 2: return dev::batch_warp_kernel<2>;
+    case 3: return dev::batch_warp_kernel<3>;
+    default: return dev::batch_warp_kernel<4>;
+    }
+}
+
+int batch_blocks_per_sm(size_t smem, int ring_bands) {
+    void (*k)(BatchArgs) = batch_kernel_of(ring_bands);
+    const int threads = ring_bands ? 256 : dev::kWsThreads;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem);
     return per_sm;
 }
 
-cudaError_t batch(const BatchArgs& a, int grid, bool ring, cudaStream_t s) {
+cudaError_t batch(const BatchArgs& a, int grid, int ring_bands, cudaStream_t s) {
     if (a.n_items <= 0) return cudaSuccess;
-    void (*k)(BatchArgs) = ring ? dev::batch_warp_kernel : dev::batch_kernel;
-    const int threads = ring ? 256 : dev::kWsThreads;
+    void (*k)(BatchArgs) = batch_kernel_of(ring_bands);
+    const int threads = ring_bands ? 256 : dev::kWsThreads;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.smem_bytes);
     k<<<grid, threads, a.smem_bytes, s>>>(a);
     return cudaGetLastError();

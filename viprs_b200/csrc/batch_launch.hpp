@@ -62,12 +62,13 @@ struct BatchArgs {
 };
 
 namespace launch {
-// Launch the persistent kernel on `grid` blocks: the shrink variant
-// (`ring`: independent warps, each with its own stage buffers of
-// a.ring_stage_bytes) or the variant for the other item kinds.
-cudaError_t batch(const BatchArgs& a, int grid, bool ring, cudaStream_t s);
+// Launch the persistent kernel on `grid` blocks: the shrink variant for
+// images of `ring_bands` bands (1..4: independent warps, each with its own
+// stage buffers of a.ring_stage_bytes) or, for ring_bands 0, the variant for
+// the other item kinds.
+cudaError_t batch(const BatchArgs& a, int grid, int ring_bands, cudaStream_t s);
 // Largest resident block count per SM for `smem` bytes of shared memory.
-int batch_blocks_per_sm(size_t smem, bool ring);
+int batch_blocks_per_sm(size_t smem, int ring_bands);
 // Shared memory of the other item kinds' variant ahead of its work region:
 // control block and the queued stage copies.
 size_t batch_ctl_bytes();

@@ -24,7 +24,8 @@ using namespace viprs;
 
 // One launch of the persistent kernel: a contiguous range of the work list.
 struct BatchLaunch {
-    bool ring = false;        // shrink items through the TMA ring
+    bool ring = false;        // shrink items (the warp shrink variant)
+    int32_t bands = 0;        // the band count of every image of a shrink launch
     int64_t offset = 0, count = 0;
     int32_t ring_slots = 0;
     uint32_t work_bytes = 0;
@@ -224,10 +225,13 @@ int build_list(viprs_batch* b) {
     b->launches.clear();
     const size_t ctl = launch::batch_ctl_bytes();
     for (int L = 0; L <= max_level; ++L) {
-        for (int kind = 0; kind < 2; ++kind) {
-            const bool ring = kind == 0;
+        // shrink items of 1, 2, 3 and 4-band images (one launch each, a
+        // kernel specialised to the band count), then the other items
+        for (int kind = 1; kind <= 5; ++kind) {
+            const bool ring = kind <= 4;
             BatchLaunch l;
             l.ring = ring;
+            l.bands = ring ? kind : 0;
             l.offset = int64_t(b->items.size());
             size_t work = 0;
             for (int image : order) {
@@ -236,6 +240,7 @@ int build_list(viprs_batch* b) {
                     const int g = gidx[size_t(image)][j];
                     const BatchStage& s = b->stages[size_t(g)];
                     if ((s.type == kBatchShrink) != ring) continue;
+                    if (ring && s.sh.bands != l.bands) continue;
                     for (int32_t k = 0; k < s.n_items; ++k) b->items.push_back(WorkItem{g, k});
                     if (s.type == kBatchShrink) continue;
                     if (s.type == kBatchReduce2D) work = std::max(work, reduce2d_need(s.r2));
@@ -251,7 +256,7 @@ int build_list(viprs_batch* b) {
             l.ring_slots = 0;
             l.smem = ring ? launch::batch_warp_smem_bytes(b->ring_stage_bytes) : ctl + l.work_bytes;
             if (l.smem > 220 * 1024) return VIPRS_ERR_INVALID_ARGUMENT;
-            int per_sm = launch::batch_blocks_per_sm(l.smem, ring);
+            int per_sm = launch::batch_blocks_per_sm(l.smem, l.bands);
             if (per_sm <= 0) return VIPRS_ERR_INVALID_ARGUMENT;
             if (ring && b->blocks_per_sm > 0) per_sm = std::min(per_sm, b->blocks_per_sm);
             l.grid = int(std::min<int64_t>(int64_t(per_sm) * sm_count(), l.count));
@@ -293,7 +298,7 @@ int launch_batch(viprs_batch* b, const uint64_t* d_srcs, const uint64_t* d_dsts,
         a.ring_slots = l.ring_slots;
         a.work_bytes = l.work_bytes;
         a.smem_bytes = uint32_t(l.smem);
-        e = launch::batch(a, l.grid, l.ring, s);
+        e = launch::batch(a, l.grid, l.bands, s);
         if (e != cudaSuccess) return cuda_status(e);
     }
     return VIPRS_OK;
