@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(256, 3) batch_warp_kernel(BatchArgs g) {
             d->err = g.err;
         }
         __syncwarp();
-        shrink_warp_index<B, false>(*d, it.index, wbuf, p);
+        shrink_warp_index<B, true>(*d, it.index, wbuf, p);
         __syncwarp();
     }
 }
