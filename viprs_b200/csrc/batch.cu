@@ -117,6 +117,9 @@ __device__ void batch_pixel_row(const PixelArgs& a, int32_t ly) {
     }
 }
 
+// R2B 3 or 4: a launch of fused-reduce tiles of R2B-band images only (the
+// code of the other item kinds is left out); 0: every item kind.
+template <int R2B>
 __device__ void batch_consumers(const BatchArgs& g, BatchCtl* ctl, const BatchStage* qstage, uint8_t* work) {
     int q = 0;
     uint32_t qph = 0;
@@ -135,7 +138,10 @@ __device__ void batch_consumers(const BatchArgs& g, BatchCtl* ctl, const BatchSt
         const int32_t index = ctl->cur;
         if (index < 0) break;
         const BatchStage& s = qstage[q];
-        switch (s.type) {
+        if (R2B != 0) {
+            const int nbx = (s.r2.out.w + s.r2.tile_w - 1) / s.r2.tile_w;
+            reduce2d_tile<uint8_t, kReduceFixed, kReduceFixed, R2B>(s.r2, index % nbx, index / nbx, work);
+        } else switch (s.type) {
         case kBatchReduce2D: {
             const int nbx = (s.r2.out.w + s.r2.tile_w - 1) / s.r2.tile_w;
             const int tbx = index % nbx, tby = index / nbx;
@@ -167,6 +173,7 @@ __device__ void batch_consumers(const BatchArgs& g, BatchCtl* ctl, const BatchSt
 
 // The other item kinds (fused reduce tiles, reduce rows, affine and pixel
 // rows), with the work region in shared memory.
+template <int R2B>
 __global__ void __launch_bounds__(kWsThreads, 3) batch_kernel(BatchArgs g) {
     extern __shared__ __align__(128) uint8_t smem_b[];
     BatchCtl* ctl = reinterpret_cast<BatchCtl*>(smem_b);
@@ -186,7 +193,7 @@ __global__ void __launch_bounds__(kWsThreads, 3) batch_kernel(BatchArgs g) {
         batch_producer(g, ctl, qstage);
         return;
     }
-    batch_consumers(g, ctl, qstage, work);
+    batch_consumers<R2B>(g, ctl, qstage, work);
 }
 
 constexpr uint32_t kWarpDesc = (sizeof(ShrinkArgs) + 127) / 128 * 128;
@@ -242,7 +249,9 @@ size_t batch_warp_smem_bytes(uint32_t stage_bytes) {
 // warp shrink of images with ring_bands bands.
 static void (*batch_kernel_of(int ring_bands))(BatchArgs) {
     switch (ring_bands) {
-    case 0: return dev::batch_kernel;
+    case 0: return dev::batch_kernel<0>;
+    case kBatchTile3: return dev::batch_kernel<3>;
+    case kBatchTile4: return dev::batch_kernel<4>;
     case 1: return dev::batch_warp_kernel<1>;
     case 2: return dev::batch_warp_kernel<2>;
     case 3: return dev::batch_warp_kernel<3>;
@@ -252,7 +261,7 @@ static void (*batch_kernel_of(int ring_bands))(BatchArgs) {
 
 int batch_blocks_per_sm(size_t smem, int ring_bands) {
     void (*k)(BatchArgs) = batch_kernel_of(ring_bands);
-    const int threads = ring_bands ? 256 : dev::kWsThreads;
+    const int threads = ring_bands >= 1 && ring_bands <= 4 ? 256 : dev::kWsThreads;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem);
@@ -262,7 +271,7 @@ int batch_blocks_per_sm(size_t smem, int ring_bands) {
 cudaError_t batch(const BatchArgs& a, int grid, int ring_bands, cudaStream_t s) {
     if (a.n_items <= 0) return cudaSuccess;
     void (*k)(BatchArgs) = batch_kernel_of(ring_bands);
-    const int threads = ring_bands ? 256 : dev::kWsThreads;
+    const int threads = ring_bands >= 1 && ring_bands <= 4 ? 256 : dev::kWsThreads;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.smem_bytes);
     k<<<grid, threads, a.smem_bytes, s>>>(a);
     return cudaGetLastError();

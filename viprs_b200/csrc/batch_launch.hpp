@@ -62,10 +62,12 @@ struct BatchArgs {
 };
 
 namespace launch {
+// Variants of the tile kernel: fused-reduce tiles of 3- or 4-band images only.
+constexpr int kBatchTile3 = 13, kBatchTile4 = 14;
 // Launch the persistent kernel on `grid` blocks: the shrink variant for
 // images of `ring_bands` bands (1..4: independent warps, each with its own
-// stage buffers of a.ring_stage_bytes) or, for ring_bands 0, the variant for
-// the other item kinds.
+// stage buffers of a.ring_stage_bytes), the tile variant for every other item
+// kind (0), or a tile variant specialised to kBatchTile3 / kBatchTile4.
 cudaError_t batch(const BatchArgs& a, int grid, int ring_bands, cudaStream_t s);
 // Largest resident block count per SM for `smem` bytes of shared memory.
 int batch_blocks_per_sm(size_t smem, int ring_bands);

@@ -25,7 +25,7 @@ using namespace viprs;
 // One launch of the persistent kernel: a contiguous range of the work list.
 struct BatchLaunch {
     bool ring = false;        // shrink items (the warp shrink variant)
-    int32_t bands = 0;        // the band count of every image of a shrink launch
+    int32_t bands = 0;        // kernel variant: the band count of a shrink launch, else 0 or kBatchTile3/4
     int64_t offset = 0, count = 0;
     int32_t ring_slots = 0;
     uint32_t work_bytes = 0;
@@ -226,12 +226,13 @@ int build_list(viprs_batch* b) {
     const size_t ctl = launch::batch_ctl_bytes();
     for (int L = 0; L <= max_level; ++L) {
         // shrink items of 1, 2, 3 and 4-band images (one launch each, a
-        // kernel specialised to the band count), then the other items
-        for (int kind = 1; kind <= 5; ++kind) {
+        // kernel specialised to the band count), the fused-reduce tiles of 3-
+        // and 4-band images (one launch each), then every other item
+        for (int kind = 1; kind <= 7; ++kind) {
             const bool ring = kind <= 4;
             BatchLaunch l;
             l.ring = ring;
-            l.bands = ring ? kind : 0;
+            l.bands = ring ? kind : (kind == 5 ? launch::kBatchTile3 : kind == 6 ? launch::kBatchTile4 : 0);
             l.offset = int64_t(b->items.size());
             size_t work = 0;
             for (int image : order) {
@@ -241,6 +242,12 @@ int build_list(viprs_batch* b) {
                     const BatchStage& s = b->stages[size_t(g)];
                     if ((s.type == kBatchShrink) != ring) continue;
                     if (ring && s.sh.bands != l.bands) continue;
+                    if (!ring) {
+                        const int tb = s.type == kBatchReduce2D && s.r2.bands == 3   ? launch::kBatchTile3
+                                       : s.type == kBatchReduce2D && s.r2.bands == 4 ? launch::kBatchTile4
+                                                                                      : 0;
+                        if (tb != l.bands) continue;
+                    }
                     for (int32_t k = 0; k < s.n_items; ++k) b->items.push_back(WorkItem{g, k});
                     if (s.type == kBatchShrink) continue;
                     if (s.type == kBatchReduce2D) work = std::max(work, reduce2d_need(s.r2));
