@@ -184,8 +184,8 @@ __host__ __device__ inline StripLayout strip_layout(const StripArgs& a) {
     return L;
 }
 
-// The block's source-row stream: row q of the sequence is plane row
-// row_of(q), staged in slot q % slots by one bulk copy of the 16-byte aligned
+// The block's source-row stream: row q of the sequence is a plane row
+// (clamped to the plane), staged in slot q % slots by one bulk copy of the 16-byte aligned
 // cover of columns [c0, c0 + ncols) (bytes whose cover would pass the end of
 // the buffer by plain loads).  Rows come in batches of kStripBatch sharing one
 // mbarrier; lane 0 of warp w issues row w of a batch and pulls row
@@ -201,8 +201,10 @@ struct StripStream {
     int32_t slots;
 };
 
-template <typename RowOf>
-__device__ __forceinline__ void strip_issue_row(const StripStream& s, RowOf row_of, int32_t batch, int w) {
+// Row batch*kStripBatch + w, whose segment starts at byte s0 of the plane
+// (its plane row clamped to the plane); the prefetch goes kStripPrefetch rows
+// further down (not clamped: a hint, kept inside the buffer).
+__device__ __forceinline__ void strip_issue_row(const StripStream& s, int64_t s0, int32_t batch, int w) {
     uint64_t* bar = &s.bars[batch & (s.slots / kStripBatch - 1)];
     const int32_t q = batch * kStripBatch + w;
     if (q >= s.nrows) {
@@ -211,7 +213,6 @@ __device__ __forceinline__ void strip_issue_row(const StripStream& s, RowOf row_
     }
     uint8_t* dst = s.stage + size_t(q & (s.slots - 1)) * s.stage_bytes;
     const int64_t n = int64_t(s.ncols) * s.bands * 4;
-    const int64_t s0 = row_of(q) * s.in->pitch + s.c0 * s.bands * 4;
     const int64_t e0 = s0 + n;
     const int64_t base = int64_t(reinterpret_cast<uintptr_t>(s.in->data) & 15);  // planes are 4-byte aligned
     const int64_t as = ((base + s0) & ~int64_t(15)) - base;
@@ -231,7 +232,7 @@ __device__ __forceinline__ void strip_issue_row(const StripStream& s, RowOf row_
         bulk_load(dst, s.in->data + as, uint32_t(ae - as), bar);
     }
     if (q + kStripPrefetch < s.nrows) {
-        const int64_t f0 = row_of(q + kStripPrefetch) * s.in->pitch + s.c0 * s.bands * 4;
+        const int64_t f0 = s0 + int64_t(kStripPrefetch) * s.in->pitch;
         const int64_t fa = ((base + f0) & ~int64_t(15)) - base;
         int64_t fe = ((base + f0 + n + 15) & ~int64_t(15)) - base;
         const int64_t lim = ((base + total) & ~int64_t(15)) - base;
@@ -298,11 +299,6 @@ __global__ void __launch_bounds__(kStripThreads, 2) reduce_strip_kernel(StripArg
     // float offset of a staged row's first value in its slot
     const int32_t lead4 = int32_t(((reinterpret_cast<uintptr_t>(a.in.data) + uint64_t(c0) * NB * 4) & 15) >> 2);
     const int64_t iny0 = a.in.y0;
-    // plane row of sequence row q
-    auto row_of = [=](int32_t q) -> int64_t {
-        const int64_t r = HF ? q0 + q - iny0 : q0 + q;
-        return r < 0 ? 0 : (r > phh ? phh : r);
-    };
     const StripStream st{&a.in, bars, stage, SB, c0, C, NB, nrows, P};
     if (tid == 0) {
         for (int i = 0; i < NBAR; ++i) mbar_init(&bars[i], kStripBatch);
@@ -313,9 +309,21 @@ __global__ void __launch_bounds__(kStripThreads, 2) reduce_strip_kernel(StripArg
 
     int32_t issued = 0, waited = 0;  // batches issued / waited for (the same in every thread)
     // issue every batch whose slots hold only rows below `free_below`
+    // lane 0 of each warp keeps the plane row (unclamped) and segment offset
+    // of its next row, warp + kStripBatch * issued, stepping kStripBatch rows
+    // at a time (a multiply only where the clamp to the plane bites)
+    const int64_t seg0 = c0 * NB * 4, pitch = a.in.pitch;
+    int64_t my_raw = (HF ? q0 - iny0 : q0) + warp;
+    auto seg_of = [&](int64_t raw) { return (raw < 0 ? 0 : (raw > phh ? phh : raw)) * pitch + seg0; };
+    int64_t my_off = seg_of(my_raw);
     auto issue_until = [&](int32_t free_below) {
         while (issued * kStripBatch < nrows && (issued + 1) * kStripBatch - P <= free_below) {
-            if (lane == 0) strip_issue_row(st, row_of, issued, warp);
+            if (lane == 0) {
+                strip_issue_row(st, my_off, issued, warp);
+                my_raw += kStripBatch;
+                if (my_raw - kStripBatch >= 0 && my_raw <= phh) my_off += kStripBatch * pitch;
+                else my_off = seg_of(my_raw);
+            }
             ++issued;
         }
     };
