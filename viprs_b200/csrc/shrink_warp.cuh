@@ -33,7 +33,7 @@ namespace viprs {
 namespace dev {
 
 constexpr int kWarpStages = 4;    // source rows in flight to shared memory per warp
-constexpr int kWarpPrefetch = 12;  // rows ahead of the consumed one pulled into L2
+constexpr int kWarpPrefetch = 8;   // rows ahead of the consumed one pulled into L2
 // Shared memory ahead of a warp's stage buffers: its kWarpStages mbarriers.
 constexpr uint32_t kWarpBars = 128;
 
