@@ -24,6 +24,7 @@ using namespace viprs;
 
 // One launch of the persistent kernel: a contiguous range of the work list.
 struct BatchLaunch {
+    int32_t level = 0;        // stage level: launches of one level are independent
     bool ring = false;        // shrink items (the warp shrink variant)
     int32_t bands = 0;        // kernel variant: the band count of a shrink launch, else 0 or kBatchTile3/4
     int64_t offset = 0, count = 0;
@@ -53,6 +54,10 @@ struct viprs_batch {
     int32_t* d_ctrl = nullptr;  // [0] error, [1 + k] cursor of launch k
     size_t counters_cap = 0, stages_cap = 0, items_cap = 0;
     uint32_t ring_stage_bytes = 0;
+    // the 4-band images' launches run on a second stream beside the others
+    // (launches of one level are independent), joined at each level boundary
+    cudaStream_t aux = nullptr;
+    cudaEvent_t ev_main = nullptr, ev_aux = nullptr;
     // captured graph
     cudaGraphExec_t graph = nullptr;
     const uint64_t* graph_srcs = nullptr;
@@ -231,6 +236,7 @@ int build_list(viprs_batch* b) {
         for (int kind = 1; kind <= 7; ++kind) {
             const bool ring = kind <= 4;
             BatchLaunch l;
+            l.level = L;
             l.ring = ring;
             l.bands = ring ? kind : (kind == 5 ? launch::kBatchTile3 : kind == 6 ? launch::kBatchTile4 : 0);
             l.offset = int64_t(b->items.size());
@@ -288,10 +294,27 @@ int build_list(viprs_batch* b) {
 }
 
 int launch_batch(viprs_batch* b, const uint64_t* d_srcs, const uint64_t* d_dsts, cudaStream_t s) {
+    if (!b->aux) return VIPRS_ERR_INVALID_ARGUMENT;
     cudaError_t e = cudaMemsetAsync(b->d_ctrl, 0, (1 + b->launches.size()) * sizeof(int32_t), s);
     if (e != cudaSuccess) return cuda_status(e);
+    // join the two streams: `to` waits for everything enqueued on `from`
+    auto join = [&](cudaStream_t from, cudaEvent_t ev, cudaStream_t to) {
+        cudaError_t r = cudaEventRecord(ev, from);
+        return r == cudaSuccess ? cudaStreamWaitEvent(to, ev, 0) : r;
+    };
+    e = join(s, b->ev_main, b->aux);
+    if (e != cudaSuccess) return cuda_status(e);
+    int level = 0;
     for (size_t k = 0; k < b->launches.size(); ++k) {
         const BatchLaunch& l = b->launches[k];
+        if (l.level != level) {
+            // a new level reads what the previous one wrote on both streams
+            e = join(b->aux, b->ev_aux, s);
+            if (e == cudaSuccess) e = join(s, b->ev_main, b->aux);
+            if (e != cudaSuccess) return cuda_status(e);
+            level = l.level;
+        }
+        const cudaStream_t ls = (l.bands == 4 || l.bands == launch::kBatchTile4) ? b->aux : s;
         BatchArgs a;
         a.stages = b->d_stages;
         a.items = b->d_items + l.offset;
@@ -305,10 +328,11 @@ int launch_batch(viprs_batch* b, const uint64_t* d_srcs, const uint64_t* d_dsts,
         a.ring_slots = l.ring_slots;
         a.work_bytes = l.work_bytes;
         a.smem_bytes = uint32_t(l.smem);
-        e = launch::batch(a, l.grid, l.bands, s);
+        e = launch::batch(a, l.grid, l.bands, ls);
         if (e != cudaSuccess) return cuda_status(e);
     }
-    return VIPRS_OK;
+    e = join(b->aux, b->ev_aux, s);  // the caller's stream ends after both
+    return cuda_status(e);
 }
 
 // A batch of one u8 chain plan per image (`chain_of(i, &chain)` builds image
@@ -331,6 +355,9 @@ int32_t batch_create(int32_t n, const uint32_t* widths, const uint32_t* heights,
     }
     if (st == VIPRS_OK) {
         cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->d_ctrl), (1 + kMaxLaunches) * sizeof(int32_t));
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_main, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_aux, cudaEventDisableTiming);
         st = cuda_status(e);
     }
     if (st == VIPRS_OK) st = build_list(b.get());
@@ -514,6 +541,9 @@ void viprs_batch_destroy(viprs_batch* b) {
     drop_graph(b);
     free_list(b);
     if (b->d_ctrl) cudaFree(b->d_ctrl);
+    if (b->ev_main) cudaEventDestroy(b->ev_main);
+    if (b->ev_aux) cudaEventDestroy(b->ev_aux);
+    if (b->aux) cudaStreamDestroy(b->aux);
     for (auto* p : b->plans) free_plan(p);
     delete b;
 }
