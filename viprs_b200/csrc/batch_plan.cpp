@@ -43,7 +43,7 @@ struct viprs_batch {
     int32_t ring_slots_knob = 0;  // kept for the configuration API; the warp shrink ignores it
     int32_t blocks_per_sm = 0;    // cap of the shrink launches (0 = occupancy maximum)
     uint32_t reduce_smem_budget = 64 * 1024;  // shared memory of one fused-reduce tile
-    int64_t item_bytes = 48 * 1024;           // source bytes per shrink work item
+    int64_t item_bytes = 32 * 1024;           // source bytes per shrink work item
     // device work list
     std::vector<BatchStage> stages;
     std::vector<WorkItem> items;
