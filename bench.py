@@ -53,12 +53,13 @@ if ROOT not in sys.path:
 
 FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (read + write) of one batch step over its algorithmic bytes, from
-# an ncu capture of both persistent launches on the first 64 images
-# (`ncu --set full --clock-control none -k regex:batch_kernel -s 2 -c 2 python bench.py
-# --images 64 --steps 2 --warmup 3 --no-cpu --no-others --no-autotune`: 1.1922 GB against
-# 1,156,046,596 B); every image adds its input once and its shrunk
-# intermediate once, so the ratio carries over to the 512-image step
-BATCH_TRAFFIC_RATIO = 1.1922e9 / 1156046596
+# an ncu capture of one step's persistent launches on the first 64 images
+# (`ncu --clock-control none --metrics dram__bytes_read.sum,dram__bytes_write.sum
+# -k regex:^batch_ -c 5 python bench.py --images 64 --steps 1 --warmup 3 --no-cpu
+# --no-others --no-autotune`, the step's four launches for these images:
+# 1,174,348,288 B against 1,156,046,596 B); every image adds its input once and
+# its shrunk intermediate once, so the ratio carries over to the 512-image step
+BATCH_TRAFFIC_RATIO = 1174348288 / 1156046596
 METRIC = "input Mpix/s batched vs per-image GPU (bit-exact u8); fwd+bwd GB/s vs HBM"
 BATCH_N = 512
 BATCH_SEED = 0x5EED0003
