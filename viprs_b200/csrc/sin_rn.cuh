@@ -24,8 +24,13 @@
 
 #if defined(__CUDACC__)
 #define VIPRS_SIN_HD __host__ __device__ __forceinline__
+// the entry point stays one out-of-line copy in device code: the samplers
+// select their kernel at run time, so an inlined copy per weight would swell
+// every sampler whether it evaluates a Lanczos weight or not
+#define VIPRS_SIN_ENTRY static __host__ __device__ __noinline__
 #else
 #define VIPRS_SIN_HD inline
+#define VIPRS_SIN_ENTRY static inline
 #endif
 
 namespace viprs {
@@ -108,7 +113,7 @@ VIPRS_SIN_HD DD cos_series(DD r) {
 }
 
 // sin(x) rounded to nearest (see the file comment), |x| <= 2^20.
-VIPRS_SIN_HD double sin_rn(double x) {
+VIPRS_SIN_ENTRY double sin_rn(double x) {
     if (!(fabs(x) >= 0x1p-26)) return x;  // |x| < 2^-26 (and NaN): sin(x) rounds to x
     const double pio2_1 = 0x1.921fb54442d18p+0, pio2_2 = 0x1.1a62633145c07p-54, pio2_3 = -0x1.f1976b7ed8fbcp-110;
     const double k = rint(x * 0x1.45f306dc9c883p-1);  // nearest multiple of pi/2
