@@ -55,7 +55,8 @@ struct viprs_batch {
     size_t counters_cap = 0, stages_cap = 0, items_cap = 0;
     uint32_t ring_stage_bytes = 0;
     // the 4-band images' launches run on a second stream beside the others
-    // (launches of one level are independent), joined at each level boundary
+    // (each stream's order carries its images' dependencies), joined around
+    // the launches that hold items of every band count
     cudaStream_t aux = nullptr;
     cudaEvent_t ev_main = nullptr, ev_aux = nullptr;
     // captured graph
@@ -304,17 +305,25 @@ int launch_batch(viprs_batch* b, const uint64_t* d_srcs, const uint64_t* d_dsts,
     };
     e = join(s, b->ev_main, b->aux);
     if (e != cudaSuccess) return cuda_status(e);
-    int level = 0;
+    // A stage reads only its own image's earlier stages, so each stream's own
+    // order carries the dependencies of its images (4-band on aux, the rest on
+    // s).  A generic launch (items of any band count) waits for aux first, and
+    // aux waits for it before its next launch.
+    bool aux_behind = false;
     for (size_t k = 0; k < b->launches.size(); ++k) {
         const BatchLaunch& l = b->launches[k];
-        if (l.level != level) {
-            // a new level reads what the previous one wrote on both streams
-            e = join(b->aux, b->ev_aux, s);
-            if (e == cudaSuccess) e = join(s, b->ev_main, b->aux);
+        const bool on_aux = l.bands == 4 || l.bands == launch::kBatchTile4;
+        if (on_aux && aux_behind) {
+            e = join(s, b->ev_main, b->aux);
             if (e != cudaSuccess) return cuda_status(e);
-            level = l.level;
+            aux_behind = false;
         }
-        const cudaStream_t ls = (l.bands == 4 || l.bands == launch::kBatchTile4) ? b->aux : s;
+        if (!l.ring && l.bands == 0) {
+            e = join(b->aux, b->ev_aux, s);
+            if (e != cudaSuccess) return cuda_status(e);
+            aux_behind = true;
+        }
+        const cudaStream_t ls = on_aux ? b->aux : s;
         BatchArgs a;
         a.stages = b->d_stages;
         a.items = b->d_items + l.offset;
