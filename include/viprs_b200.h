@@ -208,6 +208,14 @@ int32_t viprs_thumbnail_plan_nodes(int32_t target, uint32_t target_width, uint32
                                    uint32_t bands, int32_t allow_shrink_hint, viprs_node *nodes,
                                    int32_t capacity, int32_t *n_nodes, uint32_t *out_width,
                                    uint32_t *out_height, uint32_t *shrink_factor);
+/* Resize::with_gap(gap).into_pipeline_nodes (resize.rs:89-348), host only:
+   the planned nodes (kind 9 = the Zoom upscale, its factors in factor_u /
+   vfactor_u) and the output size.  SIZE_MISMATCH, with *n_nodes set, when
+   `capacity` nodes do not suffice. */
+int32_t viprs_resize_plan_nodes(double hscale, double vscale, int32_t kernel, double gap,
+                                uint32_t width, uint32_t height, viprs_node *nodes,
+                                int32_t capacity, int32_t *n_nodes, uint32_t *out_width,
+                                uint32_t *out_height);
 /* PipelineBuilder::resize(Resize::new(hscale, vscale, kernel)) (builder/resample.rs:637-711). */
 int32_t viprs_resize_plan_create(uint32_t width, uint32_t height, uint32_t bands, int32_t format,
                                  double hscale, double vscale, int32_t kernel,

@@ -200,3 +200,114 @@ def test_oracle_plan_reference_cases(oracle):
     assert nodes[0]["kind"] == "premultiply" and nodes[-1]["kind"] == "unpremultiply"
     nodes, _, _ = oracle.thumbnail_plan(1, 2048, 3, "height", 0, 400, allow_shrink_hint=False)
     assert any(n["kind"] == "affine" and n["kernel"] == 2 and (n["out_w"], n["out_h"]) == (1, 400) for n in nodes)
+
+
+# ---------------------------------------------------------------- resize planner
+# The product's resize planner (plan.cpp) pinned to the reference's own resize
+# tests (resize.rs:392-535) through viprs_resize_plan_nodes (host only).
+
+K_ZOOM = 9
+
+
+def product_resize(w, h, hscale, vscale, kernel="lanczos3", gap=2.0):
+    from viprs_b200 import _native as N
+    from viprs_b200 import api
+    nodes = (N.Node * 16)()
+    n, ow, oh = ctypes.c_int32(), ctypes.c_uint32(), ctypes.c_uint32()
+    st = N.lib().viprs_resize_plan_nodes(float(hscale), float(vscale), api.KERNELS[kernel], float(gap), w, h, nodes,
+                                         16, ctypes.byref(n), ctypes.byref(ow), ctypes.byref(oh))
+    assert st == 0
+    return [nodes[i] for i in range(n.value)], (ow.value, oh.value)
+
+
+def simulated_dimensions(w, h, nodes):
+    from viprs_b200 import _native as N
+    L = N.lib()
+    for n in nodes:
+        if n.kind == K_SHRINKH:
+            w //= n.factor_u
+        elif n.kind == K_SHRINKV:
+            h //= n.factor_u
+        elif n.kind == K_REDUCEH:
+            w = L.viprs_reduce_output_len(n.factor, w)
+        elif n.kind == K_REDUCEV:
+            h = L.viprs_reduce_output_len(n.factor, h)
+        elif n.kind == K_ZOOM:
+            w, h = w * n.factor_u, h * n.vfactor_u
+        elif n.kind == K_AFFINE:
+            w, h = n.out_width, n.out_height
+    return w, h
+
+
+def test_resize_downscale_4x_shrink2_reduce2_default_gap():
+    # resize.rs:399-412
+    nodes, _ = product_resize(128, 128, 0.25, 0.25)
+    assert [n.kind for n in nodes] == [K_SHRINKV, K_SHRINKH, K_REDUCEV, K_REDUCEH]
+    assert nodes[0].factor_u == 2 and nodes[1].factor_u == 2
+    assert abs(nodes[2].factor - 2.0) < 1e-9 and abs(nodes[3].factor - 2.0) < 1e-9
+
+
+def test_resize_downscale_4x_gap1_full_integer_shrink():
+    # resize.rs:414-426
+    nodes, _ = product_resize(128, 128, 0.25, 0.25, gap=1.0)
+    assert [(n.kind, n.factor_u) for n in nodes] == [(K_SHRINKV, 4), (K_SHRINKH, 4)]
+
+
+def test_resize_nearest_downscale_skips_prefilter_shrink():
+    # resize.rs:428-439
+    from viprs_b200 import api
+    nodes, _ = product_resize(128, 128, 0.25, 0.25, kernel="nearest")
+    assert [n.kind for n in nodes] == [K_REDUCEV, K_REDUCEH]
+    assert all(abs(n.factor - 4.0) < 1e-9 and n.kernel == api.KERNELS["nearest"] for n in nodes)
+
+
+def test_resize_mixed_down_and_up():
+    # resize.rs:441-458
+    from viprs_b200 import api
+    nodes, _ = product_resize(100, 100, 0.5, 2.5, kernel="bilinear")
+    assert nodes[0].kind == K_REDUCEH and abs(nodes[0].factor - 2.0) < 1e-9
+    assert nodes[0].kernel == api.KERNELS["bilinear"]
+    assert nodes[1].kind == K_ZOOM and (nodes[1].factor_u, nodes[1].vfactor_u) == (1, 2)
+    assert nodes[2].kind == K_AFFINE
+    assert simulated_dimensions(100, 100, nodes) == (50, 250)
+
+
+def test_resize_lbb_downscale_is_one_affine():
+    # resize.rs:460-470
+    from viprs_b200 import api
+    nodes, _ = product_resize(100, 100, 0.6, 0.6, kernel="lbb")
+    assert len(nodes) == 1 and nodes[0].kind == K_AFFINE and nodes[0].kernel == api.KERNELS["lbb"]
+    assert simulated_dimensions(100, 100, nodes) == (60, 60)
+
+
+def test_resize_lbb_2x_is_affine():
+    # resize.rs:472-486
+    nodes, _ = product_resize(25, 25, 2.0, 2.0, kernel="lbb")
+    assert len(nodes) == 1 and nodes[0].kind == K_AFFINE
+    assert list(nodes[0].matrix) == [0.5, 0.0, 0.0, 0.5] and (nodes[0].out_width, nodes[0].out_height) == (50, 50)
+
+
+def test_resize_nearest_affine_offset_is_zero():
+    # resize.rs:488-499
+    nodes, _ = product_resize(100, 100, 1.5, 1.5, kernel="nearest")
+    assert len(nodes) == 1 and nodes[0].kind == K_AFFINE and (nodes[0].tx, nodes[0].ty) == (0.0, 0.0)
+
+
+def test_resize_vsqbs_2x_affine_not_zoom():
+    # resize.rs:501-516
+    nodes, _ = product_resize(2, 2, 2.0, 2.0, kernel="vsqbs")
+    assert len(nodes) == 1 and nodes[0].kind == K_AFFINE
+    n = nodes[0]
+    assert list(n.matrix) == [0.5, 0.0, 0.0, 0.5] and abs(n.tx - 0.25) < 1e-12 and abs(n.ty - 0.25) < 1e-12
+    assert (n.out_width, n.out_height) == (4, 4)
+
+
+def test_resize_plan_dimensions_match_requested_scales():
+    # resize.rs:518-535 (property)
+    rng = np.random.default_rng(11)
+    for _ in range(400):
+        w, h = (int(v) for v in rng.integers(1, 257, 2))
+        hs, vs = (float(v) for v in rng.uniform(0.05, 4.0, 2))
+        nodes, (ow, oh) = product_resize(w, h, hs, vs)
+        assert ow == max(1, int(np.floor(w * hs + 0.5))) and oh == max(1, int(np.floor(h * vs + 0.5)))
+        assert simulated_dimensions(w, h, nodes) == (ow, oh)

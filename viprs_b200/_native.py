@@ -57,6 +57,8 @@ SIGNATURES = {
     "viprs_plan_status": (_I, [_P, _P]),
     "viprs_thumbnail_plan_nodes": (_I, [_I, _U, _U, _I, _I, _U, _U, _U, _I, _P, _I, ctypes.POINTER(_I),
                                        ctypes.POINTER(_U), ctypes.POINTER(_U), ctypes.POINTER(_U)]),
+    "viprs_resize_plan_nodes": (_I, [_D, _D, _I, _D, _U, _U, _P, _I, ctypes.POINTER(_I), ctypes.POINTER(_U),
+                                    ctypes.POINTER(_U)]),
     "viprs_reduce_output_len": (_U, [_D, _U]),
     "viprs_reduce_kernel_table": (_I, [_D, _I, ctypes.POINTER(_I), _P]),
     "viprs_reduceh": (_I, [_IMG, _IMG, _D, _I, _P]),

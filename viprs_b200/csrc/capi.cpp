@@ -872,6 +872,29 @@ int32_t viprs_chain_plan_create(uint32_t w, uint32_t h, uint32_t bands, int32_t 
     return create_chain_plan_a(w, h, bands, format, c, out);
 }
 
+// The C-ABI form of planned nodes (kind 9 = the Zoom upscale); SIZE_MISMATCH
+// when `capacity` nodes do not suffice.
+static int32_t export_nodes(const std::vector<PlanNode>& planned, viprs_node* nodes, int32_t capacity) {
+    if (int64_t(planned.size()) > capacity) return VIPRS_ERR_SIZE_MISMATCH;
+    for (size_t i = 0; i < planned.size(); ++i) {
+        const PlanNode& n = planned[i];
+        viprs_node v;
+        std::memset(&v, 0, sizeof(v));
+        v.kind = int32_t(n.kind);
+        v.factor_u = n.kind == NodeKind::Zoom ? n.zx : n.ufactor;
+        v.vfactor_u = n.kind == NodeKind::Zoom ? n.zy : n.vufactor;
+        v.ceil_mode = n.ceil ? 1 : 0;
+        v.factor = n.factor; v.vfactor = n.vfactor; v.kernel = int32_t(n.kernel);
+        std::memcpy(v.matrix, n.m, sizeof(v.matrix));
+        v.tx = n.tx; v.ty = n.ty; v.out_width = n.out_w; v.out_height = n.out_h;
+        v.extend = int32_t(n.extend); v.background = n.background; v.premultiplied = n.premultiplied ? 1 : 0;
+        v.area_x = n.ex; v.area_y = n.ey; v.area_width = n.ew; v.area_height = n.eh;
+        v.demand_hint = int32_t(n.demand);
+        nodes[i] = v;
+    }
+    return VIPRS_OK;
+}
+
 int32_t viprs_thumbnail_plan_nodes(int32_t target, uint32_t tw, uint32_t th, int32_t kernel, int32_t crop,
                                    uint32_t w, uint32_t h, uint32_t bands, int32_t allow_shrink_hint,
                                    viprs_node* nodes, int32_t capacity, int32_t* n_nodes, uint32_t* out_w,
@@ -885,22 +908,21 @@ int32_t viprs_thumbnail_plan_nodes(int32_t target, uint32_t tw, uint32_t th, int
     *out_w = plan.output_width;
     *out_h = plan.output_height;
     *shrink_factor = plan.shrink_factor;
-    if (int64_t(plan.nodes.size()) > capacity) return VIPRS_ERR_SIZE_MISMATCH;
-    for (size_t i = 0; i < plan.nodes.size(); ++i) {
-        const PlanNode& n = plan.nodes[i];
-        viprs_node v;
-        std::memset(&v, 0, sizeof(v));
-        v.kind = int32_t(n.kind);
-        v.factor_u = n.ufactor; v.vfactor_u = n.vufactor; v.ceil_mode = n.ceil ? 1 : 0;
-        v.factor = n.factor; v.vfactor = n.vfactor; v.kernel = int32_t(n.kernel);
-        std::memcpy(v.matrix, n.m, sizeof(v.matrix));
-        v.tx = n.tx; v.ty = n.ty; v.out_width = n.out_w; v.out_height = n.out_h;
-        v.extend = int32_t(n.extend); v.background = n.background; v.premultiplied = n.premultiplied ? 1 : 0;
-        v.area_x = n.ex; v.area_y = n.ey; v.area_width = n.ew; v.area_height = n.eh;
-        v.demand_hint = int32_t(n.demand);
-        nodes[i] = v;
-    }
-    return VIPRS_OK;
+    return export_nodes(plan.nodes, nodes, capacity);
+}
+
+int32_t viprs_resize_plan_nodes(double hscale, double vscale, int32_t kernel, double gap, uint32_t w, uint32_t h,
+                                viprs_node* nodes, int32_t capacity, int32_t* n_nodes, uint32_t* out_w,
+                                uint32_t* out_h) {
+    if (!n_nodes || !out_w || !out_h || (capacity > 0 && !nodes)) return VIPRS_ERR_NULL_POINTER;
+    if (capacity < 0 || !(hscale > 0.0) || !(vscale > 0.0) || !std::isfinite(hscale) || !std::isfinite(vscale))
+        return VIPRS_ERR_INVALID_ARGUMENT;
+    if (kernel < 0 || kernel > 9) return VIPRS_ERR_INVALID_KERNEL;
+    const ResizePlan plan = resize_plan(hscale, vscale, Kernel(kernel), gap, w, h);
+    *n_nodes = int32_t(plan.nodes.size());
+    *out_w = plan.output_width;
+    *out_h = plan.output_height;
+    return export_nodes(plan.nodes, nodes, capacity);
 }
 
 int32_t viprs_thumbnail_plan_create(uint32_t w, uint32_t h, uint32_t bands, int32_t format, int32_t target,
