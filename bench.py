@@ -485,6 +485,31 @@ def other_resize_f32(stream, steps):
             "launches": plan.launches}
 
 
+def other_resize_up(stream, steps):
+    """resize 2.0 of 4096x3072x3 u8 (one Zoom(2, 2) node) and resize 2.5 of
+    1024x768x3 u8 (Zoom(2, 2) + the Copy-extend Lanczos3 affine tail)."""
+    import torch
+
+    from viprs_b200 import api, synth
+    img = synth.smooth_u8(3072, 4096, 3, 0x5EED000B)
+    plan = api.resize_plan(4096, 3072, 3, torch.uint8, 2.0)
+    out = torch.empty(plan.out_shape, dtype=torch.uint8, device="cuda")
+    ms = timed(lambda: plan(img, out), steps, 3, stream)
+    b = img.numel() + out.numel()
+    small = synth.smooth_u8(768, 1024, 3, 0x5EED000C)
+    plan2 = api.resize_plan(1024, 768, 3, torch.uint8, 2.5)
+    out2 = torch.empty(plan2.out_shape, dtype=torch.uint8, device="cuda")
+    ms2 = timed(lambda: plan2(small, out2), steps, 3, stream)
+    peak, _ = measured_hbm_peak()
+    return {"workload": "resize 2.0 of 4096x3072x3 u8 (Zoom 2x2, 16-byte stores)",
+            "mpix_per_s": round(out.numel() / 3 / 1e6 / (ms / 1e3), 1), "ms": round(ms, 4),
+            "algorithmic_bytes": b, "gbs": round(b / (ms / 1e3) / 1e9, 1),
+            "frac": round(b / (ms / 1e3) / 1e9 / peak, 4), "launches": plan.launches,
+            "resize_2_5_1024x768": {"workload": "resize 2.5 Lanczos3 1024x768x3 u8 (Zoom 2x2 + affine 1.25)",
+                                    "ms": round(ms2, 4), "launches": plan2.launches,
+                                    "mpix_per_s": round(out2.numel() / 3 / 1e6 / (ms2 / 1e3), 1)}}
+
+
 def other_reduce_affine_grad(stream, steps):
     """16 x 1024^2 x 4 f32: reduce_h(2)+reduce_v(2) -> affine bilinear 512^2 (alpha path), fwd + bwd."""
     import torch
@@ -601,7 +626,8 @@ def other_mapim_grad(stream, steps):
 
 OTHERS = (("thumbnail_8192", other_thumbnail_8192), ("reduce_1024x768", other_reduce_1024),
           ("reduce_1024x768_x256", other_reduce_1024_batch),
-          ("resize_f32_6000x4000", other_resize_f32), ("reduce_affine_fwd_bwd", other_reduce_affine_grad),
+          ("resize_f32_6000x4000", other_resize_f32), ("resize_up", other_resize_up),
+          ("reduce_affine_fwd_bwd", other_reduce_affine_grad),
           ("mapim_fwd_bwd", other_mapim_grad))
 
 

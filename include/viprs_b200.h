@@ -72,7 +72,9 @@ typedef enum {
     VIPRS_THUMB_HEIGHT = 3
 } viprs_thumb_target;
 
-/* An image buffer.  row_stride is in bytes; 0 means width*bands*sample size. */
+/* An image buffer.  row_stride is in bytes; 0 means width*bands*sample size.
+   A nonzero stride is a multiple of the sample size and at least that size
+   (else INVALID_ARGUMENT). */
 typedef struct {
     void *data;
     uint32_t width;
@@ -123,6 +125,12 @@ int32_t viprs_shrinkv(const viprs_image *in, const viprs_image *out, uint32_t fa
 /* PipelineBuilder::shrink -> Shrink::process_region (resample/shrink.rs:179-293). */
 int32_t viprs_shrink(const viprs_image *in, const viprs_image *out, uint32_t hfactor,
                      uint32_t vfactor, void *stream);
+/* PipelineBuilder::zoom -> Zoom::process_region (structural/zoom.rs:310-398;
+   builder/geometry.rs:618-643): integer nearest-neighbour upscale, output
+   (x, y) = input (x / xfac, y / yfac), output size width*xfac x height*yfac.
+   A zero factor is INVALID_ARGUMENT. */
+int32_t viprs_zoom(const viprs_image *in, const viprs_image *out, uint32_t xfac, uint32_t yfac,
+                   void *stream);
 /* PipelineBuilder::premultiply -> Premultiply<U8> (structural/premultiply.rs:84-121). */
 int32_t viprs_premultiply(const viprs_image *in, const viprs_image *out, void *stream);
 /* PipelineBuilder::unpremultiply -> Unpremultiply<U8|F32> (structural/unpremultiply.rs:76-175). */
@@ -154,8 +162,9 @@ int32_t viprs_mapim(const viprs_image *src, const viprs_image *index, const vipr
 typedef enum {
     VIPRS_NODE_PREMULTIPLY = 1, VIPRS_NODE_SHRINKH = 2, VIPRS_NODE_SHRINKV = 3,
     VIPRS_NODE_REDUCEH = 4, VIPRS_NODE_REDUCEV = 5, VIPRS_NODE_AFFINE = 6,
-    VIPRS_NODE_EXTRACT_AREA = 7, VIPRS_NODE_UNPREMULTIPLY = 8, VIPRS_NODE_REDUCE = 10,
-    VIPRS_NODE_SHRINK = 11
+    VIPRS_NODE_EXTRACT_AREA = 7, VIPRS_NODE_UNPREMULTIPLY = 8,
+    VIPRS_NODE_ZOOM = 9,    /* factors in factor_u (x) / vfactor_u (y) */
+    VIPRS_NODE_REDUCE = 10, VIPRS_NODE_SHRINK = 11
 } viprs_node_kind;
 
 /* DemandHint (crates/viprs-core/src/op/demand.rs:14-27). */

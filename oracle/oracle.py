@@ -21,7 +21,7 @@ KERNELS = {
 FORMATS = {np.dtype(np.uint8): 0, np.dtype(np.uint16): 1, np.dtype(np.float32): 2}
 TARGETS = {"fitbox": 0, "force": 1, "width": 2, "height": 3}
 OP = {"shrinkh": 1, "shrinkv": 2, "reduceh": 3, "reducev": 4, "reduce": 5,
-      "premultiply": 6, "unpremultiply": 7, "affine": 8, "shrink": 9, "extract": 10}
+      "premultiply": 6, "unpremultiply": 7, "affine": 8, "shrink": 9, "extract": 10, "zoom": 11}
 DEMAND = {"any": 0, "thin": 1, "fat": 2, "smalltile": 3, "full": 4, "oneline": 5}
 EXTEND = {"black": 0, "white": 1, "background": 2, "copy": 3, "repeat": 4, "mirror": 5}
 PLAN_KINDS = {1: "premultiply", 2: "shrinkh", 3: "shrinkv", 4: "reduceh", 5: "reducev",
@@ -223,7 +223,7 @@ def thumbnail(img, target="width", tw=0, th=0, kernel="lanczos3", crop=False, th
 
 
 def resize(img, hscale, vscale=None, kernel="lanczos3", threads=1):
-    """PipelineBuilder::resize (builder/resample.rs:637-711); Zoom is not restated."""
+    """PipelineBuilder::resize (builder/resample.rs:637-711), the Zoom upscale included."""
     a = _as_image(img)
     h, w, b = a.shape
     vscale = hscale if vscale is None else vscale
@@ -237,6 +237,11 @@ def resize(img, hscale, vscale=None, kernel="lanczos3", threads=1):
     if st:
         raise ValueError(f"resize failed: status {st}")
     return out
+
+
+def zoom(img, xfac, yfac, threads=1):
+    """PipelineBuilder::zoom (builder/geometry.rs:618-643, structural/zoom.rs)."""
+    return pipeline(img, [make_node("zoom", demand="fat", ufactor=xfac, ceil_mode=yfac)], threads=threads)
 
 
 def reduce_h(img, factor, kernel="lanczos3", threads=1):

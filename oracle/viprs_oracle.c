@@ -601,6 +601,23 @@ static void reduce_process(const node_rt *nd, const tile_t *in, tile_t *out) {
     free(mid.data);
 }
 
+/* ---------------- zoom ---------------- */
+/* Zoom::process_region (structural/zoom.rs:44-149): output pixel (x, y)
+   repeats input pixel (x / xfac, y / yfac) in image coordinates; every tile
+   shape gives the same pixels. */
+static void zoom_process(const node_rt *nd, const tile_t *in, tile_t *out) {
+    const int64_t zx = nd->n.ufactor, zy = nd->n.ceil_mode;
+    const size_t px = (size_t)in->bands * fmt_size(in->fmt);
+    for (int64_t yy = 0; yy < out->r.h; yy++) {
+        const int64_t sy = (out->r.y + yy) / zy - in->r.y;
+        for (int64_t xx = 0; xx < out->r.w; xx++) {
+            const int64_t sx = (out->r.x + xx) / zx - in->r.x;
+            memcpy((uint8_t *)out->data + ((size_t)yy * (size_t)out->r.w + (size_t)xx) * px,
+                   (const uint8_t *)in->data + ((size_t)sy * (size_t)in->r.w + (size_t)sx) * px, px);
+        }
+    }
+}
+
 /* ---------------- premultiply / unpremultiply (u8) ---------------- */
 static void premultiply_process(const tile_t *in, tile_t *out) {
     const size_t bands = (size_t)in->bands, n = (size_t)in->r.w * (size_t)in->r.h;
@@ -980,6 +997,13 @@ static int32_t node_out_dims(const or_node *n, uint32_t iw, uint32_t ih, uint32_
     case OR_OP_REDUCE: *ow = reduce_output_len(n->factor, iw); *oh = reduce_output_len(n->vfactor, ih); return OR_OK;
     case OR_OP_AFFINE: *ow = n->out_w; *oh = n->out_h; return OR_OK;
     case OR_OP_EXTRACT: *ow = n->ew; *oh = n->eh; return OR_OK;
+    case OR_OP_ZOOM:
+        /* ZoomBridge::output_width/height (conversion/zoom.rs:108-115); a zero
+           factor is a build error (builder/geometry.rs:618-624) */
+        if (n->ufactor == 0 || n->ceil_mode <= 0) return OR_EINVAL;
+        if ((uint64_t)iw * n->ufactor > 0xFFFFFFFFull || (uint64_t)ih * (uint32_t)n->ceil_mode > 0xFFFFFFFFull)
+            return OR_EINVAL;
+        *ow = iw * n->ufactor; *oh = ih * (uint32_t)n->ceil_mode; return OR_OK;
     default: *ow = iw; *oh = ih; return OR_OK;
     }
 }
@@ -1021,6 +1045,13 @@ static reg_t node_required(const node_rt *nd, reg_t out) {
     case OR_OP_REDUCE: r = cfg_region_h(&nd->rk, cfg_region_v(&nd->rk2, out)); break;
     case OR_OP_AFFINE: r = affine_region(nd, out); break;
     case OR_OP_EXTRACT: r.x = out.x + nd->n.ex; r.y = out.y + nd->n.ey; break;
+    case OR_OP_ZOOM: {
+        /* Zoom::required_input_region (structural/zoom.rs:343-349) */
+        const int64_t zx = nd->n.ufactor, zy = nd->n.ceil_mode;
+        if (out.w > 0) { r.x = out.x / zx; r.w = (out.x + out.w - 1) / zx - r.x + 1; }
+        if (out.h > 0) { r.y = out.y / zy; r.h = (out.y + out.h - 1) / zy - r.y + 1; }
+        break;
+    }
     default: break;
     }
     return r;
@@ -1051,6 +1082,7 @@ static void node_process(const node_rt *nd, const tile_t *in, tile_t *out) {
     case OR_OP_UNPREMULTIPLY: unpremultiply_process(in, out); break;
     case OR_OP_AFFINE: affine_process(nd, in, out); break;
     case OR_OP_EXTRACT: memcpy(out->data, in->data, (size_t)out->r.w * out->r.h * out->bands * fmt_size(out->fmt)); break;
+    case OR_OP_ZOOM: zoom_process(nd, in, out); break;
     default: break;
     }
 }
@@ -1458,7 +1490,12 @@ static int32_t materialise(const or_plan_node *pn, int32_t np, int32_t thumb_lar
         case OR_TN_EXTRACT:
             nd.kind = OR_OP_EXTRACT; nd.ex = pn[i].ex; nd.ey = pn[i].ey; nd.ew = pn[i].ew; nd.eh = pn[i].eh;
             break;
-        default: return OR_EFORMAT; /* Zoom is not part of this restatement */
+        case OR_TN_ZOOM:
+            /* PipelineBuilder::zoom (builder/geometry.rs:618-643); ZoomBridge's hint is FatStrip */
+            nd.kind = OR_OP_ZOOM; nd.ufactor = pn[i].zx; nd.ceil_mode = (int32_t)pn[i].zy;
+            nd.demand_hint = OR_DH_FAT;
+            break;
+        default: return OR_EFORMAT;
         }
         out[n++] = nd;
     }

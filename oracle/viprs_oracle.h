@@ -48,7 +48,8 @@ enum { OR_EXT_BLACK = 0, OR_EXT_WHITE = 1, OR_EXT_BACKGROUND = 2, OR_EXT_COPY = 
 /* Op kinds of the restated pipeline. */
 enum { OR_OP_SHRINKH = 1, OR_OP_SHRINKV = 2, OR_OP_REDUCEH = 3, OR_OP_REDUCEV = 4,
        OR_OP_REDUCE = 5, OR_OP_PREMULTIPLY = 6, OR_OP_UNPREMULTIPLY = 7,
-       OR_OP_AFFINE = 8, OR_OP_SHRINK = 9, OR_OP_EXTRACT = 10 };
+       OR_OP_AFFINE = 8, OR_OP_SHRINK = 9, OR_OP_EXTRACT = 10,
+       OR_OP_ZOOM = 11 /* ufactor = x factor, ceil_mode = y factor */ };
 
 /* Status codes. */
 enum { OR_OK = 0, OR_EINVAL = 1, OR_ETAPS = 2, OR_ENOMEM = 3, OR_EFORMAT = 4 };

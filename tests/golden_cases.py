@@ -91,6 +91,10 @@ CASES = {
     "resize_libvips__smooth_gradient_linear_0_75x_cache.bin":
         (lambda: smooth_grayscale_source(4, 4), [("resize", dict(hscale=0.75, vscale=0.75, kernel="bilinear"))],
          (3, 3, 1), 0),
+    # 2x nearest: the resize plan is one Zoom(2, 2) node (resize.rs:240-263)
+    "resize_libvips__smooth_gradient_nearest_2x.bin":
+        (lambda: smooth_grayscale_source(4, 4), [("resize", dict(hscale=2.0, vscale=2.0, kernel="nearest"))],
+         (8, 8, 1), 0),
     "resize_libvips__smooth_gradient_cubic_0_75x.bin":
         (lambda: smooth_grayscale_source(4, 4), [("resize", dict(hscale=0.75, vscale=0.75, kernel="bicubic"))],
          (3, 3, 1), 0),

@@ -53,6 +53,31 @@ def test_chain_batch_reduce_uneven(oracle):
         assert np.array_equal(host(og), exp)
 
 
+def test_chain_batch_zoom(oracle):
+    """ChainBatch with a Zoom node after a reduce: the generic persistent
+    launch's pixel rows, bit-exact per image."""
+    rng = np.random.default_rng(0x5EED0009)
+    shapes = [(301, 457, 3), (64, 64, 4), (97, 89, 1)]
+    imgs = [torch.from_numpy(rng.integers(0, 256, s, dtype=np.uint8)).cuda() for s in shapes]
+    builder = api.PipelineBuilder(457, 301, 3, torch.uint8).reduce_h(2.0).zoom(3, 2)
+    batch = api.ChainBatch(shapes, builder)
+    outs = batch.run(imgs, graph=False)
+    for img, out in zip(imgs, outs):
+        exp = oracle.pipeline(host(img), [oracle.make_node("reduceh", factor=2.0, kernel="lanczos3"),
+                                          oracle.make_node("zoom", demand="fat", ufactor=3, ceil_mode=2)])
+        assert np.array_equal(host(out), exp)
+
+
+def test_resize_1024x768x3_upscale_2_5(oracle):
+    """Resize 2.5 of a 1024x768x3 u8 image: Zoom(2, 2) then the Copy-extend
+    Lanczos3 affine tail at 1.25, against the oracle."""
+    img = synth.smooth_u8(768, 1024, 3, 0x5EED000A)
+    got = host(api.resize(img, 2.5, 2.5, "lanczos3"))
+    exp = oracle.resize(host(img), 2.5, 2.5, "lanczos3", threads=THREADS)
+    assert got.shape == (1920, 2560, 3)
+    assert np.array_equal(got, exp)
+
+
 def test_chain_batch_reduce_1024x768_x256(oracle):
     """The batched 1024x768x3 workload of the benchmark (256 images)."""
     n = 256

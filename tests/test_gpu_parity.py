@@ -167,6 +167,40 @@ def test_resize(oracle, fmt, scale):
     assert_same(got, oracle.resize(img, scale, scale, "lanczos3"), fmt)
 
 
+@pytest.mark.parametrize("fmt", FMTS)
+@pytest.mark.parametrize("fac", [(1, 1), (2, 3), (3, 1), (1, 2), (5, 4)])
+@pytest.mark.parametrize("bands", [1, 3, 4])
+def test_zoom(oracle, fmt, fac, bands):
+    """Zoom: integer nearest-neighbour upscale (structural/zoom.rs), odd widths
+    so that rows start off 16-byte boundaries."""
+    rng = np.random.default_rng(fac[0] * 7 + fac[1] + bands)
+    img = rand_image(rng, 37, 53, bands, fmt)
+    got = to_host(api.zoom(to_dev(img), fac[0], fac[1]))
+    exp = oracle.zoom(img, fac[0], fac[1])
+    assert np.array_equal(exp, np.repeat(np.repeat(img, fac[1], 0), fac[0], 1))
+    assert got.shape == exp.shape and np.array_equal(got, exp)
+
+
+def test_zoom_zero_factor_is_an_error():
+    img = to_dev(np.zeros((4, 4, 1), np.uint8))
+    with pytest.raises(ViprsError):
+        api.zoom(img, 0, 2)
+
+
+@pytest.mark.parametrize("fmt", FMTS)
+@pytest.mark.parametrize("kernel", ["nearest", "bilinear", "bicubic", "lanczos3"])
+@pytest.mark.parametrize("scales", [(2.0, 2.0), (2.5, 2.5), (3.7, 1.6), (0.6, 2.3), (2.2, 0.45)])
+def test_resize_upscale(oracle, fmt, kernel, scales):
+    """Resize plans with the Zoom upscale (resize.rs:240-277): Zoom alone,
+    Zoom + Copy-extend affine tail, and mixed down/up plans."""
+    rng = np.random.default_rng(int(scales[0] * 100 + scales[1] * 10) + len(kernel))
+    img = rand_image(rng, 61, 83, 3, fmt)
+    plan, _ = oracle.resize_plan(83, 61, scales[0], scales[1], kernel)
+    assert any(n["kind"] == "zoom" for n in plan)
+    got = to_host(api.resize(to_dev(img), scales[0], scales[1], kernel))
+    assert_same(got, oracle.resize(img, scales[0], scales[1], kernel), fmt)
+
+
 def _rot(theta, s):
     return [s * np.cos(theta), -s * np.sin(theta), s * np.sin(theta), s * np.cos(theta)]
 

@@ -311,3 +311,38 @@ def test_resize_plan_dimensions_match_requested_scales():
         nodes, (ow, oh) = product_resize(w, h, hs, vs)
         assert ow == max(1, int(np.floor(w * hs + 0.5))) and oh == max(1, int(np.floor(h * vs + 0.5)))
         assert simulated_dimensions(w, h, nodes) == (ow, oh)
+
+
+def _host_image(buf, w, h, bands, fmt, stride=0):
+    from viprs_b200 import _native
+    im = _native.Image()
+    im.data = ctypes.cast(buf, ctypes.c_void_p)
+    im.width, im.height, im.bands, im.format, im.row_stride = w, h, bands, fmt, stride
+    return im
+
+
+def test_zoom_parameter_errors_before_any_device_work():
+    """PipelineBuilder::zoom rejects a zero factor (builder/geometry.rs:618-624):
+    the status comes from the host checks, before any allocation or launch, so
+    host buffers that are never touched stand in for the images."""
+    from viprs_b200 import _native
+    lib = _native.lib()
+    buf = (ctypes.c_uint8 * 64)()
+    src = _host_image(buf, 4, 4, 1, 0)
+    dst = _host_image(buf, 8, 8, 1, 0)
+    assert lib.viprs_zoom(ctypes.byref(src), ctypes.byref(dst), 0, 2, None) == 1
+    assert lib.viprs_zoom(ctypes.byref(src), ctypes.byref(dst), 2, 0, None) == 1
+    # output larger than 2^32 - 1 pixels along an axis
+    assert lib.viprs_zoom(ctypes.byref(src), ctypes.byref(dst), 0x40000000, 1, None) == 1
+
+
+@pytest.mark.parametrize("fmt,stride", [(1, 9), (2, 10), (0, 3), (2, 12)])
+def test_row_stride_must_hold_whole_samples(fmt, stride):
+    """A row stride that is not a multiple of the sample size, or shorter than
+    a row, is INVALID_ARGUMENT before any device work."""
+    from viprs_b200 import _native
+    lib = _native.lib()
+    buf = (ctypes.c_uint8 * 256)()
+    src = _host_image(buf, 4, 4, 1, fmt, stride)
+    dst = _host_image(buf, 8, 8, 1, fmt)
+    assert lib.viprs_zoom(ctypes.byref(src), ctypes.byref(dst), 2, 2, None) == 1

@@ -67,6 +67,7 @@ SIGNATURES = {
     "viprs_shrinkh": (_I, [_IMG, _IMG, _U, _I, _P]),
     "viprs_shrinkv": (_I, [_IMG, _IMG, _U, _I, _P]),
     "viprs_shrink": (_I, [_IMG, _IMG, _U, _U, _P]),
+    "viprs_zoom": (_I, [_IMG, _IMG, _U, _U, _P]),
     "viprs_premultiply": (_I, [_IMG, _IMG, _P]),
     "viprs_unpremultiply": (_I, [_IMG, _IMG, _P]),
     "viprs_affine": (_I, [_IMG, _IMG, ctypes.POINTER(_D), _D, _D, _I, _P]),

@@ -24,7 +24,7 @@ EXTEND = {"black": 0, "white": 1, "background": 2, "copy": 3, "repeat": 4, "mirr
 TARGETS = {"fitbox": 0, "force": 1, "force_exact": 1, "width": 2, "height": 3}
 DEMAND = {"any": 0, "thin": 1, "thin_strip": 1, "fat": 2, "smalltile": 3, "small_tile": 3, "full": 4, "oneline": 5}
 NODE = {"premultiply": 1, "shrink_h": 2, "shrink_v": 3, "reduce_h": 4, "reduce_v": 5, "affine": 6,
-        "extract_area": 7, "unpremultiply": 8, "reduce": 10, "shrink": 11}
+        "extract_area": 7, "unpremultiply": 8, "zoom": 9, "reduce": 10, "shrink": 11}
 
 
 def _dtype_format(dtype):
@@ -121,6 +121,16 @@ def shrink(t, hfactor, vfactor):
     h, w, b = t.shape
     out = _empty(h // vfactor if vfactor > 0 else 0, w // hfactor if hfactor > 0 else 0, b, t)
     N.check(N.lib().viprs_shrink(image(t), image(out), int(hfactor), int(vfactor), _stream()), "shrink")
+    return out
+
+
+def zoom(t, xfac, yfac):
+    """PipelineBuilder::zoom: integer nearest-neighbour upscale (structural/zoom.rs)."""
+    t = _as_hwc(t)
+    h, w, b = t.shape
+    # a zero factor is rejected by the library (builder/geometry.rs:618-624), not here
+    out = _empty(h * max(int(yfac), 0), w * max(int(xfac), 0), b, t)
+    N.check(N.lib().viprs_zoom(image(t), image(out), int(xfac), int(yfac), _stream()), "zoom")
     return out
 
 
@@ -349,6 +359,9 @@ class PipelineBuilder:
 
     def extract_area(self, x, y, w, h):
         return self._node("extract_area", area_x=x, area_y=y, area_width=w, area_height=h)
+
+    def zoom(self, xfac, yfac):
+        return self._node("zoom", demand="fat", factor_u=xfac, vfactor_u=yfac)
 
     def thumbnail(self, target="width", target_width=0, target_height=0, kernel="lanczos3", crop=False):
         if self.nodes:

@@ -4,6 +4,7 @@
 
 #include "affine_launch.hpp"
 #include "common.cuh"
+#include "interp_weights.hpp"
 #include "sin_rn.cuh"
 
 namespace viprs {
@@ -12,43 +13,6 @@ namespace dev {
 __device__ __forceinline__ int64_t trunc_i64(double v) {
     // Rust `as i64` for the finite, moderate values reaching here
     return (int64_t)v;
-}
-
-__device__ __forceinline__ double bicubic_w(double x) {
-    x = fabs(x);
-    if (x < 1.0) return fma(2.5 * x, -x, 1.5 * x * x * x) + 1.0;
-    if (x < 2.0) return fma(4.0, -x, fma(2.5 * x, x, -0.5 * x * x * x)) + 2.0;
-    return 0.0;
-}
-
-// InterpolationKernel::interpolate (kernel.rs:133-214); the Lanczos sines are
-// rounded to nearest (sin_rn.cuh), as the platform sin viprs calls rounds them
-__device__ __forceinline__ double kernel_w(int k, double x) {
-    const double eps = 2.220446049250313e-16;
-    const double pi = 3.141592653589793;
-    switch (k) {
-    case 0: return fabs(x) < 0.5 ? 1.0 : 0.0;
-    case 1: x = fabs(x); return x < 1.0 ? 1.0 - x : 0.0;
-    case 2: case 7: case 5: return bicubic_w(x);
-    case 3:
-        x = fabs(x);
-        if (x < 0.5) return fma(2.0 * x, -x, 1.0);
-        if (x < 1.5) return fma(2.5, -x, x * x) + 1.5;
-        return 0.0;
-    case 8: {
-        x = fabs(x);
-        if (x < eps) return 1.0;
-        if (x < 2.0) { const double p = pi * x; return 2.0 * sinrn::sin_rn(p) * sinrn::sin_rn(p / 2.0) / (p * p); }
-        return 0.0;
-    }
-    case 9: {
-        x = fabs(x);
-        if (x < eps) return 1.0;
-        if (x < 3.0) { const double p = pi * x; return 3.0 * sinrn::sin_rn(p) * sinrn::sin_rn(p / 3.0) / (p * p); }
-        return 0.0;
-    }
-    default: return 0.0;
-    }
 }
 
 __device__ __forceinline__ int64_t tile_origin(int64_t v, int64_t off, int64_t t) {
@@ -297,6 +261,80 @@ struct AffineCtx {
         }
         for (int b = 0; b < bands; ++b) out[b] = sample(x, y, b, false, 0, 1.0);
     }
+    // pixel() for the separable kernels with the point-sampling weights of the
+    // pixel's column and row given (kAxisTaps each): the taps, their order, the
+    // weight sum and the fma accumulation of sample() / sbp(), every tap read
+    // once for all bands.  x and y are finite (per-axis table positions).
+    template <int NB = 0>
+    __device__ void pixel_tab(double x, double y, const double* wxs, const double* wys, double* out) const {
+        constexpr int MB = NB > 0 ? NB : 8;
+        const int bands = NB > 0 ? NB : a.bands;
+        const int nt = separable_taps(a.kernel), support = nt / 2;
+        const int64_t tx0 = trunc_i64(floor(x)) - (support - 1), ty0 = trunc_i64(floor(y)) - (support - 1);
+        const bool pm = bands == 4 && !a.premultiplied;
+        const int ab = bands - 1;
+        const double amax = sizeof(T) == 4 ? 1.0 : (sizeof(T) == 2 ? 65535.0 : 255.0);
+        const double f = fill();
+        if (!isfinite(x) || !isfinite(y)) {
+            for (int b = 0; b < bands; ++b) out[b] = f;
+            return;
+        }
+        double wx[kAxisTaps], acc[MB];
+#pragma unroll
+        for (int t = 0; t < kAxisTaps; ++t) wx[t] = wxs[t];
+#pragma unroll
+        for (int b = 0; b < MB; ++b) acc[b] = 0.0;
+        double wsum = 0.0;
+        for (int j = 0; j < nt; ++j) {
+            const double wy = wys[j];
+            if (wy == 0.0) continue;
+            const int64_t iy = ty0 + j;
+#pragma unroll
+            for (int i = 0; i < kAxisTaps; ++i) {
+                if (i >= nt) break;
+                if (wx[i] == 0.0) continue;
+                const double w = wx[i] * wy;
+                wsum += w;
+                bool ok;
+                const T* px = tap(tx0 + i, iy, &ok);
+                if (pm) {
+                    const double av = ok ? (double)px[ab] : f;
+#pragma unroll
+                    for (int b = 0; b < MB; ++b) {
+                        if (b >= ab) break;
+                        const double v = ok ? (double)px[b] : f;
+                        acc[b] = fma(v * (av / amax), w, acc[b]);
+                    }
+                    acc[ab] = fma(av, w, acc[ab]);
+                } else {
+#pragma unroll
+                    for (int b = 0; b < MB; ++b) {
+                        if (b >= bands) break;
+                        const double v = ok ? (double)px[b] : f;
+                        acc[b] = fma(v, w, acc[b]);
+                    }
+                }
+            }
+        }
+        if (pm) {
+            double alpha = wsum > 0.0 ? acc[ab] / wsum : f;
+            alpha = alpha < 0.0 ? 0.0 : (alpha > amax ? amax : alpha);
+            const double na = alpha / amax;
+#pragma unroll
+            for (int b = 0; b < MB; ++b) {
+                if (b >= ab) break;
+                const double p = wsum > 0.0 ? acc[b] / wsum : f;
+                out[b] = na > 0.0 ? p / na : 0.0;
+            }
+            out[ab] = alpha;
+            return;
+        }
+#pragma unroll
+        for (int b = 0; b < MB; ++b) {
+            if (b >= bands) break;
+            out[b] = wsum > 0.0 ? acc[b] / wsum : f;
+        }
+    }
 };
 
 template <typename T>
@@ -441,6 +479,9 @@ __device__ void affine_pixel(const AffineArgs& a, AffineCtx<T>& c, AffineRow& ro
                 v[b] = acc;
             }
         }
+    } else if (a.wx != nullptr && inside) {
+        // separable walk, weights from the per-axis tables
+        c.template pixel_tab<NB>(a.xs[X], a.ys[Y], a.wx + X * kAxisTaps, a.wy + Y * kAxisTaps, v);
     } else {
         double x_in, y_in;
         if (a.separable && a.xs != nullptr && inside) {

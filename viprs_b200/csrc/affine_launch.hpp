@@ -31,6 +31,11 @@ struct AffineArgs {
     int32_t separable = 0;   // b == c == 0: positions from per-axis tables
     const double* xs = nullptr;  // per output column x_in (separable general path)
     const double* ys = nullptr;  // per output row y_in
+    // separable general path, kernels other than nearest / bilinear: the
+    // kAxisTaps point-sampling weights of each output column (wx) and row (wy),
+    // taps floor(x) - (support - 1) onwards, zero past the kernel's taps
+    const double* wx = nullptr;
+    const double* wy = nullptr;
     int32_t unpremul_out = 0;
     int32_t group = 1;       // consecutive output pixels per thread (set by the launcher)
 };
@@ -69,5 +74,11 @@ int affine_stage_setup(const PlanNode& n, uint32_t in_w, uint32_t in_h, uint32_t
 // Per-axis positions of viprs's incremental walk (affine/core.rs:1593-1632)
 // for a diagonal matrix over the tile grid in `a`.
 void affine_axis_tables(const AffineArgs& a, double* xs, double* ys);
+// Per-axis weights of the separable sampler for positions xs / ys (kAxisTaps
+// per output column into wx, per output row into wy); the kernel reads them
+// instead of evaluating InterpolationKernel::interpolate per pixel and band.
+constexpr int kAxisTaps = 6;
+bool affine_weight_tables_apply(const AffineArgs& a);
+void affine_weight_tables(const AffineArgs& a, const double* xs, const double* ys, double* wx, double* wy);
 
 }  // namespace viprs

@@ -10,6 +10,7 @@
 #include <cmath>
 
 #include "affine_launch.hpp"
+#include "interp_weights.hpp"
 #include "viprs_b200.h"
 
 namespace viprs {
@@ -118,6 +119,28 @@ void affine_axis_tables(const AffineArgs& a, double* xs, double* ys) {
         for (int64_t r = Y0; r < int64_t(Y); ++r) y += m[3];
         ys[Y] = y;
     }
+}
+
+bool affine_weight_tables_apply(const AffineArgs& a) {
+    return a.separable && !a.fast && a.kernel != 0 && a.kernel != 1;
+}
+
+void affine_weight_tables(const AffineArgs& a, const double* xs, const double* ys, double* wx, double* wy) {
+    const int nt = separable_taps(a.kernel), support = nt / 2;
+    auto axis = [&](const double* pos, uint32_t n, double* w) {
+        for (uint32_t i = 0; i < n; ++i) {
+            const double p = pos[i];
+            if (!std::isfinite(p)) {  // the kernel fills such pixels without weights
+                for (int t = 0; t < kAxisTaps; ++t) w[size_t(i) * kAxisTaps + t] = 0.0;
+                continue;
+            }
+            const int64_t t0 = int64_t(std::floor(p)) - (support - 1);
+            for (int t = 0; t < kAxisTaps; ++t)
+                w[size_t(i) * kAxisTaps + t] = t < nt ? kernel_w(a.kernel, std::fabs(double(t0 + t) - p)) : 0.0;
+        }
+    };
+    axis(xs, a.total_w, wx);
+    axis(ys, a.total_h, wy);
 }
 
 }  // namespace viprs

@@ -103,6 +103,16 @@ __device__ void batch_pixel_row(const PixelArgs& a, int32_t ly) {
     const int bands = a.bands;
     const uint8_t* src = a.in.data + (int64_t)ly * a.in.pitch;
     uint8_t* dst = a.out.data + (int64_t)ly * a.out.pitch;
+    if (a.op == 3) {
+        // Zoom: the source row and pixel of each output pixel (zoom.rs:44-104)
+        src = a.in.data + ((a.out.y0 + ly) / a.zy - a.in.y0) * a.in.pitch;
+        for (int32_t x = threadIdx.x; x < a.out.w; x += kCThreads) {
+            const uint8_t* s = src + ((a.out.x0 + x) / a.zx - a.in.x0) * bands;
+            uint8_t* d = dst + (int64_t)x * bands;
+            for (int b = 0; b < bands; ++b) d[b] = s[b];
+        }
+        return;
+    }
     for (int32_t x = threadIdx.x; x < a.out.w; x += kCThreads) {
         const uint8_t* s = src + (int64_t)x * bands;
         uint8_t* d = dst + (int64_t)x * bands;

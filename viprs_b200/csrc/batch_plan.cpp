@@ -153,6 +153,10 @@ int plan_stages(viprs_batch* b, int image, std::vector<std::vector<BatchStage>>*
                 bs.af.xs = reinterpret_cast<const double*>(p->d_tables + st.starts_off);
                 bs.af.ys = reinterpret_cast<const double*>(p->d_tables + st.phases_off);
             }
+            if (st.axis_weights) {
+                bs.af.wx = reinterpret_cast<const double*>(p->d_tables + st.coeffs_off);
+                bs.af.wy = reinterpret_cast<const double*>(p->d_tables + st.coeffs2_off);
+            }
             bs.n_items = outp.h;
             break;
         }

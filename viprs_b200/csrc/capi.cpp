@@ -71,7 +71,11 @@ int required_region(const PlanNode& n, const ReduceKernel* rk, const ReduceKerne
     }
     case NodeKind::Affine: *in = affine_required_region(n, in_w, in_h, out); break;
     case NodeKind::ExtractArea: in->x = out.x + n.ex; in->y = out.y + n.ey; break;
-    case NodeKind::Zoom: return VIPRS_ERR_UNSUPPORTED_FORMAT;
+    case NodeKind::Zoom:
+        // Zoom::required_input_region (structural/zoom.rs:343-349)
+        if (out.w > 0) { in->x = out.x / n.zx; in->w = (out.x + out.w - 1) / n.zx - in->x + 1; }
+        if (out.h > 0) { in->y = out.y / n.zy; in->h = (out.y + out.h - 1) / n.zy - in->y + 1; }
+        break;
     default: break;
     }
     return VIPRS_OK;
@@ -407,7 +411,22 @@ int build_chain(viprs_plan* p, const Chain& chain) {
                 affine_axis_tables(st.af, xs.data(), ys.data());
                 st.starts_off = push_table(p->host_tables, xs.data(), xs.size() * 8);
                 st.phases_off = push_table(p->host_tables, ys.data(), ys.size() * 8);
+                if (affine_weight_tables_apply(st.af)) {
+                    std::vector<double> wx(xs.size() * kAxisTaps), wy(ys.size() * kAxisTaps);
+                    affine_weight_tables(st.af, xs.data(), ys.data(), wx.data(), wy.data());
+                    st.coeffs_off = push_table(p->host_tables, wx.data(), wx.size() * 8);
+                    st.coeffs2_off = push_table(p->host_tables, wy.data(), wy.size() * 8);
+                    st.axis_weights = true;
+                }
             }
+            p->stages.push_back(st);
+            cur = st.out_plane; ++i;
+            continue;
+        }
+        if (nd.kind == NodeKind::Zoom) {
+            Stage st; st.type = StageType::Pixel; st.in_plane = cur; st.out_plane = plane_for(i);
+            st.px.bands = int32_t(p->bands); st.px.fmt = p->fmt; st.px.op = 3;
+            st.px.zx = int32_t(nd.zx); st.px.zy = int32_t(nd.zy);
             p->stages.push_back(st);
             cur = st.out_plane; ++i;
             continue;
@@ -545,6 +564,10 @@ int execute_a(viprs_plan* p, const void* src, void* dst, cudaStream_t s, int fir
                 a.xs = reinterpret_cast<const double*>(p->d_tables + st.starts_off);
                 a.ys = reinterpret_cast<const double*>(p->d_tables + st.phases_off);
             }
+            if (st.axis_weights) {
+                a.wx = reinterpret_cast<const double*>(p->d_tables + st.coeffs_off);
+                a.wy = reinterpret_cast<const double*>(p->d_tables + st.coeffs2_off);
+            }
             e = launch::affine(a, s);
             break;
         }
@@ -558,6 +581,10 @@ int check_image(const viprs_image* im) {
     if (!im || !im->data) return VIPRS_ERR_NULL_POINTER;
     if (im->bands == 0) return VIPRS_ERR_INVALID_ARGUMENT;
     if (im->format < 0 || im->format > 2) return VIPRS_ERR_UNSUPPORTED_FORMAT;
+    // a row must start on a sample and hold a whole row of pixels
+    const uint64_t es = format_size(Format(im->format));
+    if (im->row_stride && (im->row_stride % es || im->row_stride < uint64_t(im->width) * im->bands * es))
+        return VIPRS_ERR_INVALID_ARGUMENT;
     return VIPRS_OK;
 }
 
@@ -647,6 +674,7 @@ int32_t nodes_to_chain(const viprs_node* nodes, int32_t n_nodes, int32_t demand_
         case VIPRS_NODE_REDUCE: n.kind = NodeKind::Reduce; break;
         case VIPRS_NODE_AFFINE: n.kind = NodeKind::Affine; break;
         case VIPRS_NODE_EXTRACT_AREA: n.kind = NodeKind::ExtractArea; break;
+        case VIPRS_NODE_ZOOM: n.kind = NodeKind::Zoom; break;
         default: return VIPRS_ERR_INVALID_ARGUMENT;
         }
         if (v.kernel < 0 || v.kernel > 9) return VIPRS_ERR_INVALID_KERNEL;
@@ -659,6 +687,7 @@ int32_t nodes_to_chain(const viprs_node* nodes, int32_t n_nodes, int32_t demand_
         n.extend = Extend(v.extend); n.background = v.background; n.premultiplied = v.premultiplied != 0;
         n.ex = v.area_x; n.ey = v.area_y;
         if (n.kind == NodeKind::ExtractArea) { n.ew = v.area_width; n.eh = v.area_height; }
+        if (n.kind == NodeKind::Zoom) { n.zx = v.factor_u; n.zy = v.vfactor_u; }
         n.demand = Demand(v.demand_hint);
         c.nodes.push_back(n);
     }
@@ -782,6 +811,11 @@ int32_t viprs_shrinkv(const viprs_image* in, const viprs_image* out, uint32_t fa
 
 int32_t viprs_shrink(const viprs_image* in, const viprs_image* out, uint32_t hf, uint32_t vf, void* stream) {
     PlanNode n; n.kind = NodeKind::Shrink; n.ufactor = hf; n.vufactor = vf;
+    return run_single(in, out, n, stream);
+}
+
+int32_t viprs_zoom(const viprs_image* in, const viprs_image* out, uint32_t xfac, uint32_t yfac, void* stream) {
+    PlanNode n; n.kind = NodeKind::Zoom; n.zx = xfac; n.zy = yfac;
     return run_single(in, out, n, stream);
 }
 

@@ -29,6 +29,8 @@ struct Stage {
     // offsets of this stage's tables inside the plan table buffer
     size_t starts_off = 0, phases_off = 0, coeffs_off = 0;
     size_t starts2_off = 0, phases2_off = 0, coeffs2_off = 0;
+    // affine: per-axis weight tables at coeffs_off (columns) / coeffs2_off (rows)
+    bool axis_weights = false;
 };
 
 struct PlaneInfo {

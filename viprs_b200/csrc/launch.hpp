@@ -157,7 +157,10 @@ struct PixelArgs {
     OutPlaneArg out;
     int32_t bands = 1;
     int32_t fmt = kU8;
-    int32_t op = 0;  // 0 copy, 1 premultiply, 2 unpremultiply
+    int32_t op = 0;  // 0 copy, 1 premultiply, 2 unpremultiply, 3 zoom
+    // zoom: output (x, y) takes source (x / zx, y / zy), both in image
+    // coordinates (the planes' origins x0 / y0 map them to local ones)
+    int32_t zx = 1, zy = 1;
 };
 
 namespace launch {

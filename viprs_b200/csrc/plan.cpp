@@ -403,7 +403,11 @@ int node_output_dims(const PlanNode& n, uint32_t iw, uint32_t ih, uint32_t* ow, 
     case NodeKind::ExtractArea:
         if (uint64_t(n.ex) + n.ew > iw || uint64_t(n.ey) + n.eh > ih) return VIPRS_ERR_INVALID_ARGUMENT;
         *ow = n.ew; *oh = n.eh; return VIPRS_OK;
-    case NodeKind::Zoom: *ow = iw * n.zx; *oh = ih * n.zy; return VIPRS_OK;
+    case NodeKind::Zoom:
+        // PipelineBuilder::zoom rejects a zero factor (builder/geometry.rs:618-624)
+        if (n.zx == 0 || n.zy == 0) return VIPRS_ERR_INVALID_ARGUMENT;
+        if (uint64_t(iw) * n.zx > 0xFFFFFFFFull || uint64_t(ih) * n.zy > 0xFFFFFFFFull) return VIPRS_ERR_INVALID_ARGUMENT;
+        *ow = iw * n.zx; *oh = ih * n.zy; return VIPRS_OK;
     default: *ow = iw; *oh = ih; return VIPRS_OK;
     }
 }
@@ -453,6 +457,7 @@ int builder_resize_chain(uint32_t w, uint32_t h, uint32_t bands, double hscale, 
     for (PlanNode n : plan.nodes) {
         n.demand = Demand::ThinStrip;
         if (n.kind == NodeKind::Affine) { n.extend = Extend::Copy; n.demand = Demand::SmallTile; }
+        if (n.kind == NodeKind::Zoom) n.demand = Demand::FatStrip;  // ZoomBridge's hint
         out->nodes.push_back(n);
     }
     return VIPRS_OK;

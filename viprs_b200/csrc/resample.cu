@@ -10,6 +10,7 @@
 //   reduce_v_kernel ..... ReduceV (reducev.rs:99-162; reduce_simd.rs:2700-2888) and
 //                         the vertical half of ReduceOp (reduce.rs:137-170)
 //   pixel_kernel ........ Premultiply / Unpremultiply / ExtractArea copies
+//   zoom_kernel ......... Zoom (structural/zoom.rs:44-149), 16-byte stores
 //
 // Memory traffic: the shrink reads every source sample exactly once with
 // 16-byte loads into shared memory (coalesced across the block) and writes
@@ -549,6 +550,20 @@ cudaError_t reduce2d(const Reduce2DArgs& a, cudaStream_t s) {
 cudaError_t pixel(const PixelArgs& a, cudaStream_t s) {
     const int64_t npx = (int64_t)a.out.w * a.out.h;
     if (npx <= 0) return cudaSuccess;
+    if (a.op == 3) {
+        // one block row per output row (grid-strided past 65535), enough
+        // blocks along x for one 16-byte chunk per thread
+        const int64_t row_bytes = (int64_t)a.out.w * a.bands * fmt_size(a.fmt);
+        const int64_t chunks = row_bytes / 16 + 1;
+        const dim3 grid((unsigned)std::max<int64_t>(1, std::min<int64_t>((chunks + 255) / 256, 64)),
+                        (unsigned)std::min<int64_t>(a.out.h, 65535));
+        switch (a.fmt) {
+        case kU8: dev::zoom_kernel<uint8_t><<<grid, 256, 0, s>>>(a); break;
+        case kU16: dev::zoom_kernel<uint16_t><<<grid, 256, 0, s>>>(a); break;
+        default: dev::zoom_kernel<float><<<grid, 256, 0, s>>>(a); break;
+        }
+        return cudaGetLastError();
+    }
     const unsigned grid = (unsigned)std::min<int64_t>((npx + 255) / 256, 148 * 16);
     switch (a.fmt) {
     case kU8: dev::pixel_kernel<uint8_t><<<grid, 256, 0, s>>>(a); break;

@@ -1097,5 +1097,57 @@ __global__ void pixel_kernel(PixelArgs a) {
     }
 }
 
+// Zoom: integer nearest-neighbour upscale (structural/zoom.rs:44-104): output
+// (x, y) repeats source (x / zx, y / zy).  blockIdx.y walks output rows; each
+// thread fills one 16-byte-aligned chunk of the row with a vector store,
+// gathering its elements from the source row (L1-resident: a source row is
+// read by zy output rows and each source pixel by zx output pixels) with the
+// pixel and repeat counters stepped instead of divided.  The elements before
+// the row's first 16-byte boundary and after its last are written singly.
+template <typename T>
+__global__ void __launch_bounds__(256) zoom_kernel(PixelArgs a) {
+    constexpr int V = 16 / (int)sizeof(T);
+    const int bands = a.bands;
+    const int64_t n = (int64_t)a.out.w * bands;
+    const int64_t zx = a.zx;
+    for (int64_t y = blockIdx.y; y < a.out.h; y += gridDim.y) {
+        const int64_t sy = (a.out.y0 + y) / a.zy - a.in.y0;
+        const T* src = reinterpret_cast<const T*>(a.in.data + sy * a.in.pitch);
+        T* dst = reinterpret_cast<T*>(a.out.data + y * a.out.pitch);
+        const int64_t mis = (int64_t)(reinterpret_cast<uintptr_t>(dst) & 15);
+        // a row not aligned to its element size never reaches a 16-byte
+        // boundary at an element: all of it is written singly
+        const int64_t head = mis % (int64_t)sizeof(T) ? n : (mis ? min(n, (16 - mis) / (int64_t)sizeof(T)) : 0);
+        const int64_t chunks = (n - head) / V;
+        const int64_t tail = head + chunks * V;
+        const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+        for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < chunks; c += stride) {
+            const int64_t e0 = head + c * V;
+            const int64_t x = e0 / bands;
+            int b = (int)(e0 - x * bands);
+            const int64_t gx = a.out.x0 + x;
+            int64_t q = gx / zx;
+            int64_t r = gx - q * zx;
+            union { T t[V]; uint4 u; } pk;
+#pragma unroll
+            for (int k = 0; k < V; ++k) {
+                pk.t[k] = src[(q - a.in.x0) * bands + b];
+                if (++b == bands) {
+                    b = 0;
+                    if (++r == zx) { r = 0; ++q; }
+                }
+            }
+            *reinterpret_cast<uint4*>(dst + e0) = pk.u;
+        }
+        const int64_t singles = head + (n - tail);
+        for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < singles; t += stride) {
+            const int64_t e = t < head ? t : tail + (t - head);
+            const int64_t x = e / bands;
+            const int b = (int)(e - x * bands);
+            dst[e] = src[((a.out.x0 + x) / zx - a.in.x0) * bands + b];
+        }
+    }
+}
+
 }  // namespace dev
 }  // namespace viprs
