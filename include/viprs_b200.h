@@ -73,8 +73,8 @@ typedef enum {
 } viprs_thumb_target;
 
 /* An image buffer.  row_stride is in bytes; 0 means width*bands*sample size.
-   A nonzero stride is a multiple of the sample size and at least that size
-   (else INVALID_ARGUMENT). */
+   data is aligned to the sample size; a nonzero stride is a multiple of the
+   sample size and at least that size (else INVALID_ARGUMENT). */
 typedef struct {
     void *data;
     uint32_t width;

@@ -170,14 +170,32 @@ def test_resize(oracle, fmt, scale):
 @pytest.mark.parametrize("fmt", FMTS)
 @pytest.mark.parametrize("fac", [(1, 1), (2, 3), (3, 1), (1, 2), (5, 4)])
 @pytest.mark.parametrize("bands", [1, 3, 4])
-def test_zoom(oracle, fmt, fac, bands):
-    """Zoom: integer nearest-neighbour upscale (structural/zoom.rs), odd widths
-    so that rows start off 16-byte boundaries."""
-    rng = np.random.default_rng(fac[0] * 7 + fac[1] + bands)
-    img = rand_image(rng, 37, 53, bands, fmt)
+@pytest.mark.parametrize("width", [53, 64])
+def test_zoom(oracle, fmt, fac, bands, width):
+    """Zoom: integer nearest-neighbour upscale (structural/zoom.rs).  Width 53
+    gives rows that start off 16-byte boundaries (the per-row kernel), width 64
+    rows whose pitch is a multiple of 16 (output rows of a source row together)."""
+    rng = np.random.default_rng(fac[0] * 7 + fac[1] + bands + width)
+    img = rand_image(rng, 37, width, bands, fmt)
     got = to_host(api.zoom(to_dev(img), fac[0], fac[1]))
     exp = oracle.zoom(img, fac[0], fac[1])
     assert np.array_equal(exp, np.repeat(np.repeat(img, fac[1], 0), fac[0], 1))
+    assert got.shape == exp.shape and np.array_equal(got, exp)
+
+
+@pytest.mark.parametrize("fmt", FMTS)
+@pytest.mark.parametrize("area", [(5, 7, 48, 30), (4, 3, 37, 41), (0, 1, 64, 9)])
+def test_zoom_then_extract(oracle, fmt, area):
+    """Zoom into an intermediate plane whose region starts inside the image
+    (the ExtractArea after it asks for an offset window), bit-exact."""
+    rng = np.random.default_rng(area[0] * 31 + area[2])
+    img = rand_image(rng, 29, 35, 2, fmt)
+    b = api.PipelineBuilder.from_tensor(to_dev(img)).zoom(3, 2).extract_area(*area)
+    got = to_host(b.run())
+    exp = oracle.pipeline(img, [oracle.make_node("zoom", demand="fat", ufactor=3, ceil_mode=2),
+                                oracle.make_node("extract", ex=area[0], ey=area[1], ew=area[2], eh=area[3])])
+    assert np.array_equal(exp, np.repeat(np.repeat(img, 2, 0), 3, 1)[area[1]:area[1] + area[3],
+                                                                       area[0]:area[0] + area[2]])
     assert got.shape == exp.shape and np.array_equal(got, exp)
 
 

@@ -346,3 +346,15 @@ def test_row_stride_must_hold_whole_samples(fmt, stride):
     src = _host_image(buf, 4, 4, 1, fmt, stride)
     dst = _host_image(buf, 8, 8, 1, fmt)
     assert lib.viprs_zoom(ctypes.byref(src), ctypes.byref(dst), 2, 2, None) == 1
+
+
+@pytest.mark.parametrize("fmt", [1, 2])
+def test_data_must_be_sample_aligned(fmt):
+    """u16 / f32 data at an odd address is INVALID_ARGUMENT before any device work."""
+    from viprs_b200 import _native
+    lib = _native.lib()
+    buf = (ctypes.c_uint8 * 256)()
+    base = ctypes.addressof(buf)
+    src = _host_image(base + 1, 4, 4, 1, fmt)
+    dst = _host_image(base, 8, 8, 1, fmt)
+    assert lib.viprs_zoom(ctypes.byref(src), ctypes.byref(dst), 2, 2, None) == 1

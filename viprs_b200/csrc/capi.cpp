@@ -583,6 +583,7 @@ int check_image(const viprs_image* im) {
     if (im->format < 0 || im->format > 2) return VIPRS_ERR_UNSUPPORTED_FORMAT;
     // a row must start on a sample and hold a whole row of pixels
     const uint64_t es = format_size(Format(im->format));
+    if (reinterpret_cast<uintptr_t>(im->data) % es) return VIPRS_ERR_INVALID_ARGUMENT;
     if (im->row_stride && (im->row_stride % es || im->row_stride < uint64_t(im->width) * im->bands * es))
         return VIPRS_ERR_INVALID_ARGUMENT;
     return VIPRS_OK;

@@ -555,8 +555,20 @@ cudaError_t pixel(const PixelArgs& a, cudaStream_t s) {
         // blocks along x for one 16-byte chunk per thread
         const int64_t row_bytes = (int64_t)a.out.w * a.bands * fmt_size(a.fmt);
         const int64_t chunks = row_bytes / 16 + 1;
-        const dim3 grid((unsigned)std::max<int64_t>(1, std::min<int64_t>((chunks + 255) / 256, 64)),
-                        (unsigned)std::min<int64_t>(a.out.h, 65535));
+        const unsigned gx = (unsigned)std::max<int64_t>(1, std::min<int64_t>((chunks + 255) / 256, 64));
+        if (a.out.pitch % 16 == 0 && a.bands <= dev::kZoomMaxBands && a.in.h > 0) {
+            // output rows of one source row together (see zoom_rows_kernel)
+            const unsigned gxr = (unsigned)std::max<int64_t>(
+                1, std::min<int64_t>((chunks + dev::kZoomChunks - 1) / dev::kZoomChunks, 64));
+            const dim3 grid(gxr, (unsigned)std::min<int64_t>(a.in.h, 65535));
+            switch (a.fmt) {
+            case kU8: dev::zoom_rows_kernel<uint8_t><<<grid, 256, 0, s>>>(a); break;
+            case kU16: dev::zoom_rows_kernel<uint16_t><<<grid, 256, 0, s>>>(a); break;
+            default: dev::zoom_rows_kernel<float><<<grid, 256, 0, s>>>(a); break;
+            }
+            return cudaGetLastError();
+        }
+        const dim3 grid(gx, (unsigned)std::min<int64_t>(a.out.h, 65535));
         switch (a.fmt) {
         case kU8: dev::zoom_kernel<uint8_t><<<grid, 256, 0, s>>>(a); break;
         case kU16: dev::zoom_kernel<uint16_t><<<grid, 256, 0, s>>>(a); break;

@@ -1149,5 +1149,90 @@ __global__ void __launch_bounds__(256) zoom_kernel(PixelArgs a) {
     }
 }
 
+// Zoom for destinations whose rows share their 16-byte phase (pitch a
+// multiple of 16) and at most kZoomMaxBands bands.  blockIdx.y walks SOURCE
+// rows: the zy output rows that repeat one source row are identical, so each
+// 16-byte chunk is gathered once and stored to all of them.  A block takes
+// kZoomChunks chunks of the row at a time (kZoomChunks / 256 per thread,
+// strided so that a warp's stores are contiguous), stages the source span
+// they read in shared memory with 4-byte loads (the span's first and last
+// words may reach up to 3 bytes past it: a word never crosses a page), and
+// gathers from there.
+constexpr int kZoomMaxBands = 64;
+constexpr int kZoomPerThread = 4;
+constexpr int kZoomChunks = 256 * kZoomPerThread;
+// span bytes: kZoomChunks 16-byte chunks read at most kZoomChunks * 16 - 1 + 3
+// pixels' worth of sample bytes beyond them, plus 3 bytes of word alignment
+constexpr int kZoomSpanWords = (kZoomChunks * 16 + 3 * kZoomMaxBands * 4 + 8) / 4;
+
+template <typename T>
+__global__ void __launch_bounds__(256) zoom_rows_kernel(PixelArgs a) {
+    constexpr int V = 16 / (int)sizeof(T);
+    __shared__ __align__(16) uint32_t span[kZoomSpanWords];
+    const uint8_t* span_b = reinterpret_cast<const uint8_t*>(span);
+    const int bands = a.bands;
+    const int64_t n = (int64_t)a.out.w * bands;
+    const int64_t zx = a.zx, zy = a.zy;
+    const int64_t mis = (int64_t)(reinterpret_cast<uintptr_t>(a.out.data) & 15);
+    const int64_t head = mis % (int64_t)sizeof(T) ? n : (mis ? min(n, (16 - mis) / (int64_t)sizeof(T)) : 0);
+    const int64_t chunks = (n - head) / V;
+    const int64_t tail = head + chunks * V;
+    for (int64_t r = blockIdx.y; r < a.in.h; r += gridDim.y) {
+        const int64_t gsy = a.in.y0 + r;
+        const int64_t y_lo = max(gsy * zy - a.out.y0, (int64_t)0);
+        const int64_t y_hi = min((gsy + 1) * zy - a.out.y0, (int64_t)a.out.h);
+        if (y_lo >= y_hi) continue;  // the same for the whole block
+        const T* src = reinterpret_cast<const T*>(a.in.data + r * a.in.pitch);
+        for (int64_t c0 = (int64_t)blockIdx.x * kZoomChunks; c0 < chunks; c0 += (int64_t)gridDim.x * kZoomChunks) {
+            const int64_t c1 = min(chunks, c0 + kZoomChunks);
+            const int64_t e_first = head + c0 * V, e_last = head + c1 * V - 1;
+            const int64_t p_first = (a.out.x0 + e_first / bands) / zx - a.in.x0;
+            const int64_t p_last = (a.out.x0 + e_last / bands) / zx - a.in.x0;
+            const uint8_t* sb = reinterpret_cast<const uint8_t*>(src + p_first * bands);
+            const uint8_t* se = reinterpret_cast<const uint8_t*>(src + (p_last + 1) * bands);
+            const uint32_t* w0 = reinterpret_cast<const uint32_t*>(reinterpret_cast<uintptr_t>(sb) & ~(uintptr_t)3);
+            const int delta = (int)(sb - reinterpret_cast<const uint8_t*>(w0));
+            const int nw = (int)((se - reinterpret_cast<const uint8_t*>(w0) + 3) >> 2);
+            __syncthreads();  // the previous span's readers are done
+            for (int i = threadIdx.x; i < nw; i += blockDim.x) span[i] = __ldg(w0 + i);
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < kZoomPerThread; ++k) {
+                const int64_t c = c0 + threadIdx.x + 256 * k;
+                if (c >= c1) break;
+                const int64_t e0 = head + c * V;
+                const int64_t x = e0 / bands;
+                int b = (int)(e0 - x * bands);
+                const int64_t gx = a.out.x0 + x;
+                const int64_t q = gx / zx;
+                int64_t rem = gx - q * zx;
+                int si = (int)((q - a.in.x0 - p_first) * bands) + b;
+                union { T t[V]; uint4 u; } pk;
+#pragma unroll
+                for (int j = 0; j < V; ++j) {
+                    pk.t[j] = *reinterpret_cast<const T*>(span_b + delta + si * (int)sizeof(T));
+                    ++si;
+                    if (++b == bands) {
+                        b = 0;
+                        if (++rem == zx) rem = 0;  // next source pixel: si already points at it
+                        else si -= bands;          // the same source pixel again
+                    }
+                }
+                for (int64_t y = y_lo; y < y_hi; ++y)
+                    *reinterpret_cast<uint4*>(reinterpret_cast<T*>(a.out.data + y * a.out.pitch) + e0) = pk.u;
+            }
+        }
+        const int64_t singles = head + (n - tail);
+        const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+        for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < singles; t += stride) {
+            const int64_t e = t < head ? t : tail + (t - head);
+            const int64_t x = e / bands;
+            const int b = (int)(e - x * bands);
+            const T v = src[((a.out.x0 + x) / zx - a.in.x0) * bands + b];
+            for (int64_t y = y_lo; y < y_hi; ++y) reinterpret_cast<T*>(a.out.data + y * a.out.pitch)[e] = v;
+        }
+    }
+}
+
 }  // namespace dev
 }  // namespace viprs
