@@ -167,3 +167,25 @@ def test_mapim_alpha_opaque_matches_premultiplied(oracle):
     idx = np.stack([xx * 1.2 + 0.3, yy * 1.1 + 0.45], -1).astype(np.float32)
     for kernel in ("nearest", "bilinear"):
         assert np.array_equal(oracle.mapim(src, idx, kernel), oracle.mapim(src, idx, kernel, premultiplied=True))
+
+
+def test_zoom_repeats_nearest_neighbour(oracle):
+    """structural/zoom.rs process_region_repeats_nearest_neighbour: Zoom(2, 2)
+    of [[1, 2], [3, 4]]."""
+    src = np.array([[1, 2], [3, 4]], np.uint8)[:, :, None]
+    out = oracle.zoom(src, 2, 2)[:, :, 0]
+    assert out.reshape(-1).tolist() == [1, 1, 2, 2, 1, 1, 2, 2, 3, 3, 4, 4, 3, 3, 4, 4]
+
+
+def test_zoom_output_dimensions_scale_by_factor(oracle):
+    """structural/zoom.rs output_dimensions_scale_by_factor: ZoomBridge(3, 2)
+    maps 4 x 5 to 12 x 10."""
+    out = oracle.zoom(np.zeros((5, 4, 1), np.uint8), 3, 2)
+    assert out.shape == (10, 12, 1)
+
+
+@pytest.mark.parametrize("rows,cols", [(1, 1), (3, 5), (6, 6)])
+def test_zoom_factor_1_is_identity(oracle, rows, cols):
+    """structural/zoom.rs zoom_factor_1_is_identity (sizes 1..=6)."""
+    src = np.arange(rows * cols, dtype=np.uint8).reshape(rows, cols, 1)
+    assert np.array_equal(oracle.zoom(src, 1, 1), src)
