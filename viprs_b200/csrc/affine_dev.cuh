@@ -285,6 +285,38 @@ struct AffineCtx {
 #pragma unroll
         for (int b = 0; b < MB; ++b) acc[b] = 0.0;
         double wsum = 0.0;
+        // every tap inside the image, the tile's input region and the plane:
+        // each reads the image at its own address (tap() would resolve to the
+        // same), so the taps are loaded directly
+        const int64_t px0 = tx0 - a.in.x0, py0 = ty0 - a.in.y0;
+        const bool interior = tx0 >= rx0 && tx0 + nt - 1 <= rx1 && ty0 >= ry0 && ty0 + nt - 1 <= ry1 &&
+                              px0 >= 0 && px0 + nt <= (int64_t)a.in.w && py0 >= 0 && py0 + nt <= (int64_t)a.in.h;
+        if (interior && !pm) {
+            const uint8_t* row = a.in.data + py0 * a.in.pitch;
+            for (int j = 0; j < nt; ++j, row += a.in.pitch) {
+                const double wy = wys[j];
+                if (wy == 0.0) continue;
+                const T* px = reinterpret_cast<const T*>(row) + px0 * bands;
+#pragma unroll
+                for (int i = 0; i < kAxisTaps; ++i) {
+                    if (i >= nt) break;
+                    if (wx[i] == 0.0) continue;
+                    const double w = wx[i] * wy;
+                    wsum += w;
+#pragma unroll
+                    for (int b = 0; b < MB; ++b) {
+                        if (b >= bands) break;
+                        acc[b] = fma((double)px[i * bands + b], w, acc[b]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < MB; ++b) {
+                if (b >= bands) break;
+                out[b] = wsum > 0.0 ? acc[b] / wsum : f;
+            }
+            return;
+        }
         for (int j = 0; j < nt; ++j) {
             const double wy = wys[j];
             if (wy == 0.0) continue;
@@ -509,7 +541,7 @@ __device__ void affine_pixel(const AffineArgs& a, int64_t lx, int64_t ly) {
 // the output rows (grid-stride): a thread's pixels share the tile region and
 // the incremental walk.
 template <typename T, int NB>
-__global__ void __launch_bounds__(256) affine_kernel(AffineArgs a) {
+__global__ void __launch_bounds__(256, 2) affine_kernel(AffineArgs a) {
     const int G = a.group;
     const int64_t lx0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * G;
     if (lx0 >= a.out.w) return;
