@@ -500,6 +500,10 @@ def other_resize_up(stream, steps):
     plan2 = api.resize_plan(1024, 768, 3, torch.uint8, 2.5)
     out2 = torch.empty(plan2.out_shape, dtype=torch.uint8, device="cuda")
     ms2 = timed(lambda: plan2(small, out2), steps, 3, stream)
+    sim_b = api.PipelineBuilder(1024, 768, 3, torch.uint8).similarity(1.25, 30.0, "bicubic")
+    plan3 = sim_b.build()
+    out3 = torch.empty(plan3.out_shape, dtype=torch.uint8, device="cuda")
+    ms3 = timed(lambda: plan3(small, out3), steps, 3, stream)
     peak, _ = measured_hbm_peak()
     return {"workload": "resize 2.0 of 4096x3072x3 u8 (Zoom 2x2, 16-byte stores)",
             "mpix_per_s": round(out.numel() / 3 / 1e6 / (ms / 1e3), 1), "ms": round(ms, 4),
@@ -507,7 +511,11 @@ def other_resize_up(stream, steps):
             "frac": round(b / (ms / 1e3) / 1e9 / peak, 4), "launches": plan.launches,
             "resize_2_5_1024x768": {"workload": "resize 2.5 Lanczos3 1024x768x3 u8 (Zoom 2x2 + affine 1.25)",
                                     "ms": round(ms2, 4), "launches": plan2.launches,
-                                    "mpix_per_s": round(out2.numel() / 3 / 1e6 / (ms2 / 1e3), 1)}}
+                                    "mpix_per_s": round(out2.numel() / 3 / 1e6 / (ms2 / 1e3), 1)},
+            "similarity_1024x768": {"workload": "similarity scale 1.25 angle 30 bicubic 1024x768x3 u8 (auto canvas)",
+                                    "ms": round(ms3, 4), "launches": plan3.launches,
+                                    "out": list(plan3.out_shape),
+                                    "mpix_per_s": round(out3.numel() / 3 / 1e6 / (ms3 / 1e3), 1)}}
 
 
 def other_reduce_affine_grad(stream, steps):

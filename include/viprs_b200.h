@@ -125,6 +125,14 @@ int32_t viprs_shrinkv(const viprs_image *in, const viprs_image *out, uint32_t fa
 /* PipelineBuilder::shrink -> Shrink::process_region (resample/shrink.rs:179-293). */
 int32_t viprs_shrink(const viprs_image *in, const viprs_image *out, uint32_t hfactor,
                      uint32_t vfactor, void *stream);
+/* PipelineBuilder::similarity -> SimilarityOp::new_auto_canvas
+   (resample/similarity.rs:47-81, 178-232; builder/resample.rs:595-626): scale
+   and rotate by `angle` degrees about the origin onto the transformed
+   bounding box (libvips's canvas rounding), i.e. an affine with Background(0).
+   A scale that is not finite and positive counts as 1.  `out` has the canvas
+   size viprs_similarity_node reports. */
+int32_t viprs_similarity(const viprs_image *in, const viprs_image *out, double scale, double angle,
+                         int32_t kernel, void *stream);
 /* PipelineBuilder::zoom -> Zoom::process_region (structural/zoom.rs:310-398;
    builder/geometry.rs:618-643): integer nearest-neighbour upscale, output
    (x, y) = input (x / xfac, y / yfac), output size width*xfac x height*yfac.
@@ -225,6 +233,15 @@ int32_t viprs_resize_plan_nodes(double hscale, double vscale, int32_t kernel, do
                                 uint32_t width, uint32_t height, viprs_node *nodes,
                                 int32_t capacity, int32_t *n_nodes, uint32_t *out_width,
                                 uint32_t *out_height);
+/* Host only: the output size of a node chain on a width x height source
+   (PipelineBuilder::current_dimensions after those builder calls). */
+int32_t viprs_chain_output_size(uint32_t width, uint32_t height, const viprs_node *nodes,
+                                int32_t n_nodes, uint32_t *out_width, uint32_t *out_height);
+/* Host only: the Affine node PipelineBuilder::similarity runs on a width x
+   height image (backward matrix, canvas translation in tx / ty, canvas size in
+   out_width / out_height, SmallTile hint), for a chain plan or a batch. */
+int32_t viprs_similarity_node(double scale, double angle, int32_t kernel, uint32_t width,
+                              uint32_t height, viprs_node *node);
 /* PipelineBuilder::resize(Resize::new(hscale, vscale, kernel)) (builder/resample.rs:637-711). */
 int32_t viprs_resize_plan_create(uint32_t width, uint32_t height, uint32_t bands, int32_t format,
                                  double hscale, double vscale, int32_t kernel,

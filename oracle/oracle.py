@@ -8,6 +8,7 @@ Images are numpy arrays shaped (height, width, bands), row-major and
 band-interleaved like viprs's tiles (crates/viprs-core/src/image/region.rs).
 """
 import ctypes
+import math
 import os
 
 import numpy as np
@@ -272,6 +273,41 @@ def affine_backward(img, m, tx, ty, out_w, out_h, kernel="bilinear", extend="bac
                   kernel=kernel, extend=extend, background=float(background),
                   premultiplied=int(premultiplied), demand=demand)
     return pipeline(img, [n], threads=threads)
+
+
+def _round_vips(v):
+    """round_vips (resample/similarity.rs:223-230): half away from zero, truncated."""
+    return int(v + 0.5) if v > 0.0 else int(v - 0.5)
+
+
+def similarity_node(w, h, scale, angle):
+    """SimilarityOp::new_auto_canvas (resample/similarity.rs:47-81, 178-221): the
+    backward matrix, the canvas translation and the canvas size."""
+    s = scale if math.isfinite(scale) and scale > 0.0 else 1.0
+    rad = angle * (math.pi / 180.0)
+    c, sn = math.cos(rad), math.sin(rad)
+    a, b, cc, d = s * c, s * -sn, s * sn, s * c
+    left = top = cw = ch = 0
+    if w and h:
+        W, H = float(w), float(h)
+        x2, y2, x3, y3 = a * W, cc * W, b * H, d * H
+        x4, y4 = _fma(b, H, a * W), _fma(d, H, cc * W)
+        lo_x, hi_x = min(0.0, x2, x3, x4), max(0.0, x2, x3, x4)
+        lo_y, hi_y = min(0.0, y2, y3, y4), max(0.0, y2, y3, y4)
+        left, top = _round_vips(lo_x), _round_vips(lo_y)
+        cw, ch = max(_round_vips(hi_x - lo_x), 0), max(_round_vips(hi_y - lo_y), 0)
+    m = [c / s, sn / s, -sn / s, c / s]
+    tx = _fma(m[1], float(top), m[0] * float(left))
+    ty = _fma(m[3], float(top), m[2] * float(left))
+    return m, tx, ty, cw, ch
+
+
+def similarity(img, scale, angle, kernel="bilinear", threads=1):
+    """PipelineBuilder::similarity (builder/resample.rs:595-626): the affine of
+    similarity_node with Background(0) on SmallTile tiles."""
+    a = _as_image(img)
+    m, tx, ty, cw, ch = similarity_node(a.shape[1], a.shape[0], scale, angle)
+    return affine_backward(a, m, tx, ty, cw, ch, kernel, "background", 0.0, demand="smalltile", threads=threads)
 
 
 def forward_affine_to_backward(matrix, tx, ty):

@@ -199,6 +199,36 @@ def test_zoom_then_extract(oracle, fmt, area):
     assert got.shape == exp.shape and np.array_equal(got, exp)
 
 
+@pytest.mark.parametrize("fmt", [np.uint8, np.uint16, np.float32])
+@pytest.mark.parametrize("kernel", ["nearest", "bilinear", "bicubic", "lanczos3"])
+@pytest.mark.parametrize("sa", [(1.0, 0.0), (0.75, 12.0), (1.25, 90.0), (2.0, 45.0), (0.6, -137.5)])
+@pytest.mark.parametrize("bands", [1, 3])
+def test_similarity(oracle, fmt, kernel, sa, bands):
+    """PipelineBuilder::similarity (resample/similarity.rs): the auto-canvas
+    affine, bit-exact (u8/u16) or within the f32 bar against the oracle."""
+    rng = np.random.default_rng(int(sa[0] * 100) + abs(int(sa[1])) + bands)
+    img = rand_image(rng, 47, 61, bands, fmt)
+    got = to_host(api.similarity(to_dev(img), sa[0], sa[1], kernel))
+    exp = oracle.similarity(img, sa[0], sa[1], kernel)
+    assert got.shape == exp.shape
+    assert_same(got, exp, fmt)
+
+
+def test_similarity_in_a_chain(oracle):
+    """similarity after a reduce, through the builder (canvas from the
+    chain's current size)."""
+    rng = np.random.default_rng(11)
+    img = rand_image(rng, 90, 120, 3, np.uint8)
+    b = api.PipelineBuilder.from_tensor(to_dev(img)).reduce_h(2.0, "lanczos3").similarity(1.5, 30.0, "bicubic")
+    got = to_host(b.run())
+    mid = oracle.reduce_h(img, 2.0, "lanczos3")
+    m, tx, ty, cw, ch = oracle.similarity_node(mid.shape[1], mid.shape[0], 1.5, 30.0)
+    exp = oracle.pipeline(img, [oracle.make_node("reduceh", factor=2.0, kernel="lanczos3"),
+                                oracle.make_node("affine", m=m, tx=tx, ty=ty, out_w=cw, out_h=ch, kernel="bicubic",
+                                                 extend="background", background=0.0, demand="smalltile")])
+    assert got.shape == exp.shape and np.array_equal(got, exp)
+
+
 def test_zoom_zero_factor_is_an_error():
     img = to_dev(np.zeros((4, 4, 1), np.uint8))
     with pytest.raises(ViprsError):

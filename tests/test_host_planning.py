@@ -358,3 +358,27 @@ def test_data_must_be_sample_aligned(fmt):
     src = _host_image(base + 1, 4, 4, 1, fmt)
     dst = _host_image(base, 8, 8, 1, fmt)
     assert lib.viprs_zoom(ctypes.byref(src), ctypes.byref(dst), 2, 2, None) == 1
+
+
+@pytest.mark.parametrize("scale", [1.0, 0.75, 1.25, 2.0, 0.3, -4.0])
+@pytest.mark.parametrize("angle", [0.0, 12.0, 30.0, 45.0, 90.0, 137.5, 180.0, -60.0, 270.0])
+@pytest.mark.parametrize("size", [(4, 3), (4, 2), (5, 3), (640, 480), (1, 1), (1023, 17)])
+def test_similarity_node_matches_oracle(oracle, scale, angle, size):
+    """The product's similarity planner (viprs_similarity_node) against the
+    oracle's restatement of SimilarityOp::new_auto_canvas, field for field."""
+    from viprs_b200 import _native
+    n = _native.Node()
+    assert _native.lib().viprs_similarity_node(scale, angle, 1, size[0], size[1], ctypes.byref(n)) == 0
+    m, tx, ty, cw, ch = oracle.similarity_node(size[0], size[1], scale, angle)
+    assert list(n.matrix) == m and (n.tx, n.ty) == (tx, ty)
+    assert (n.out_width, n.out_height) == (cw, ch)
+    assert n.kind == 6 and n.extend == 2 and n.background == 0.0 and n.demand_hint == 3
+
+
+def test_chain_output_size_on_host():
+    """viprs_chain_output_size follows the builder's current dimensions."""
+    from viprs_b200 import api
+    b = api.PipelineBuilder(1024, 768, 3, None).shrink_h(2).zoom(3, 2).reduce_v(2.0)
+    assert b.output_size() == (1536, 768)
+    b.similarity(1.0, 90.0)
+    assert b.output_size() == (768, 1536)

@@ -189,3 +189,26 @@ def test_zoom_factor_1_is_identity(oracle, rows, cols):
     """structural/zoom.rs zoom_factor_1_is_identity (sizes 1..=6)."""
     src = np.arange(rows * cols, dtype=np.uint8).reshape(rows, cols, 1)
     assert np.array_equal(oracle.zoom(src, 1, 1), src)
+
+
+def test_similarity_canvas_kats(oracle):
+    """resample/similarity.rs unit tests: auto canvas of the identity (4 x 3),
+    a right angle (4 x 2 -> 2 x 4), scale 1.25 (5 x 3 -> 6 x 4, libvips's
+    transform-rect rounding), invalid scales fall back to 1, empty input."""
+    assert oracle.similarity_node(4, 3, 1.0, 0.0)[3:] == (4, 3)
+    assert oracle.similarity_node(4, 2, 1.0, 90.0)[3:] == (2, 4)
+    assert oracle.similarity_node(5, 3, 1.25, 0.0)[3:] == (6, 4)
+    assert oracle.similarity_node(0, 3, -4.0, 0.0)[3:] == (0, 0)
+    assert oracle.similarity_node(7, 5, float("nan"), 30.0) == oracle.similarity_node(7, 5, 1.0, 30.0)
+    assert oracle.similarity_node(7, 5, -4.0, 30.0) == oracle.similarity_node(7, 5, 1.0, 30.0)
+    assert oracle._round_vips(-1.2) == -1 and oracle._round_vips(-1.8) == -2
+
+
+@pytest.mark.parametrize("kernel", ["nearest", "bilinear", "bicubic"])
+def test_similarity_identity(oracle, kernel):
+    """scale 1, angle 0 is the identity (similarity.rs scale1_angle0_is_identity,
+    identity_preserves_uniform_input)."""
+    src = np.arange(16, dtype=np.uint8).reshape(4, 4, 1)
+    assert np.array_equal(oracle.similarity(src, 1.0, 0.0, kernel), src)
+    uni = np.full((5, 7, 1), 173, np.uint8)
+    assert np.array_equal(oracle.similarity(uni, 1.0, 0.0, kernel), uni)

@@ -68,6 +68,9 @@ SIGNATURES = {
     "viprs_shrinkv": (_I, [_IMG, _IMG, _U, _I, _P]),
     "viprs_shrink": (_I, [_IMG, _IMG, _U, _U, _P]),
     "viprs_zoom": (_I, [_IMG, _IMG, _U, _U, _P]),
+    "viprs_similarity": (_I, [_IMG, _IMG, _D, _D, _I, _P]),
+    "viprs_similarity_node": (_I, [_D, _D, _I, _U, _U, ctypes.POINTER(Node)]),
+    "viprs_chain_output_size": (_I, [_U, _U, _P, _I, ctypes.POINTER(_U), ctypes.POINTER(_U)]),
     "viprs_premultiply": (_I, [_IMG, _IMG, _P]),
     "viprs_unpremultiply": (_I, [_IMG, _IMG, _P]),
     "viprs_affine": (_I, [_IMG, _IMG, ctypes.POINTER(_D), _D, _D, _I, _P]),

@@ -124,6 +124,26 @@ def shrink(t, hfactor, vfactor):
     return out
 
 
+def similarity_node(width, height, scale, angle, kernel="bilinear"):
+    """The Affine node PipelineBuilder::similarity runs (resample/similarity.rs:47-81)."""
+    n = N.Node()
+    N.check(N.lib().viprs_similarity_node(float(scale), float(angle), _kernel(kernel), int(width), int(height),
+                                          ctypes.byref(n)), "similarity")
+    return n
+
+
+def similarity(t, scale, angle, kernel="bilinear"):
+    """PipelineBuilder::similarity: scale and rotate by `angle` degrees onto the
+    transformed bounding box, Background(0) (resample/similarity.rs)."""
+    t = _as_hwc(t)
+    h, w, b = t.shape
+    n = similarity_node(w, h, scale, angle, kernel)
+    out = _empty(n.out_height, n.out_width, b, t)
+    N.check(N.lib().viprs_similarity(image(t), image(out), float(scale), float(angle), _kernel(kernel), _stream()),
+            "similarity")
+    return out
+
+
 def zoom(t, xfac, yfac):
     """PipelineBuilder::zoom: integer nearest-neighbour upscale (structural/zoom.rs)."""
     t = _as_hwc(t)
@@ -363,6 +383,13 @@ class PipelineBuilder:
     def zoom(self, xfac, yfac):
         return self._node("zoom", demand="fat", factor_u=xfac, vfactor_u=yfac)
 
+    def similarity(self, scale, angle, kernel="bilinear"):
+        if self._composite is not None:
+            raise ValueError("thumbnail/resize must be the only op of this builder")
+        w, h = self.output_size()
+        self.nodes.append(similarity_node(w, h, scale, angle, kernel))
+        return self
+
     def thumbnail(self, target="width", target_width=0, target_height=0, kernel="lanczos3", crop=False):
         if self.nodes:
             raise ValueError("thumbnail is planned on the source image: call it first")
@@ -375,6 +402,17 @@ class PipelineBuilder:
             raise ValueError("resize is planned on the source image: call it first")
         self._composite = resize_plan(self.width, self.height, self.bands, self.dtype, hscale, vscale, kernel)
         return self
+
+    def output_size(self):
+        """(width, height) after the nodes so far (PipelineBuilder::current_dimensions)."""
+        if self._composite is not None:
+            h, w, _ = self._composite.out_shape
+            return w, h
+        arr = (N.Node * max(1, len(self.nodes)))(*self.nodes)
+        ow, oh = ctypes.c_uint32(), ctypes.c_uint32()
+        N.check(N.lib().viprs_chain_output_size(self.width, self.height, arr, len(self.nodes), ctypes.byref(ow),
+                                                ctypes.byref(oh)), "chain_output_size")
+        return ow.value, oh.value
 
     def build(self):
         if self._composite is not None:

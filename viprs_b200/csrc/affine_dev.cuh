@@ -227,6 +227,24 @@ struct AffineCtx {
             default: break;
             }
         }
+        if (a.kernel >= 2) {
+            // separable kernels: each axis's weights once for all bands (the
+            // values sample() evaluates per band), then pixel_tab's taps
+            if (!isfinite(x) || !isfinite(y)) {
+                for (int b = 0; b < bands; ++b) out[b] = fill();
+                return;
+            }
+            const int k = a.kernel, nt = separable_taps(k), support = nt / 2;
+            const int64_t tx0 = trunc_i64(floor(x)) - (support - 1), ty0 = trunc_i64(floor(y)) - (support - 1);
+            double wxs[kAxisTaps], wys[kAxisTaps];
+#pragma unroll
+            for (int t = 0; t < kAxisTaps; ++t) {
+                wxs[t] = t < nt ? kernel_w(k, fabs((double)(tx0 + t) - x)) : 0.0;
+                wys[t] = t < nt ? kernel_w(k, fabs((double)(ty0 + t) - y)) : 0.0;
+            }
+            pixel_tab<NB>(x, y, wxs, wys, out);
+            return;
+        }
         if (bands == 4 && !a.premultiplied) {
             if (!isfinite(x) || !isfinite(y)) {
                 for (int b = 0; b < bands; ++b) out[b] = fill();

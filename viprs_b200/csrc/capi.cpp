@@ -815,6 +815,15 @@ int32_t viprs_shrink(const viprs_image* in, const viprs_image* out, uint32_t hf,
     return run_single(in, out, n, stream);
 }
 
+int32_t viprs_similarity(const viprs_image* in, const viprs_image* out, double scale, double angle, int32_t kernel,
+                         void* stream) {
+    if (kernel < 0 || kernel > 9) return VIPRS_ERR_INVALID_KERNEL;
+    if (!std::isfinite(angle)) return VIPRS_ERR_INVALID_ARGUMENT;
+    if (!in) return VIPRS_ERR_NULL_POINTER;
+    const PlanNode n = similarity_node(scale, angle, Kernel(kernel), in->width, in->height);
+    return run_single(in, out, n, stream);
+}
+
 int32_t viprs_zoom(const viprs_image* in, const viprs_image* out, uint32_t xfac, uint32_t yfac, void* stream) {
     PlanNode n; n.kind = NodeKind::Zoom; n.zx = xfac; n.zy = yfac;
     return run_single(in, out, n, stream);
@@ -958,6 +967,28 @@ int32_t viprs_resize_plan_nodes(double hscale, double vscale, int32_t kernel, do
     *out_w = plan.output_width;
     *out_h = plan.output_height;
     return export_nodes(plan.nodes, nodes, capacity);
+}
+
+int32_t viprs_chain_output_size(uint32_t w, uint32_t h, const viprs_node* nodes, int32_t n_nodes, uint32_t* out_w,
+                                uint32_t* out_h) {
+    if (!out_w || !out_h) return VIPRS_ERR_NULL_POINTER;
+    Chain c;
+    int32_t st = nodes_to_chain(nodes, n_nodes, -1, &c);
+    if (st) return st;
+    for (const PlanNode& n : c.nodes) {
+        st = node_output_dims(n, w, h, &w, &h);
+        if (st) return st;
+    }
+    *out_w = w;
+    *out_h = h;
+    return VIPRS_OK;
+}
+
+int32_t viprs_similarity_node(double scale, double angle, int32_t kernel, uint32_t w, uint32_t h, viprs_node* node) {
+    if (!node) return VIPRS_ERR_NULL_POINTER;
+    if (kernel < 0 || kernel > 9) return VIPRS_ERR_INVALID_KERNEL;
+    if (!std::isfinite(angle)) return VIPRS_ERR_INVALID_ARGUMENT;
+    return export_nodes({similarity_node(scale, angle, Kernel(kernel), w, h)}, node, 1);
 }
 
 int32_t viprs_thumbnail_plan_create(uint32_t w, uint32_t h, uint32_t bands, int32_t format, int32_t target,

@@ -4,7 +4,9 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <climits>
 #include <cmath>
+#include <cstdint>
 
 #include "viprs_b200.h"
 
@@ -461,6 +463,50 @@ int builder_resize_chain(uint32_t w, uint32_t h, uint32_t bands, double hscale, 
         out->nodes.push_back(n);
     }
     return VIPRS_OK;
+}
+
+// round_vips (resample/similarity.rs:223-230): half away from zero, then
+// Rust's saturating `as i32`.
+static int32_t round_vips(double v) {
+    const double r = v > 0.0 ? v + 0.5 : v - 0.5;
+    if (!(r == r)) return 0;
+    if (r >= 2147483647.0) return INT32_MAX;
+    if (r <= -2147483648.0) return INT32_MIN;
+    return int32_t(r);
+}
+
+PlanNode similarity_node(double scale, double angle, Kernel kernel, uint32_t in_w, uint32_t in_h) {
+    const double s = std::isfinite(scale) && scale > 0.0 ? scale : 1.0;  // safe_scale (:178-185)
+    const double rad = angle * (kPi / 180.0);                            // f64::to_radians
+    const double c = std::cos(rad), sn = std::sin(rad);
+    // auto_canvas (:191-221) of the forward matrix
+    const double a = s * c, b = s * -sn, cc = s * sn, d = s * c;
+    int32_t left = 0, top = 0, cw = 0, ch = 0;
+    if (in_w != 0 && in_h != 0) {
+        const double W = double(in_w), H = double(in_h);
+        const double x2 = a * W, y2 = cc * W, x3 = b * H, y3 = d * H;
+        const double x4 = std::fma(b, H, a * W), y4 = std::fma(d, H, cc * W);
+        const double l = std::fmin(std::fmin(std::fmin(0.0, x2), x3), x4);
+        const double r = std::fmax(std::fmax(std::fmax(0.0, x2), x3), x4);
+        const double t = std::fmin(std::fmin(std::fmin(0.0, y2), y3), y4);
+        const double bt = std::fmax(std::fmax(std::fmax(0.0, y2), y3), y4);
+        left = round_vips(l);
+        top = round_vips(t);
+        cw = std::max(round_vips(r - l), 0);
+        ch = std::max(round_vips(bt - t), 0);
+    }
+    PlanNode n;
+    n.kind = NodeKind::Affine;
+    // inverse_similarity_matrix (:187-189), translation of the canvas origin (:66-67)
+    n.m[0] = c / s; n.m[1] = sn / s; n.m[2] = -sn / s; n.m[3] = c / s;
+    n.tx = std::fma(n.m[1], double(top), n.m[0] * double(left));
+    n.ty = std::fma(n.m[3], double(top), n.m[2] * double(left));
+    n.out_w = uint32_t(cw); n.out_h = uint32_t(ch);
+    n.kernel = kernel;
+    n.extend = Extend::Background;  // Affine::new's Background(0)
+    n.background = 0.0;
+    n.demand = Demand::SmallTile;   // SimilarityBridge's hint
+    return n;
 }
 
 int forward_affine_to_backward(const double f[4], double tx, double ty, double b[4], double* btx, double* bty) {

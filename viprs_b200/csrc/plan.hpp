@@ -126,6 +126,11 @@ int builder_thumbnail_chain(uint32_t w, uint32_t h, uint32_t bands, ThumbTarget 
 int builder_resize_chain(uint32_t w, uint32_t h, uint32_t bands, double hscale, double vscale,
                          Kernel kernel, Chain* out);
 
+// SimilarityOp::new_auto_canvas (resample/similarity.rs:47-81, 178-232) as the
+// Affine node PipelineBuilder::similarity runs (builder/resample.rs:595-626):
+// backward matrix, canvas translation and size, Background(0), SmallTile.
+PlanNode similarity_node(double scale, double angle, Kernel kernel, uint32_t in_w, uint32_t in_h);
+
 // forward_affine_to_backward (builder/resample.rs:25-60); status 0 ok.
 int forward_affine_to_backward(const double fwd[4], double tx, double ty, double bwd[4], double* btx,
                                double* bty);
